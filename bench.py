@@ -1,0 +1,399 @@
+"""Throughput benchmark of the FlowPM particle-mesh step on B200.
+
+Workload (one "step" = one full forward simulation through the library):
+128^3 particles on a 128^3 mesh, box 200 Mpc/h, Planck15, 2LPT initial
+conditions at a0 = 0.1 from a seeded Eisenstein-Hu Gaussian field, then 40
+kick-drift-kick steps to a = 1 (41 force evaluations); FP32 displacement
+state, FP64 background.  Metric: particle-updates/s = particles x leapfrog
+steps / device time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun every rank advances its own replica (different seed), the
+timed region is bracketed by barriers and the max device time over ranks is
+used.  ``--impl reference`` times the CPU restatement of the reference's
+algorithm (torch on the host cores) on a bounded sample of the same
+workload instead.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_MESH = 128
+BOX = 200.0
+A0 = 0.1
+N_STEPS = 40
+METRIC = 'particle-updates/s'
+WORKLOAD = ('C2: forward PM, 128^3 particles / 128^3 mesh, box 200 Mpc/h, '
+            'Planck15, 2LPT at a0=0.1, 40 KDK steps to a=1')
+# Algorithmic HBM bytes (FP32, Np = Nc): per leapfrog step of the whole
+# pass 60 Np + 64 Nc = 124 B per particle-update; per launch of the fused
+# step kernel: read d, p (24 Np) + write d, p (24 Np) + gather the three
+# force meshes (12 Nc) + paint the density (4 Nc) = 64 B per particle.
+STEP_BYTES_PER_PART = 124
+KERNEL_BYTES_PER_PART = 64
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+  ap = argparse.ArgumentParser()
+  ap.add_argument('--gpus', type=int, default=1)
+  ap.add_argument('--steps', type=int, default=10)
+  ap.add_argument('--warmup', type=int, default=3)
+  ap.add_argument('--impl', default='flowpm_b200',
+                  choices=['flowpm_b200', 'reference'])
+  ap.add_argument('--no-cpu-baseline', action='store_true')
+  return ap.parse_args()
+
+
+def dist_env():
+  rank = int(os.environ.get('RANK', 0))
+  world = int(os.environ.get('WORLD_SIZE', 1))
+  local = int(os.environ.get('LOCAL_RANK', 0))
+  return rank, world, local
+
+
+def pk_fn():
+  from flowpm_b200 import cosmology, tfpower
+  cosmo = cosmology.Planck15()
+  kk = np.logspace(-4, 2, 4096)
+  pk = tfpower.linear_matter_power(cosmo, kk)
+  return lambda k: np.interp(np.log(np.maximum(k, 1e-30)), np.log(kk), pk,
+                             left=0.0)
+
+
+class ClockSampler(object):
+  """nvidia-smi clock / throttle samples during the timed region."""
+  Q = ('index,clocks.sm,clocks.max.sm,power.draw,'
+       'clocks_event_reasons.hw_slowdown,'
+       'clocks_event_reasons.hw_thermal_slowdown,'
+       'clocks_event_reasons.sw_thermal_slowdown,'
+       'clocks_event_reasons.sw_power_cap')
+
+  def __init__(self, index):
+    self.index = index
+    self.proc = None
+
+  def __enter__(self):
+    try:
+      self.proc = subprocess.Popen(
+          ['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.Q,
+           '--format=csv,noheader,nounits', '-lms', '200'],
+          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+      self.proc = None
+    time.sleep(0.3)
+    return self
+
+  def __exit__(self, *exc):
+    self.lines = []
+    if self.proc is not None:
+      time.sleep(0.3)
+      self.proc.terminate()
+      out, _ = self.proc.communicate(timeout=10)
+      self.lines = [l for l in out.splitlines() if l.strip()]
+    return False
+
+  def summary(self):
+    sm, mx, reasons = [], None, set()
+    names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+             'sw_power_cap']
+    for l in self.lines:
+      f = [x.strip() for x in l.split(',')]
+      if len(f) < 8:
+        continue
+      try:
+        sm.append(float(f[1]))
+        mx = float(f[2])
+      except ValueError:
+        continue
+      for n, v in zip(names, f[4:8]):
+        if v.lower().startswith('active'):
+          reasons.add(n)
+    return {
+        'sm_mhz': float(np.median(sm)) if sm else None,
+        'sm_max_mhz': mx,
+        'reasons': sorted(reasons),
+        'samples': len(sm)
+    }
+
+
+def peaks():
+  path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+  try:
+    with open(path) as f:
+      return float(json.load(f)['hbm_gbs']), 'measured'
+  except (OSError, KeyError, ValueError):
+    return 6650.0, 'fallback'
+
+
+def cpu_baseline(sample_steps=2):
+  """Oracle (torch on the host cores) on the same 128^3 workload: 2LPT
+  initial state, then ``sample_steps`` leapfrog steps plus the initial
+  force; returns particle-updates/s of the leapfrog steps."""
+  from oracle import background as obg
+  from oracle import pm as opm
+  torch.set_num_threads(os.cpu_count() or 1)
+  rng = np.random.default_rng(0)
+  lin = torch.tensor(rng.standard_normal((1, N_MESH, N_MESH, N_MESH)) * 0.3,
+                     dtype=torch.float32)
+  b = obg.Background({}, dtype=np.float32)
+  s0 = opm.lpt_init(b, lin, A0, order=2)
+  stages = np.linspace(A0, 1.0, N_STEPS + 1)[:sample_steps + 1]
+  t0 = time.perf_counter()
+  opm.nbody(b, s0, stages, N_MESH)
+  dt = time.perf_counter() - t0
+  n = N_MESH**3 * sample_steps
+  return {
+      'value': n / dt,
+      'unit': METRIC,
+      'cores': torch.get_num_threads(),
+      'kind': 'port',
+      'sample': '%d of the 40 leapfrog steps (+ the initial force) of the '
+                '128^3 workload, torch-CPU restatement of flowpm/tfpm.py, '
+                'FP32, %.1f s' % (sample_steps, dt)
+  }
+
+
+def run_reference(args, rank, world):
+  """CPU arm: the oracle port of the reference on the host cores."""
+  if rank != 0:
+    return
+  from oracle import background as obg
+  from oracle import pm as opm
+  torch.set_num_threads(os.cpu_count() or 1)
+  rng = np.random.default_rng(0)
+  lin = torch.tensor(rng.standard_normal((1, N_MESH, N_MESH, N_MESH)) * 0.3,
+                     dtype=torch.float32)
+  b = obg.Background({}, dtype=np.float32)
+  s0 = opm.lpt_init(b, lin, A0, order=2)
+  stages = np.linspace(A0, 1.0, N_STEPS + 1)
+  # one bench step = one leapfrog step (kick, drift, force, kick) of the
+  # 128^3 workload; the initial force is computed once, untimed
+  state = opm.force(b, s0, N_MESH)
+  times = []
+  for i in range(args.warmup + args.steps):
+    a0, a1 = stages[i % N_STEPS], stages[i % N_STEPS + 1]
+    ah = (a0 * a1)**0.5
+    t0 = time.perf_counter()
+    st = opm.kick(b, state, a0, a0, ah)
+    st = opm.drift(b, st, a0, ah, a1)
+    st = opm.force(b, st, N_MESH)
+    st = opm.kick(b, st, ah, a1, a1)
+    dt = time.perf_counter() - t0
+    if i >= args.warmup:
+      times.append(dt)
+  t = float(np.sum(times))
+  v = N_MESH**3 * len(times) / t
+  line = {
+      'impl': 'reference',
+      'metric': METRIC,
+      'value': v,
+      'unit': METRIC,
+      'n_gpus': world,
+      'steps': args.steps,
+      'warmup': args.warmup,
+      'ms_per_step': 1e3 * t / len(times),
+      'higher_is_better': True,
+      'scaling': 'weak',
+      'vs_baseline': None,
+      'dtype': 'f32',
+      'data': 'synthetic',
+      'config': {'workload': WORKLOAD, 'mesh': N_MESH,
+                 'particles': N_MESH**3, 'box': BOX,
+                 'step': 'one leapfrog step of the workload (CPU sample)'},
+      'cpu_baseline': {
+          'value': v, 'unit': METRIC, 'cores': torch.get_num_threads(),
+          'kind': 'port',
+          'sample': '%d leapfrog steps of the 128^3 workload, torch-CPU '
+                    'restatement of flowpm/tfpm.py (FP32)' % len(times)},
+      'e2e': {'value': v, 'unit': METRIC, 'h2d_bytes_per_step': 0,
+              'd2h_bytes_per_step': 0},
+  }
+  print(json.dumps(line))
+
+
+def main():
+  args = parse()
+  rank, world, local = dist_env()
+  if args.impl == 'reference':
+    run_reference(args, rank, world)
+    return
+  import flowpm_b200 as fpm
+  from flowpm_b200 import _lib, tfbackground
+  from flowpm_b200._plans import get_plan
+  torch.cuda.set_device(local)
+  dist = None
+  if world > 1:
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group('nccl', timeout=timedelta(seconds=300))
+
+  def barrier():
+    if dist is not None:
+      dist.barrier()
+    torch.cuda.synchronize()
+
+  cosmo = fpm.cosmology.Planck15()
+  nc = [N_MESH] * 3
+  npart = N_MESH**3
+  lin = fpm.linear_field(nc, BOX, pk_fn(), batch_size=1, seed=1000 + rank)
+  s0 = fpm.lpt_init(cosmo, lin, A0, order=2)
+  stages = np.linspace(A0, 1.0, N_STEPS + 1)
+  plan = get_plan([tuple(nc) + (1,)])
+  coefs = tfbackground.nbody_coefficients(cosmo, stages)
+  st = _lib.stream_ptr()
+  _lib.call('fpm_nbody_set_steps', plan.handle, N_STEPS, _lib.ivec([N_STEPS]),
+            _lib.dvec(coefs.ravel()), _lib.dvec([1.5 * cosmo.Omega_m]), st)
+  d0 = fpm.tfpm._to_disp(s0[0], nc).contiguous()
+  p0 = s0[1].contiguous().clone()
+  d, p = torch.empty_like(d0), torch.empty_like(p0)
+  f = torch.empty_like(d0)
+  flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device='cuda')
+
+  def one_step():
+    _lib.call('fpm_nbody_run', plan.handle, _lib.ptr(d), _lib.ptr(p),
+              _lib.ptr(f), None, 0, st)
+
+  def reset():
+    d.copy_(d0)
+    p.copy_(p0)
+    flush.fill_(float(rank))  # evicts L2 (256 MB > 126 MB)
+
+  for _ in range(args.warmup):
+    reset()
+    one_step()
+  if plan.status(st):
+    raise RuntimeError('non-finite state in warm-up')
+  starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+  ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+  _lib.call('fpm_plan_profile', plan.handle, 1)
+  n_launch0 = _lib.lib.fpm_launch_count()
+  barrier()
+  with ClockSampler(local) as clk:
+    for i in range(args.steps):
+      reset()
+      starts[i].record()
+      one_step()
+      ends[i].record()
+    barrier()
+  n_launch = _lib.lib.fpm_launch_count() - n_launch0
+  ms = float(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+  kt, kn = {}, {}
+  for kind, name in [(0, 'step'), (1, 'fourier'), (2, 'paint')]:
+    tot, cnt = _lib.c_double(), _lib.c_int64()
+    _lib.call('fpm_plan_profile_read', plan.handle, kind,
+              _lib.ctypes.byref(tot), _lib.ctypes.byref(cnt))
+    kt[name], kn[name] = tot.value, cnt.value
+  _lib.call('fpm_plan_profile', plan.handle, 0)
+  if plan.status(st):
+    raise RuntimeError('non-finite state in the timed region')
+  ms_max = ms
+  if dist is not None:
+    t = torch.tensor([ms], device='cuda', dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+  updates = float(npart) * N_STEPS * args.steps * world
+  value = updates / (ms_max * 1e-3)
+
+  # End to end through the public API: host state in (pinned), nbody,
+  # final state back to the host, every step.
+  host_in = s0.cpu().pin_memory()
+  host_out = torch.empty_like(host_in).pin_memory()
+  e_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+  e_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+  for i in range(args.warmup + args.steps):
+    if i >= args.warmup:
+      flush.fill_(1.0)
+      e_s[i - args.warmup].record()
+    dev = host_in.to('cuda', non_blocking=True)
+    out = fpm.nbody(cosmo, dev, stages, nc, check_finite=False)
+    host_out.copy_(out, non_blocking=True)
+    if i >= args.warmup:
+      e_e[i - args.warmup].record()
+  torch.cuda.synchronize()
+  ms_e2e = float(sum(s.elapsed_time(e) for s, e in zip(e_s, e_e)))
+  if dist is not None:
+    t = torch.tensor([ms_e2e], device='cuda', dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_e2e = float(t.item())
+  if not np.isfinite(host_out.numpy()).all():
+    raise RuntimeError('non-finite end-to-end result')
+  e2e_value = updates / (ms_e2e * 1e-3)
+
+  peak, peak_kind = peaks()
+  step_ms = kt['step'] / max(kn['step'], 1)
+  kbytes = KERNEL_BYTES_PER_PART * npart
+  achieved = kbytes / (step_ms * 1e-3) / 1e9
+  whole = STEP_BYTES_PER_PART * npart * N_STEPS * args.steps / (ms * 1e-3) / 1e9
+  line = {
+      'metric': METRIC,
+      'value': value,
+      'unit': METRIC,
+      'n_gpus': world,
+      'steps': args.steps,
+      'warmup': args.warmup,
+      'ms_per_step': ms_max / args.steps,
+      'higher_is_better': True,
+      'scaling': 'weak',
+      'vs_baseline': None,
+      'dtype': 'f32',
+      'data': 'synthetic',
+      'config': {
+          'workload': WORKLOAD,
+          'mesh': N_MESH,
+          'particles': npart,
+          'box': BOX,
+          'leapfrog_steps_per_step': N_STEPS,
+          'background': 'f64',
+          'parallelism': 'replicas x%d' % world,
+          'l2': 'flushed (256 MB write) before every timed step',
+      },
+      'e2e': {
+          'value': e2e_value,
+          'unit': METRIC,
+          'h2d_bytes_per_step': int(host_in.numel() * 4),
+          'd2h_bytes_per_step': int(host_out.numel() * 4),
+      },
+      'gpu_launches': int(n_launch),
+      'roofline': {
+          'kernel': 'k_step (fused readout + kick + drift + CIC paint)',
+          'bound': 'hbm',
+          'achieved': achieved,
+          'peak': peak,
+          'peak_kind': peak_kind,
+          'unit': 'GB/s',
+          'frac': achieved / peak,
+          'traffic': None,
+          'algorithmic_bytes_per_launch': kbytes,
+          'avg_launch_ms': step_ms,
+      },
+      'whole_step_roofline': {
+          'bytes_per_particle_update': STEP_BYTES_PER_PART,
+          'achieved_gbs': whole,
+          'frac': whole / peak,
+      },
+      'kernel_ms_per_step': {k: kt[k] / args.steps for k in kt},
+      'clocks': clk.summary(),
+  }
+  if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    line['cpu_baseline'] = cpu_baseline()
+  if rank == 0:
+    print(json.dumps(line))
+  if dist is not None:
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+  main()

@@ -1,0 +1,72 @@
+"""Plan objects of the C library (``fpm_plan_create``) and their cache.
+
+A plan owns the cuFFT plans and mesh work buffers of one set of
+simulations; creating it allocates device memory, so plans are cached per
+(device, dims, options) and reused across calls.
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+
+
+class Plan(object):
+  """One ``fpm_plan``: ``dims`` is a list of (nx, ny, nz, pm_nc_factor)."""
+
+  def __init__(self, dims, r_split=0.0, flags=0):
+    self.dims = [tuple(int(v) for v in d) for d in dims]
+    self.flags = int(flags)
+    self.r_split = float(r_split)
+    flat = [v for d in self.dims for v in d]
+    h = ctypes.c_void_p()
+    _lib.call('fpm_plan_create', ctypes.byref(h), len(self.dims),
+              _lib.ivec(flat), self.r_split, self.flags)
+    self.handle = h
+    np_tot, nbytes = ctypes.c_int64(), ctypes.c_int64()
+    _lib.call('fpm_plan_info', h, ctypes.byref(np_tot), ctypes.byref(nbytes))
+    self.total_particles = np_tot.value
+    self.device_bytes = nbytes.value
+
+  @property
+  def nsims(self):
+    return len(self.dims)
+
+  def status(self, stream=None):
+    """Read and clear the device status word (synchronises the stream)."""
+    v = ctypes.c_int32()
+    _lib.call('fpm_plan_status', self.handle, ctypes.byref(v),
+              stream or _lib.stream_ptr())
+    return v.value
+
+  def close(self):
+    if getattr(self, 'handle', None) is not None and self.handle.value:
+      _lib.lib.fpm_plan_destroy(self.handle)
+      self.handle = None
+
+  def __del__(self):
+    try:
+      self.close()
+    except Exception:  # interpreter shutdown
+      pass
+
+
+_cache = {}
+
+
+def get_plan(dims, r_split=0.0, flags=0):
+  key = (torch.cuda.current_device(), tuple(tuple(d) for d in dims),
+         float(r_split), int(flags))
+  plan = _cache.get(key)
+  if plan is None:
+    plan = Plan(dims, r_split, flags)
+    _cache[key] = plan
+  return plan
+
+
+def clear_plans():
+  """Release every cached plan (their device buffers and cuFFT plans)."""
+  torch.cuda.synchronize()
+  for p in list(_cache.values()):
+    p.close()
+  _cache.clear()

@@ -1,0 +1,553 @@
+// Particle-mesh step kernels for sm_100a.
+//
+// All kernels are persistent grid-stride loops over "chunks" of kChunk
+// elements; a chunk never straddles two simulations, and the owning
+// simulation is found by binary search over the per-sim first chunk, so the
+// same launch advances a batch of simulations of different sizes.
+#include <atomic>
+
+#include "fpm_kernels.cuh"
+
+namespace fpm {
+
+// ---------------------------------------------------------------------------
+// Particle kernels
+// ---------------------------------------------------------------------------
+
+// Lattice coordinates of particle `local` of a sim (index (i*ny + j)*nz + k,
+// the order of np.indices(nc).reshape(3, -1).T at flowpm/tfpm.py:162).
+__device__ __forceinline__ void lattice_ijk(const SimDev& S, int64_t local,
+                                            int& i, int& j, int& k) {
+  const int64_t t = local / S.nz;
+  k = (int)(local - t * S.nz);
+  i = (int)(t / S.ny);
+  j = (int)(t - (int64_t)i * S.ny);
+}
+
+// Position in force-mesh units: (q + d) * bf, as the reference's
+// state[0] * pm_nc_factor with state[0] = q + d.
+__device__ __forceinline__ float3 mesh_pos(const SimDev& S, int i, int j,
+                                           int k, float3 d) {
+  const float b = (float)S.bf;
+  float3 x;
+  x.x = __fmul_rn(__fadd_rn((float)i, d.x), b);
+  x.y = __fmul_rn(__fadd_rn((float)j, d.y), b);
+  x.z = __fmul_rn(__fadd_rn((float)k, d.z), b);
+  return x;
+}
+
+__device__ __forceinline__ void paint8(float* __restrict__ m, int my, int mz,
+                                       const Axis& ax, const Axis& ay,
+                                       const Axis& az) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
+    const float w = cic_w(ax, ay, az, cx, cy, cz);
+    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
+              iz = cz ? az.i1 : az.i0;
+    red_add(m + ((int64_t)ix * my + iy) * mz + iz, w);
+  }
+}
+
+// Readout of the three force components at the same 8 neighbours.
+__device__ __forceinline__ float3 readout3(const float* __restrict__ f0,
+                                           int64_t mcells, int my, int mz,
+                                           const Axis& ax, const Axis& ay,
+                                           const Axis& az) {
+  float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
+    const float w = cic_w(ax, ay, az, cx, cy, cz);
+    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
+              iz = cz ? az.i1 : az.i0;
+    const int64_t o = ((int64_t)ix * my + iy) * mz + iz;
+    r0 = __fadd_rn(r0, __fmul_rn(__ldg(f0 + o), w));
+    r1 = __fadd_rn(r1, __fmul_rn(__ldg(f0 + mcells + o), w));
+    r2 = __fadd_rn(r2, __fmul_rn(__ldg(f0 + 2 * mcells + o), w));
+  }
+  return make_float3(r0, r1, r2);
+}
+
+__device__ __forceinline__ float3 ld3(const float* p, int64_t g) {
+  return make_float3(p[3 * g], p[3 * g + 1], p[3 * g + 2]);
+}
+__device__ __forceinline__ void st3(float* p, int64_t g, float3 v) {
+  p[3 * g] = v.x;
+  p[3 * g + 1] = v.y;
+  p[3 * g + 2] = v.z;
+}
+// a + s * b with the two roundings of the reference (update = fac * F,
+// state = state + update).
+__device__ __forceinline__ float3 axpy(float3 a, float s, float3 b) {
+  return make_float3(__fadd_rn(a.x, __fmul_rn(s, b.x)),
+                     __fadd_rn(a.y, __fmul_rn(s, b.y)),
+                     __fadd_rn(a.z, __fmul_rn(s, b.z)));
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_paint_lattice(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+                const float* __restrict__ disp, float* __restrict__ rho,
+                int32_t* status) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const SimDev S = sims[find_sim(sims, nsims, ch, kPart)];
+    const int64_t base = (ch - S.ch_p) * kChunk + threadIdx.x;
+    float* m = rho + S.m_off;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t local = base + it * kThreads;
+      if (local >= S.np) break;
+      int i, j, k;
+      lattice_ijk(S, local, i, j, k);
+      const float3 d = ld3(disp, S.p_off + local);
+      const float3 x = mesh_pos(S, i, j, k, d);
+      if (!finite3(x.x, x.y, x.z)) atomicOr(status, FPM_STATUS_NONFINITE_POS);
+      paint8(m, S.my, S.mz, cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
+             cic_axis(x.z, S.mz));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+       StepArgs a) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kPart);
+    const SimDev S = sims[s];
+    const int T = a.nsteps[s];
+    if (a.it > T) continue;  // this sim has finished
+    const float* cf = a.coefs + (int64_t)s * a.max_steps * 3;
+    const float ke = a.it >= 1 ? cf[(a.it - 1) * 3 + 2] : 0.f;
+    const bool last = (a.it == T);
+    const float ks = last ? 0.f : cf[a.it * 3 + 0];
+    const float dr = last ? 0.f : cf[a.it * 3 + 1];
+    const float fac = a.ffac[s];
+    const float invb = 1.0f / (float)S.bf;
+    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
+    const float* f0 = a.fmesh + 3 * S.m_off;
+    float* m = a.rho + S.m_off;
+    const int64_t base = (ch - S.ch_p) * kChunk + threadIdx.x;
+#pragma unroll 1
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t local = base + it * kThreads;
+      if (local >= S.np) break;
+      const int64_t g = S.p_off + local;
+      int i, j, k;
+      lattice_ijk(S, local, i, j, k);
+      float3 d = ld3(a.disp, g);
+      float3 p = ld3(a.mom, g);
+      const float3 x = mesh_pos(S, i, j, k, d);
+      const Axis ax = cic_axis(x.x, S.mx), ay = cic_axis(x.y, S.my),
+                 az = cic_axis(x.z, S.mz);
+      float3 f = readout3(f0, mcells, S.my, S.mz, ax, ay, az);
+      // force = readout * factor / pm_nc_factor (flowpm/tfpm.py:218, :356)
+      f.x = __fmul_rn(__fmul_rn(f.x, fac), invb);
+      f.y = __fmul_rn(__fmul_rn(f.y, fac), invb);
+      f.z = __fmul_rn(__fmul_rn(f.z, fac), invb);
+      if (a.it >= 1) p = axpy(p, ke, f);  // closing kick of step it-1
+      if (a.inter && a.it >= 1) {
+        float* o = a.inter + (int64_t)(a.it - 1) * 3 * a.total_np * 3;
+        st3(o, g,
+            make_float3(__fadd_rn((float)i, d.x), __fadd_rn((float)j, d.y),
+                        __fadd_rn((float)k, d.z)));
+        st3(o + a.total_np * 3, g, p);
+        st3(o + 2 * a.total_np * 3, g, f);
+      }
+      if (last) {
+        st3(a.force_out, g, f);
+        st3(a.mom, g, p);
+        if (!finite3(p.x, p.y, p.z) || !finite3(f.x, f.y, f.z))
+          atomicOr(a.status, FPM_STATUS_NONFINITE_MOM);
+        continue;
+      }
+      p = axpy(p, ks, f);  // opening kick of step it
+      d = axpy(d, dr, p);  // drift of step it
+      st3(a.mom, g, p);
+      st3(a.disp, g, d);
+      const float3 xn = mesh_pos(S, i, j, k, d);
+      if (!finite3(xn.x, xn.y, xn.z))
+        atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
+      paint8(m, S.my, S.mz, cic_axis(xn.x, S.mx), cic_axis(xn.y, S.my),
+             cic_axis(xn.z, S.mz));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_force_readout(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+                const float* __restrict__ disp,
+                const float* __restrict__ fmesh,
+                const float* __restrict__ ffac, float* __restrict__ force) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kPart);
+    const SimDev S = sims[s];
+    const float fac = ffac[s];
+    const float invb = 1.0f / (float)S.bf;
+    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
+    const float* f0 = fmesh + 3 * S.m_off;
+    const int64_t base = (ch - S.ch_p) * kChunk + threadIdx.x;
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t local = base + it * kThreads;
+      if (local >= S.np) break;
+      const int64_t g = S.p_off + local;
+      int i, j, k;
+      lattice_ijk(S, local, i, j, k);
+      const float3 x = mesh_pos(S, i, j, k, ld3(disp, g));
+      float3 f = readout3(f0, mcells, S.my, S.mz, cic_axis(x.x, S.mx),
+                          cic_axis(x.y, S.my), cic_axis(x.z, S.mz));
+      f.x = __fmul_rn(__fmul_rn(f.x, fac), invb);
+      f.y = __fmul_rn(__fmul_rn(f.y, fac), invb);
+      f.z = __fmul_rn(__fmul_rn(f.z, fac), invb);
+      st3(force, g, f);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fourier kernels
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void mode_ijl(int64_t local, int ny, int nzh,
+                                         int& i, int& j, int& l) {
+  const int64_t t = local / nzh;
+  l = (int)(local - t * nzh);
+  i = (int)(t / ny);
+  j = (int)(t - (int64_t)i * ny);
+}
+
+// Force spectra, flowpm/tfpm.py:199-215 apply_longrange:
+//   pot_k = delta_k * lap * longrange;  force_d = pot_k * (i g_d)
+// with delta_k = R2C(rho) / (nbar N^3), lap = 1/k^2 rounded to float (0 at
+// k = 0, where the gradient vanishes anyway), g_d the 4-point gradient.
+__global__ void __launch_bounds__(kThreads)
+k_fourier_force(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+                const float2* __restrict__ dk, float2* __restrict__ fk,
+                float* __restrict__ rho_zero, AxisTabs tabs, double r2,
+                int deconv) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const SimDev S = sims[find_sim(sims, nsims, ch, kSpec)];
+    const int64_t nmodes = (int64_t)S.mx * S.my * S.mzh;
+    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
+    // 1 / (nbar N^3) with nbar = Np / N^3 = 1 / bf^3.
+    const float pre =
+        (float)((double)S.bf * S.bf * S.bf / (double)mcells);
+    const double* kkx = tabs.kk + S.tab;
+    const double* kky = kkx + S.mx;
+    const double* kkz = kky + S.my;
+    const float* gx = tabs.grad + S.tab;
+    const float* gy = gx + S.mx;
+    const float* gz = gy + S.my;
+    const float* wx = tabs.win + S.tab;
+    const float* wy = wx + S.mx;
+    const float* wz = wy + S.my;
+    const int64_t base = (ch - S.ch_s) * kChunk + threadIdx.x;
+    const float2* din = dk + S.s_off;
+    float2* o0 = fk + 3 * S.s_off;
+    float2* o1 = o0 + nmodes;
+    float2* o2 = o1 + nmodes;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t local = base + it * kThreads;
+      if (local < nmodes) {
+        int i, j, l;
+        mode_ijl(local, S.my, S.mzh, i, j, l);
+        const double kk = kkx[i] + kky[j] + kkz[l];
+        float w = kk == 0.0 ? 0.f : (float)(1.0 / kk);
+        if (r2 != 0.0) w = __fmul_rn(w, (float)exp(-kk * r2));
+        if (deconv) w = __fmul_rn(w, __fmul_rn(__fmul_rn(wx[i], wy[j]), wz[l]));
+        float2 dv = din[local];
+        dv.x = __fmul_rn(dv.x, pre);
+        dv.y = __fmul_rn(dv.y, pre);
+        const float pr = __fmul_rn(dv.x, w), pi = __fmul_rn(dv.y, w);
+        const float g0 = gx[i], g1 = gy[j], g2 = gz[l];
+        o0[local] = make_float2(-__fmul_rn(pi, g0), __fmul_rn(pr, g0));
+        o1[local] = make_float2(-__fmul_rn(pi, g1), __fmul_rn(pr, g1));
+        o2[local] = make_float2(-__fmul_rn(pi, g2), __fmul_rn(pr, g2));
+      }
+      // Zero the density mesh for the next paint (2 cells per mode slot).
+      if (rho_zero) {
+        for (int64_t c = local; c < mcells; c += nmodes)
+          rho_zero[S.m_off + c] = 0.f;
+      }
+    }
+  }
+}
+
+// LPT spectra (flowpm/tfpm.py:66-145 lpt1 / lpt2_source on the lattice).
+__global__ void __launch_bounds__(kThreads)
+k_lpt_fourier(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+              const float2* __restrict__ dk, float2* __restrict__ out,
+              int mode, AxisTabs tabs) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const SimDev S = sims[find_sim(sims, nsims, ch, kLatSpec)];
+    const int64_t nmodes = (int64_t)S.nx * S.ny * S.lzh;
+    const int64_t ncells = (int64_t)S.nx * S.ny * S.nz;
+    const float pre = (float)(1.0 / (double)ncells);
+    const double* kkx = tabs.kk + S.ltab;
+    const double* kky = kkx + S.nx;
+    const double* kkz = kky + S.ny;
+    const float* gx = tabs.grad + S.ltab;
+    const float* gy = gx + S.nx;
+    const float* gz = gy + S.ny;
+    const int nout = mode == 0 ? 9 : 3;
+    float2* o = out + (int64_t)nout * S.ls_off;
+    const int64_t base = (ch - S.ch_ls) * kChunk + threadIdx.x;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t local = base + it * kThreads;
+      if (local >= nmodes) break;
+      int i, j, l;
+      mode_ijl(local, S.ny, S.lzh, i, j, l);
+      const double kk = kkx[i] + kky[j] + kkz[l];
+      // laplace_kernel is 1 at k = 0 in the reference (flowpm/kernels.py:
+      // 42-48); every LPT weight also carries a gradient, which is 0 there.
+      const float lap = kk == 0.0 ? 1.f : (float)(1.0 / kk);
+      float2 dv = dk[S.ls_off + local];
+      dv.x = __fmul_rn(dv.x, pre);
+      dv.y = __fmul_rn(dv.y, pre);
+      const float g[3] = {gx[i], gy[j], gz[l]};
+      // psi_d: kweight = (i g_d) * lap = (0, g*lap); delta * kweight.
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float gl = __fmul_rn(g[d], lap);
+        o[d * nmodes + local] =
+            make_float2(-__fmul_rn(dv.y, gl), __fmul_rn(dv.x, gl));
+      }
+      if (mode == 0) {
+        // phi_ij: kweight = lap * (i g_i) * (i g_j) = -(lap g_i) g_j.
+        const int pi_[6] = {0, 1, 2, 1, 2, 0};
+        const int pj_[6] = {0, 1, 2, 2, 0, 1};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const float w = -__fmul_rn(__fmul_rn(lap, g[pi_[q]]), g[pj_[q]]);
+          o[(3 + q) * nmodes + local] =
+              make_float2(__fmul_rn(dv.x, w), __fmul_rn(dv.y, w));
+        }
+      }
+    }
+  }
+}
+
+// source = 3/7 * [phi_1 phi_2 + phi_2 phi_0 + phi_0 phi_1
+//                 - phi_12^2 - phi_20^2 - phi_01^2]  (flowpm/tfpm.py:128-144)
+__global__ void __launch_bounds__(kThreads)
+k_lpt2_source(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+              const float* __restrict__ phi9, float* __restrict__ source) {
+  const float c37 = (float)(3.0 / 7.0);
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const SimDev S = sims[find_sim(sims, nsims, ch, kLat)];
+    const int64_t ncells = (int64_t)S.nx * S.ny * S.nz;
+    const float* ph = phi9 + 9 * S.l_off;
+    const int64_t base = (ch - S.ch_l) * kChunk + threadIdx.x;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t c = base + it * kThreads;
+      if (c >= ncells) break;
+      const float p0 = ph[3 * ncells + c], p1 = ph[4 * ncells + c],
+                  p2 = ph[5 * ncells + c];
+      const float q12 = ph[6 * ncells + c], q20 = ph[7 * ncells + c],
+                  q01 = ph[8 * ncells + c];
+      float s = __fmul_rn(p1, p2);
+      s = __fadd_rn(s, __fmul_rn(p2, p0));
+      s = __fadd_rn(s, __fmul_rn(p0, p1));
+      s = __fsub_rn(s, __fmul_rn(q12, q12));
+      s = __fsub_rn(s, __fmul_rn(q20, q20));
+      s = __fsub_rn(s, __fmul_rn(q01, q01));
+      source[S.l_off + c] = __fmul_rn(s, c37);
+    }
+  }
+}
+
+// flowpm/tfpm.py:166-179: DX = D1 psi1 (+ D2 psi2), P and F likewise.  The
+// readout at the lattice points returns the mesh value at the particle's own
+// cell (weights 1, 0, ..., 0), so psi is read directly.
+__global__ void __launch_bounds__(kThreads)
+k_lpt_particles(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+                const float* __restrict__ psi1, int m1,
+                const float* __restrict__ psi2, int m2,
+                const float* __restrict__ coef, float* __restrict__ disp,
+                float* __restrict__ mom, float* __restrict__ force) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kPart);
+    const SimDev S = sims[s];
+    const int64_t ncells = (int64_t)S.nx * S.ny * S.nz;
+    const float* c = coef + 6 * s;
+    const float* p1 = psi1 + (int64_t)m1 * S.l_off;
+    const float* p2 = psi2 ? psi2 + (int64_t)m2 * S.l_off : nullptr;
+    const int64_t base = (ch - S.ch_p) * kChunk + threadIdx.x;
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t local = base + it * kThreads;
+      if (local >= S.np) break;
+      const int64_t g = S.p_off + local;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float dx1 = __fmul_rn(c[0], p1[d * ncells + local]);
+        float dx = dx1;
+        float pp = __fmul_rn(c[2], dx1);
+        float ff = __fmul_rn(c[4], dx1);
+        if (p2) {
+          const float dx2 = __fmul_rn(c[1], p2[d * ncells + local]);
+          dx = __fadd_rn(dx1, dx2);
+          pp = __fadd_rn(pp, __fmul_rn(c[3], dx2));
+          ff = __fadd_rn(ff, __fmul_rn(c[5], dx2));
+        }
+        disp[3 * g + d] = dx;
+        mom[3 * g + d] = pp;
+        force[3 * g + d] = ff;
+      }
+    }
+  }
+}
+
+// lineark = whitec * amp, whitec = R2C(white) / N^3 (flowpm/tfpm.py:58-61).
+__global__ void __launch_bounds__(kThreads)
+k_linear_mul(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+             float2* __restrict__ wk, const float* __restrict__ amp) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const SimDev S = sims[find_sim(sims, nsims, ch, kLatSpec)];
+    const int64_t nmodes = (int64_t)S.nx * S.ny * S.lzh;
+    const float pre = (float)(1.0 / ((double)S.nx * S.ny * S.nz));
+    const int64_t base = (ch - S.ch_ls) * kChunk + threadIdx.x;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t local = base + it * kThreads;
+      if (local >= nmodes) break;
+      const int64_t o = S.ls_off + local;
+      float2 v = wk[o];
+      const float a = amp[o];
+      v.x = __fmul_rn(__fmul_rn(v.x, pre), a);
+      v.y = __fmul_rn(__fmul_rn(v.y, pre), a);
+      wk[o] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11) + Box-Muller white noise.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+    const uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += W0;
+    k.y += W1;
+  }
+  return c;
+}
+
+// Uniform in (0, 1): (r + 0.5) / 2^32.
+__device__ __forceinline__ double u01(uint32_t r) {
+  return ((double)r + 0.5) * (1.0 / 4294967296.0);
+}
+
+// out[e - off] = stddev * z(e) for global element indices e in [off, off+n);
+// z(4m + q) is lane q of the Box-Muller pairs of Philox block m.
+__global__ void __launch_bounds__(kThreads)
+k_white_noise(float* __restrict__ out, int64_t off, int64_t n, uint2 key,
+              double stddev) {
+  const int64_t g0 = off / 4, g1 = (off + n + 3) / 4;
+  for (int64_t m = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+       m < g1; m += (int64_t)gridDim.x * blockDim.x) {
+    const uint4 r = philox4x32_10(
+        make_uint4((uint32_t)m, (uint32_t)((uint64_t)m >> 32), 0u, 0u), key);
+    const double ra = sqrt(-2.0 * log(u01(r.x)));
+    const double rb = sqrt(-2.0 * log(u01(r.z)));
+    double sa, ca, sb, cb;
+    sincospi(2.0 * u01(r.y), &sa, &ca);
+    sincospi(2.0 * u01(r.w), &sb, &cb);
+    const double z[4] = {ra * ca, ra * sa, rb * cb, rb * sb};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t e = 4 * m + q;
+      if (e >= off && e < off + n) out[e - off] = (float)(stddev * z[q]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Launch wrappers
+// ---------------------------------------------------------------------------
+std::atomic<int64_t> g_launches{0};
+
+void launch_paint_lattice(const SimDev* sims, int nsims, int64_t nchunks,
+                          const float* disp, float* rho, int32_t* status,
+                          cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_paint_lattice<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks,
+                                                          disp, rho, status);
+}
+
+void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
+                          const float2* dk, float2* fk, float* rho_zero,
+                          AxisTabs tabs, double r_split2, int deconv,
+                          cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_fourier_force<<<grid_for(nchunks), kThreads, 0, st>>>(
+      sims, nsims, nchunks, dk, fk, rho_zero, tabs, r_split2, deconv);
+}
+
+void launch_step(const SimDev* sims, int nsims, int64_t nchunks,
+                 const StepArgs& a, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_step<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
+}
+
+void launch_force_readout(const SimDev* sims, int nsims, int64_t nchunks,
+                          const float* disp, const float* fmesh,
+                          const float* ffac, float* force, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_force_readout<<<grid_for(nchunks), kThreads, 0, st>>>(
+      sims, nsims, nchunks, disp, fmesh, ffac, force);
+}
+
+void launch_lpt_fourier(const SimDev* sims, int nsims, int64_t nchunks,
+                        const float2* dk, float2* out, int mode, AxisTabs tabs,
+                        cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_lpt_fourier<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks,
+                                                        dk, out, mode, tabs);
+}
+
+void launch_lpt2_source(const SimDev* sims, int nsims, int64_t nchunks,
+                        const float* phi9, float* source, cudaStream_t st) {
+  k_lpt2_source<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks,
+                                                        phi9, source);
+}
+
+void launch_lpt_particles(const SimDev* sims, int nsims, int64_t nchunks,
+                          const float* psi1, int m1, const float* psi2, int m2,
+                          const float* coef, float* disp, float* mom,
+                          float* force, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_lpt_particles<<<grid_for(nchunks), kThreads, 0, st>>>(
+      sims, nsims, nchunks, psi1, m1, psi2, m2, coef, disp, mom, force);
+}
+
+void launch_linear_mul(const SimDev* sims, int nsims, int64_t nchunks,
+                       float2* wk, const float* amp, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_linear_mul<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks,
+                                                       wk, amp);
+}
+
+void launch_white_noise(float* out, int64_t off, int64_t n, uint64_t seed,
+                        double stddev, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const int64_t groups = (off + n + 3) / 4 - off / 4;
+  int64_t blocks = (groups + kThreads - 1) / kThreads;
+  const int64_t cap = (int64_t)kNumSMs * 32;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  k_white_noise<<<(unsigned)blocks, kThreads, 0, st>>>(
+      out, off, n, make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)), stddev);
+}
+
+}  // namespace fpm
+
+extern "C" int64_t fpm_launch_count(void) {
+  return fpm::g_launches.load(std::memory_order_relaxed);
+}

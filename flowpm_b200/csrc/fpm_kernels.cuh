@@ -1,0 +1,80 @@
+// Launch wrappers of the particle-mesh step kernels (fpm_kernels.cu), used by
+// the plan orchestration in fpm_plan.cu.
+#pragma once
+
+#include "fpm_internal.cuh"
+
+#include <atomic>
+
+namespace fpm {
+
+// Kernels launched by the library since it was loaded (fpm_launch_count).
+extern std::atomic<int64_t> g_launches;
+
+struct StepArgs {
+  float* disp;             // (total_np, 3) displacement from the lattice
+  float* mom;              // (total_np, 3)
+  float* force_out;        // (total_np, 3), written when a sim finishes
+  float* inter;            // (max_steps, 3, total_np, 3) or null
+  const float* fmesh;      // force meshes: sim s, component c at
+                           //   fmesh + 3*m_off + c*mcells
+  float* rho;              // density target of the next paint
+  const float* coefs;      // (nsims, max_steps, 3) {kick_start, drift, kick_end}
+  const float* ffac;       // (nsims) force prefactor (1.5 Omega_m)
+  const int32_t* nsteps;   // (nsims)
+  int32_t* status;         // device status word
+  int64_t total_np;
+  int max_steps;
+  int it;                  // global iteration 0..max_steps
+};
+
+// Paint every particle at (q + disp) * bf into rho (which must be zeroed).
+void launch_paint_lattice(const SimDev* sims, int nsims, int64_t nchunks,
+                          const float* disp, float* rho, int32_t* status,
+                          cudaStream_t st);
+
+// R2C output -> three force spectra (Green's function * gradient, optional
+// CIC deconvolution and Gaussian long-range window); also zeroes rho.
+void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
+                          const float2* dk, float2* fk, float* rho_zero,
+                          AxisTabs tabs, double r_split2, int deconv,
+                          cudaStream_t st);
+
+// Fused readout + kick(end) + kick(start) + drift + paint of one iteration.
+void launch_step(const SimDev* sims, int nsims, int64_t nchunks,
+                 const StepArgs& a, cudaStream_t st);
+
+// Readout of the three force meshes at (q + disp) * bf, times ffac / bf.
+void launch_force_readout(const SimDev* sims, int nsims, int64_t nchunks,
+                          const float* disp, const float* fmesh,
+                          const float* ffac, float* force, cudaStream_t st);
+
+// Lattice spectra for LPT.  mode 0: from delta_L write 9 spectra
+// {psi1_x, psi1_y, psi1_z, phi_00, phi_11, phi_22, phi_12, phi_20, phi_01};
+// mode 1: write the 3 spectra psi_d.  Input is the unnormalised R2C output,
+// scaled by 1 / (nx ny nz).
+void launch_lpt_fourier(const SimDev* sims, int nsims, int64_t nchunks,
+                        const float2* dk, float2* out, int mode, AxisTabs tabs,
+                        cudaStream_t st);
+
+// 2LPT source 3/7 * sum(phi_ii phi_jj - phi_ij^2) on the lattice meshes.
+void launch_lpt2_source(const SimDev* sims, int nsims, int64_t nchunks,
+                        const float* phi9, float* source, cudaStream_t st);
+
+// LPT particle initialisation from the psi meshes (order 1 or 2).
+// psi1 / psi2 of sim s start at psi + m * l_off (m = meshes per sim).
+void launch_lpt_particles(const SimDev* sims, int nsims, int64_t nchunks,
+                          const float* psi1, int m1, const float* psi2, int m2,
+                          const float* coef, float* disp, float* mom,
+                          float* force, cudaStream_t st);
+
+// lineark = R2C(white) / N^3 * amp, in place on the lattice spectra.
+void launch_linear_mul(const SimDev* sims, int nsims, int64_t nchunks,
+                       float2* wk, const float* amp, cudaStream_t st);
+
+// Philox4x32-10 + Box-Muller white noise: out[e - off] = stddev * N(0, 1)
+// for the global element indices e in [off, off + n).
+void launch_white_noise(float* out, int64_t off, int64_t n, uint64_t seed,
+                        double stddev, cudaStream_t st);
+
+}  // namespace fpm

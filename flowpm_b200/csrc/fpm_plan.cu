@@ -1,0 +1,786 @@
+// Plans, cuFFT orchestration and the C ABI of the particle-mesh step.
+//
+// A plan holds a set of simulations advanced together, their device
+// descriptors, the per-axis Fourier tables, the mesh work buffers and the
+// batched cuFFT plans (one set per run of consecutive simulations with equal
+// dimensions).  Everything a call needs is allocated at creation, so the
+// step entry points are stream-ordered launches only and can be captured in
+// a CUDA graph.
+#include <cufft.h>
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <tuple>
+#include <vector>
+
+#include "fpm_kernels.cuh"
+
+using namespace fpm;
+
+namespace {
+
+// Kernels timed by fpm_plan_profile.
+constexpr int kProfKinds = 3;  // 0 step, 1 fourier force, 2 initial paint
+
+struct Run {
+  int first, count;        // simulations [first, first + count)
+  cufftHandle r2c = 0, c2r3 = 0;                   // force mesh
+  cufftHandle lr2c = 0, lc2r9 = 0, lc2r3 = 0, lc2r1 = 0;  // lattice
+};
+
+template <typename T>
+T* dalloc(size_t n, size_t& total, bool& ok) {
+  if (!ok || n == 0) return nullptr;
+  void* p = nullptr;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
+    ok = false;
+    return nullptr;
+  }
+  total += n * sizeof(T);
+  return (T*)p;
+}
+
+}  // namespace
+
+struct fpm_plan {
+  int nsims = 0;
+  unsigned flags = 0;
+  double r_split = 0;
+  std::vector<SimDev> sims;
+  std::vector<Run> runs;
+  SimDev* d_sims = nullptr;
+  int64_t total_np = 0, total_m = 0, total_s = 0, total_l = 0, total_ls = 0;
+  int64_t ch_p = 0, ch_s = 0, ch_m = 0, ch_l = 0, ch_ls = 0;
+  // tables
+  double* d_kk = nullptr;
+  float* d_grad = nullptr;
+  float* d_win = nullptr;
+  // force-mesh buffers
+  float* rho = nullptr;
+  float2* dk = nullptr;
+  float2* fk = nullptr;
+  float* fmesh = nullptr;
+  // lattice buffers (FPM_PLAN_LPT)
+  float* lreal1 = nullptr;
+  float2* lspec1 = nullptr;
+  float2* lspec9 = nullptr;
+  float* lreal9 = nullptr;
+  float* lreal3 = nullptr;
+  // parameters
+  float* d_coefs = nullptr;
+  int coef_cap = 0;     // steps capacity of d_coefs
+  int max_steps = 0;
+  int32_t* d_nsteps = nullptr;
+  float* d_ffac = nullptr;
+  float* d_lcoef = nullptr;
+  int32_t* d_status = nullptr;
+  void* work = nullptr;
+  size_t device_bytes = 0;
+  bool steps_set = false;
+  // optional per-kernel timing (fpm_plan_profile)
+  bool profile = false;
+  std::vector<cudaEvent_t> ev[kProfKinds];
+  size_t ev_used[kProfKinds] = {0, 0, 0};
+};
+
+namespace {
+
+AxisTabs tabs_of(const fpm_plan* p) { return AxisTabs{p->d_kk, p->d_grad, p->d_win}; }
+
+// Record the next timing event of `kind` on st (no-op unless profiling).
+void prof_mark(fpm_plan* p, int kind, cudaStream_t st) {
+  if (!p->profile) return;
+  auto& v = p->ev[kind];
+  if (p->ev_used[kind] == v.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    v.push_back(e);
+  }
+  cudaEventRecord(v[p->ev_used[kind]++], st);
+}
+
+void destroy_handles(fpm_plan* p) {
+  for (auto& r : p->runs) {
+    cufftHandle* hs[] = {&r.r2c, &r.c2r3, &r.lr2c, &r.lc2r9, &r.lc2r3, &r.lc2r1};
+    for (cufftHandle* h : hs)
+      if (*h) {
+        cufftDestroy(*h);
+        *h = 0;
+      }
+  }
+}
+
+void free_all(fpm_plan* p) {
+  destroy_handles(p);
+  for (int k = 0; k < kProfKinds; ++k)
+    for (cudaEvent_t e : p->ev[k]) cudaEventDestroy(e);
+  void* bufs[] = {p->d_sims, p->d_kk,   p->d_grad,  p->d_win,   p->rho,
+                  p->dk,     p->fk,     p->fmesh,   p->lreal1,  p->lspec1,
+                  p->lspec9, p->lreal9, p->lreal3,  p->d_coefs, p->d_nsteps,
+                  p->d_ffac, p->d_lcoef, p->d_status, p->work};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+}
+
+// k = 2 pi fftfreq(i, n) exactly as numpy: (i * (1/n)) * (2 pi), with
+// i -> i - n for i >= (n + 1) / 2 (flowpm/kernels.py:16-17).
+double kfreq(int i, int n) {
+  const int half = (n - 1) / 2 + 1;
+  const double v = 1.0 / (double)n;
+  const double f = (double)(i < half ? i : i - n) * v;
+  return f * (2.0 * M_PI);
+}
+
+void axis_tables(int n, bool order0, std::vector<double>& kk,
+                 std::vector<float>& grad, std::vector<float>& win) {
+  for (int i = 0; i < n; ++i) {
+    const double k = kfreq(i, n);
+    kk.push_back(k * k);
+    double g;
+    if (order0) {
+      g = (i == n / 2) ? 0.0 : k;  // kernels.py:66-70 zeroes entry len//2
+    } else {
+      g = 1 / 6.0 * (8 * std::sin(k) - std::sin(2 * k));  // kernels.py:75
+    }
+    grad.push_back((float)g);
+    const double x = k / (2 * M_PI);
+    const double sc = x == 0.0 ? 1.0 : std::sin(M_PI * x) / (M_PI * x);
+    win.push_back((float)(1.0 / (sc * sc)));
+  }
+}
+
+int make_plan(cufftHandle* h, int nx, int ny, int nz, cufftType type,
+              int batch, size_t* ws) {
+  if (cufftCreate(h) != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  if (cufftSetAutoAllocation(*h, 0) != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  long long n[3] = {nx, ny, nz};
+  size_t w = 0;
+  cufftResult r = cufftMakePlanMany64(*h, 3, n, nullptr, 1, 0, nullptr, 1, 0,
+                                      type, batch, &w);
+  if (r == CUFFT_ALLOC_FAILED) return FPM_ERR_OOM;
+  if (r != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  if (w > *ws) *ws = w;
+  return FPM_OK;
+}
+
+int exec_r2c(cufftHandle h, float* in, float2* out, cudaStream_t st) {
+  if (cufftSetStream(h, st) != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  return cufftExecR2C(h, in, (cufftComplex*)out) == CUFFT_SUCCESS
+             ? FPM_OK
+             : FPM_ERR_CUFFT;
+}
+
+int exec_c2r(cufftHandle h, float2* in, float* out, cudaStream_t st) {
+  if (cufftSetStream(h, st) != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  return cufftExecC2R(h, (cufftComplex*)in, out) == CUFFT_SUCCESS
+             ? FPM_OK
+             : FPM_ERR_CUFFT;
+}
+
+int launch_ok() {
+  return cudaGetLastError() == cudaSuccess ? FPM_OK : FPM_ERR_CUDA;
+}
+
+#define FPM_TRY(x)            \
+  do {                        \
+    int rc_ = (x);            \
+    if (rc_ != FPM_OK) return rc_; \
+  } while (0)
+
+#define FPM_CUDA(x) \
+  do {              \
+    if ((x) != cudaSuccess) return FPM_ERR_CUDA; \
+  } while (0)
+
+// Density of the current positions -> force meshes (paint must be done).
+int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho) {
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_r2c(r.r2c, p->rho + S.m_off, p->dk + S.s_off, st));
+  }
+  prof_mark(p, 1, st);
+  launch_fourier_force(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
+                       zero_rho ? p->rho : nullptr, tabs_of(p),
+                       p->r_split * p->r_split,
+                       (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0, st);
+  prof_mark(p, 1, st);
+  FPM_TRY(launch_ok());
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_c2r(r.c2r3, p->fk + 3 * S.s_off, p->fmesh + 3 * S.m_off, st));
+  }
+  return FPM_OK;
+}
+
+int upload_ffac(fpm_plan* p, const double* force_fac, cudaStream_t st) {
+  std::vector<float> f(p->nsims);
+  for (int s = 0; s < p->nsims; ++s) f[s] = (float)force_fac[s];
+  FPM_CUDA(cudaMemcpyAsync(p->d_ffac, f.data(), sizeof(float) * p->nsims,
+                           cudaMemcpyHostToDevice, st));
+  return FPM_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int fpm_version(void) { return 100; }
+
+extern "C" const char* fpm_error_string(int code) {
+  switch (code) {
+    case FPM_OK: return "ok";
+    case FPM_ERR_ARG: return "invalid argument";
+    case FPM_ERR_ALIGN: return "misaligned pointer";
+    case FPM_ERR_OOM: return "out of device memory";
+    case FPM_ERR_CUDA: return "CUDA runtime error";
+    case FPM_ERR_CUFFT: return "cuFFT error";
+    case FPM_ERR_NONFINITE: return "non-finite particle state";
+    case FPM_ERR_STATE: return "call out of order";
+    case FPM_ERR_UNSUPPORTED: return "unsupported request";
+    default: return "unknown error";
+  }
+}
+
+extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
+                               double r_split, unsigned flags) {
+  if (!out || nsims < 1 || !dims || r_split < 0) return FPM_ERR_ARG;
+  *out = nullptr;
+  fpm_plan* p = new (std::nothrow) fpm_plan();
+  if (!p) return FPM_ERR_OOM;
+  p->nsims = nsims;
+  p->flags = flags;
+  p->r_split = r_split;
+  std::vector<double> kk;
+  std::vector<float> grad, win;
+  const bool order0 = (flags & FPM_PLAN_GRAD_ORDER0) != 0;
+  const int64_t kMaxCells = (int64_t)1 << 31;
+  for (int s = 0; s < nsims; ++s) {
+    SimDev S;
+    std::memset(&S, 0, sizeof(S));
+    S.nx = dims[4 * s];
+    S.ny = dims[4 * s + 1];
+    S.nz = dims[4 * s + 2];
+    S.bf = dims[4 * s + 3];
+    if (S.nx < 2 || S.ny < 2 || S.nz < 2 || S.bf < 1 || S.bf > 8) {
+      delete p;
+      return FPM_ERR_ARG;
+    }
+    S.mx = S.nx * S.bf;
+    S.my = S.ny * S.bf;
+    S.mz = S.nz * S.bf;
+    if ((int64_t)S.mx * S.my * S.mz >= kMaxCells) {
+      delete p;
+      return FPM_ERR_UNSUPPORTED;
+    }
+    S.mzh = S.mz / 2 + 1;
+    S.lzh = S.nz / 2 + 1;
+    S.np = (int64_t)S.nx * S.ny * S.nz;
+    S.p_off = p->total_np;
+    S.m_off = p->total_m;
+    S.s_off = p->total_s;
+    S.l_off = p->total_l;
+    S.ls_off = p->total_ls;
+    const int64_t nm = (int64_t)S.mx * S.my * S.mz;
+    const int64_t ns = (int64_t)S.mx * S.my * S.mzh;
+    const int64_t nls = (int64_t)S.nx * S.ny * S.lzh;
+    S.ch_p = p->ch_p;
+    S.ch_s = p->ch_s;
+    S.ch_m = p->ch_m;
+    S.ch_l = p->ch_l;
+    S.ch_ls = p->ch_ls;
+    p->ch_p += (S.np + kChunk - 1) / kChunk;
+    p->ch_s += (ns + kChunk - 1) / kChunk;
+    p->ch_m += (nm + kChunk - 1) / kChunk;
+    p->ch_l += (S.np + kChunk - 1) / kChunk;
+    p->ch_ls += (nls + kChunk - 1) / kChunk;
+    p->total_np += S.np;
+    p->total_m += nm;
+    p->total_s += ns;
+    p->total_l += S.np;
+    p->total_ls += nls;
+    S.tab = (int)kk.size();
+    axis_tables(S.mx, order0, kk, grad, win);
+    axis_tables(S.my, order0, kk, grad, win);
+    axis_tables(S.mz, order0, kk, grad, win);
+    S.ltab = (int)kk.size();
+    axis_tables(S.nx, order0, kk, grad, win);
+    axis_tables(S.ny, order0, kk, grad, win);
+    axis_tables(S.nz, order0, kk, grad, win);
+    p->sims.push_back(S);
+    if (s > 0 && dims[4 * s] == dims[4 * s - 4] &&
+        dims[4 * s + 1] == dims[4 * s - 3] &&
+        dims[4 * s + 2] == dims[4 * s - 2] &&
+        dims[4 * s + 3] == dims[4 * s - 1]) {
+      p->runs.back().count++;
+    } else {
+      Run r;
+      r.first = s;
+      r.count = 1;
+      p->runs.push_back(r);
+    }
+  }
+
+  int rc = FPM_OK;
+  size_t ws = 0;
+  const bool lpt = (flags & FPM_PLAN_LPT) != 0;
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    if (rc == FPM_OK)
+      rc = make_plan(&r.r2c, S.mx, S.my, S.mz, CUFFT_R2C, r.count, &ws);
+    if (rc == FPM_OK)
+      rc = make_plan(&r.c2r3, S.mx, S.my, S.mz, CUFFT_C2R, 3 * r.count, &ws);
+    if (lpt) {
+      if (rc == FPM_OK)
+        rc = make_plan(&r.lr2c, S.nx, S.ny, S.nz, CUFFT_R2C, r.count, &ws);
+      if (rc == FPM_OK)
+        rc = make_plan(&r.lc2r9, S.nx, S.ny, S.nz, CUFFT_C2R, 9 * r.count, &ws);
+      if (rc == FPM_OK)
+        rc = make_plan(&r.lc2r3, S.nx, S.ny, S.nz, CUFFT_C2R, 3 * r.count, &ws);
+      if (rc == FPM_OK)
+        rc = make_plan(&r.lc2r1, S.nx, S.ny, S.nz, CUFFT_C2R, r.count, &ws);
+    }
+  }
+  if (rc != FPM_OK) {
+    free_all(p);
+    delete p;
+    return rc;
+  }
+
+  bool ok = true;
+  size_t& tot = p->device_bytes;
+  p->d_sims = dalloc<SimDev>(nsims, tot, ok);
+  p->d_kk = dalloc<double>(kk.size(), tot, ok);
+  p->d_grad = dalloc<float>(grad.size(), tot, ok);
+  p->d_win = dalloc<float>(win.size(), tot, ok);
+  p->rho = dalloc<float>(p->total_m, tot, ok);
+  p->dk = dalloc<float2>(p->total_s, tot, ok);
+  p->fk = dalloc<float2>(3 * p->total_s, tot, ok);
+  p->fmesh = dalloc<float>(3 * p->total_m, tot, ok);
+  if (lpt) {
+    p->lreal1 = dalloc<float>(p->total_l, tot, ok);
+    p->lspec1 = dalloc<float2>(p->total_ls, tot, ok);
+    p->lspec9 = dalloc<float2>(9 * p->total_ls, tot, ok);
+    p->lreal9 = dalloc<float>(9 * p->total_l, tot, ok);
+    p->lreal3 = dalloc<float>(3 * p->total_l, tot, ok);
+  }
+  p->d_nsteps = dalloc<int32_t>(nsims, tot, ok);
+  p->d_ffac = dalloc<float>(nsims, tot, ok);
+  p->d_lcoef = dalloc<float>(6 * (size_t)nsims, tot, ok);
+  p->d_status = dalloc<int32_t>(1, tot, ok);
+  if (ws > 0) {
+    if (ok && cudaMalloc(&p->work, ws) != cudaSuccess) ok = false;
+    if (ok) tot += ws;
+  }
+  if (!ok) {
+    cudaGetLastError();
+    free_all(p);
+    delete p;
+    return FPM_ERR_OOM;
+  }
+  for (auto& r : p->runs) {
+    cufftHandle hs[] = {r.r2c, r.c2r3, r.lr2c, r.lc2r9, r.lc2r3, r.lc2r1};
+    for (cufftHandle h : hs)
+      if (h && cufftSetWorkArea(h, p->work) != CUFFT_SUCCESS) rc = FPM_ERR_CUFFT;
+  }
+  if (rc == FPM_OK &&
+      (cudaMemcpy(p->d_sims, p->sims.data(), sizeof(SimDev) * nsims,
+                  cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(p->d_kk, kk.data(), sizeof(double) * kk.size(),
+                  cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(p->d_grad, grad.data(), sizeof(float) * grad.size(),
+                  cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(p->d_win, win.data(), sizeof(float) * win.size(),
+                  cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemset(p->d_status, 0, sizeof(int32_t)) != cudaSuccess))
+    rc = FPM_ERR_CUDA;
+  if (rc != FPM_OK) {
+    free_all(p);
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return FPM_OK;
+}
+
+extern "C" int fpm_plan_destroy(fpm_plan* p) {
+  if (!p) return FPM_ERR_ARG;
+  free_all(p);
+  delete p;
+  return FPM_OK;
+}
+
+extern "C" int fpm_plan_info(const fpm_plan* p, int64_t* total_particles,
+                             int64_t* device_bytes) {
+  if (!p) return FPM_ERR_ARG;
+  if (total_particles) *total_particles = p->total_np;
+  if (device_bytes) *device_bytes = (int64_t)p->device_bytes;
+  return FPM_OK;
+}
+
+extern "C" int fpm_plan_status(fpm_plan* p, int32_t* status, void* stream) {
+  if (!p || !status) return FPM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  int32_t v = 0;
+  FPM_CUDA(cudaMemcpyAsync(&v, p->d_status, sizeof(int32_t),
+                           cudaMemcpyDeviceToHost, st));
+  FPM_CUDA(cudaMemsetAsync(p->d_status, 0, sizeof(int32_t), st));
+  FPM_CUDA(cudaStreamSynchronize(st));
+  *status = v;
+  return FPM_OK;
+}
+
+extern "C" int fpm_force(fpm_plan* p, const float* disp,
+                         const double* force_fac, float* force, void* stream) {
+  if (!p || !disp || !force_fac || !force) return FPM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  FPM_TRY(upload_ffac(p, force_fac, st));
+  FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
+  launch_paint_lattice(p->d_sims, p->nsims, p->ch_p, disp, p->rho,
+                       p->d_status, st);
+  FPM_TRY(launch_ok());
+  FPM_TRY(force_meshes(p, st, false));
+  launch_force_readout(p->d_sims, p->nsims, p->ch_p, disp, p->fmesh,
+                       p->d_ffac, force, st);
+  return launch_ok();
+}
+
+extern "C" int fpm_nbody_set_steps(fpm_plan* p, int max_steps,
+                                   const int32_t* nsteps, const double* coefs,
+                                   const double* force_fac, void* stream) {
+  if (!p || max_steps < 0 || !nsteps || !force_fac ||
+      (max_steps > 0 && !coefs))
+    return FPM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int s = 0; s < p->nsims; ++s)
+    if (nsteps[s] < 0 || nsteps[s] > max_steps) return FPM_ERR_ARG;
+  if (max_steps > p->coef_cap) {
+    if (p->d_coefs) {
+      FPM_CUDA(cudaStreamSynchronize(st));
+      cudaFree(p->d_coefs);
+      p->device_bytes -= sizeof(float) * 3 * (size_t)p->nsims * p->coef_cap;
+      p->d_coefs = nullptr;
+      p->coef_cap = 0;
+    }
+    if (cudaMalloc(&p->d_coefs, sizeof(float) * 3 * (size_t)p->nsims *
+                                    max_steps) != cudaSuccess) {
+      cudaGetLastError();
+      return FPM_ERR_OOM;
+    }
+    p->coef_cap = max_steps;
+    p->device_bytes += sizeof(float) * 3 * (size_t)p->nsims * max_steps;
+  }
+  if (max_steps > 0) {
+    std::vector<float> c(3 * (size_t)p->nsims * max_steps);
+    for (size_t i = 0; i < c.size(); ++i) c[i] = (float)coefs[i];
+    FPM_CUDA(cudaMemcpyAsync(p->d_coefs, c.data(), sizeof(float) * c.size(),
+                             cudaMemcpyHostToDevice, st));
+  }
+  FPM_CUDA(cudaMemcpyAsync(p->d_nsteps, nsteps, sizeof(int32_t) * p->nsims,
+                           cudaMemcpyHostToDevice, st));
+  FPM_TRY(upload_ffac(p, force_fac, st));
+  // The uploads read pageable host vectors that die with this call.
+  FPM_CUDA(cudaStreamSynchronize(st));
+  p->max_steps = max_steps;
+  p->steps_set = true;
+  return FPM_OK;
+}
+
+extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
+                             float* force, float* inter, unsigned flags,
+                             void* stream) {
+  if (!p || !disp || !mom || !force) return FPM_ERR_ARG;
+  if (!p->steps_set) return FPM_ERR_STATE;
+  if ((flags & FPM_NBODY_INTERMEDIATE) && !inter) return FPM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  StepArgs a;
+  a.disp = disp;
+  a.mom = mom;
+  a.force_out = force;
+  a.inter = (flags & FPM_NBODY_INTERMEDIATE) ? inter : nullptr;
+  a.fmesh = p->fmesh;
+  a.rho = p->rho;
+  a.coefs = p->d_coefs;
+  a.ffac = p->d_ffac;
+  a.nsteps = p->d_nsteps;
+  a.status = p->d_status;
+  a.total_np = p->total_np;
+  a.max_steps = p->max_steps;
+  FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
+  prof_mark(p, 2, st);
+  launch_paint_lattice(p->d_sims, p->nsims, p->ch_p, disp, p->rho,
+                       p->d_status, st);
+  prof_mark(p, 2, st);
+  FPM_TRY(launch_ok());
+  for (int it = 0; it <= p->max_steps; ++it) {
+    FPM_TRY(force_meshes(p, st, it < p->max_steps));
+    a.it = it;
+    prof_mark(p, 0, st);
+    launch_step(p->d_sims, p->nsims, p->ch_p, a, st);
+    prof_mark(p, 0, st);
+    FPM_TRY(launch_ok());
+  }
+  return FPM_OK;
+}
+
+extern "C" int fpm_nbody(fpm_plan* p, float* disp, float* mom, float* force,
+                         int max_steps, const int32_t* nsteps,
+                         const double* coefs, const double* force_fac,
+                         float* inter, unsigned flags, void* stream) {
+  FPM_TRY(fpm_nbody_set_steps(p, max_steps, nsteps, coefs, force_fac, stream));
+  return fpm_nbody_run(p, disp, mom, force, inter, flags, stream);
+}
+
+extern "C" int fpm_lpt_init(fpm_plan* p, const float* linear,
+                            const double* coef, int order, float* disp,
+                            float* mom, float* force, void* stream) {
+  if (!p || !linear || !coef || !disp || !mom || !force ||
+      (order != 1 && order != 2))
+    return FPM_ERR_ARG;
+  if (!(p->flags & FPM_PLAN_LPT)) return FPM_ERR_STATE;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<float> c(6 * (size_t)p->nsims);
+  for (size_t i = 0; i < c.size(); ++i) c[i] = (float)coef[i];
+  FPM_CUDA(cudaMemcpyAsync(p->d_lcoef, c.data(), sizeof(float) * c.size(),
+                           cudaMemcpyHostToDevice, st));
+  // cuFFT R2C may use its input as scratch for some sizes: transform a copy.
+  FPM_CUDA(cudaMemcpyAsync(p->lreal1, linear, sizeof(float) * p->total_l,
+                           cudaMemcpyDeviceToDevice, st));
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_r2c(r.lr2c, p->lreal1 + S.l_off, p->lspec1 + S.ls_off, st));
+  }
+  launch_lpt_fourier(p->d_sims, p->nsims, p->ch_ls, p->lspec1, p->lspec9, 0,
+                     tabs_of(p), st);
+  FPM_TRY(launch_ok());
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_c2r(r.lc2r9, p->lspec9 + 9 * S.ls_off,
+                     p->lreal9 + 9 * S.l_off, st));
+  }
+  const float* psi2 = nullptr;
+  if (order == 2) {
+    launch_lpt2_source(p->d_sims, p->nsims, p->ch_l, p->lreal9, p->lreal1, st);
+    FPM_TRY(launch_ok());
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      FPM_TRY(exec_r2c(r.lr2c, p->lreal1 + S.l_off, p->lspec1 + S.ls_off, st));
+    }
+    launch_lpt_fourier(p->d_sims, p->nsims, p->ch_ls, p->lspec1, p->lspec9, 1,
+                       tabs_of(p), st);
+    FPM_TRY(launch_ok());
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      FPM_TRY(exec_c2r(r.lc2r3, p->lspec9 + 3 * S.ls_off,
+                       p->lreal3 + 3 * S.l_off, st));
+    }
+    psi2 = p->lreal3;
+  }
+  launch_lpt_particles(p->d_sims, p->nsims, p->ch_p, p->lreal9, 9, psi2, 3,
+                       p->d_lcoef, disp, mom, force, st);
+  FPM_TRY(launch_ok());
+  // The coefficient upload reads a host vector that dies with this call.
+  FPM_CUDA(cudaStreamSynchronize(st));
+  return FPM_OK;
+}
+
+extern "C" int fpm_linear_field(fpm_plan* p, const float* amp, uint64_t seed,
+                                int generate, float* white, float* linear,
+                                void* stream) {
+  if (!p || !amp || !linear || (!generate && !white)) return FPM_ERR_ARG;
+  if (!(p->flags & FPM_PLAN_LPT)) return FPM_ERR_STATE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (generate) {
+    float* w = white ? white : p->lreal1;
+    for (int s = 0; s < p->nsims; ++s) {
+      const SimDev& S = p->sims[s];
+      launch_white_noise(w + S.l_off, S.l_off, S.np, seed,
+                         std::sqrt((double)S.np), st);
+    }
+    FPM_TRY(launch_ok());
+    if (w != p->lreal1)
+      FPM_CUDA(cudaMemcpyAsync(p->lreal1, w, sizeof(float) * p->total_l,
+                               cudaMemcpyDeviceToDevice, st));
+  } else {
+    FPM_CUDA(cudaMemcpyAsync(p->lreal1, white, sizeof(float) * p->total_l,
+                             cudaMemcpyDeviceToDevice, st));
+  }
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_r2c(r.lr2c, p->lreal1 + S.l_off, p->lspec1 + S.ls_off, st));
+  }
+  launch_linear_mul(p->d_sims, p->nsims, p->ch_ls, p->lspec1, amp, st);
+  FPM_TRY(launch_ok());
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_c2r(r.lc2r1, p->lspec1 + S.ls_off, linear + S.l_off, st));
+  }
+  return FPM_OK;
+}
+
+extern "C" int fpm_white_noise(float* out, int64_t n, uint64_t seed,
+                               double stddev, void* stream) {
+  if (n < 0 || (n > 0 && !out)) return FPM_ERR_ARG;
+  if (n == 0) return FPM_OK;
+  launch_white_noise(out, 0, n, seed, stddev, (cudaStream_t)stream);
+  return launch_ok();
+}
+
+extern "C" int fpm_plan_profile(fpm_plan* p, int enable) {
+  if (!p) return FPM_ERR_ARG;
+  p->profile = enable != 0;
+  for (int k = 0; k < kProfKinds; ++k) p->ev_used[k] = 0;
+  return FPM_OK;
+}
+
+extern "C" int fpm_plan_profile_read(fpm_plan* p, int kind, double* total_ms,
+                                     int64_t* launches) {
+  if (!p || kind < 0 || kind >= kProfKinds || !total_ms || !launches)
+    return FPM_ERR_ARG;
+  double t = 0;
+  const size_t n = p->ev_used[kind] / 2;
+  for (size_t i = 0; i < n; ++i) {
+    float ms = 0;
+    if (cudaEventSynchronize(p->ev[kind][2 * i + 1]) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, p->ev[kind][2 * i],
+                             p->ev[kind][2 * i + 1]) != cudaSuccess)
+      return FPM_ERR_CUDA;
+    t += ms;
+  }
+  *total_ms = t;
+  *launches = (int64_t)n;
+  p->ev_used[kind] = 0;
+  return FPM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Full-spectrum normalised FFTs (flowpm/utils.py:213 r2c3d, :244 c2r3d).
+// ---------------------------------------------------------------------------
+namespace {
+
+std::mutex g_fft_mu;
+std::map<std::tuple<int, int, int, int, int, int>, cufftHandle> g_fft_plans;
+
+int c2c_plan(int batch, int nx, int ny, int nz, int dbl, cufftHandle* h) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return FPM_ERR_CUDA;
+  auto key = std::make_tuple(dev, batch, nx, ny, nz, dbl);
+  std::lock_guard<std::mutex> lk(g_fft_mu);
+  auto it = g_fft_plans.find(key);
+  if (it != g_fft_plans.end()) {
+    *h = it->second;
+    return FPM_OK;
+  }
+  int n[3] = {nx, ny, nz};
+  cufftHandle hh;
+  if (cufftPlanMany(&hh, 3, n, nullptr, 1, 0, nullptr, 1, 0,
+                    dbl ? CUFFT_Z2Z : CUFFT_C2C, batch) != CUFFT_SUCCESS)
+    return FPM_ERR_CUFFT;
+  g_fft_plans[key] = hh;
+  *h = hh;
+  return FPM_OK;
+}
+
+template <typename R, typename C>
+__global__ void k_real_to_complex(const R* in, C* out, int64_t n, R scale) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    C v;
+    v.x = in[i] * scale;
+    v.y = 0;
+    out[i] = v;
+  }
+}
+
+template <typename C, typename R>
+__global__ void k_scale_complex(C* data, int64_t n, R scale) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    C v = data[i];
+    v.x *= scale;
+    v.y *= scale;
+    data[i] = v;
+  }
+}
+
+template <typename C, typename R>
+__global__ void k_complex_real(const C* in, R* out, int64_t n, R scale) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[i].x * scale;
+}
+
+unsigned grid_n(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  if (b > (int64_t)kNumSMs * 32) b = (int64_t)kNumSMs * 32;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+extern "C" int fpm_r2c3d(const void* rfield, void* cfield, int batch, int nx,
+                         int ny, int nz, double scale, int double_precision,
+                         void* stream) {
+  if (!rfield || !cfield || batch < 1 || nx < 1 || ny < 1 || nz < 1)
+    return FPM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t n = (int64_t)batch * nx * ny * nz;
+  cufftHandle h;
+  FPM_TRY(c2c_plan(batch, nx, ny, nz, double_precision, &h));
+  if (cufftSetStream(h, st) != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  if (double_precision) {
+    k_real_to_complex<<<grid_n(n), 256, 0, st>>>(
+        (const double*)rfield, (double2*)cfield, n, 1.0);
+    if (cufftExecZ2Z(h, (cufftDoubleComplex*)cfield,
+                     (cufftDoubleComplex*)cfield,
+                     CUFFT_FORWARD) != CUFFT_SUCCESS)
+      return FPM_ERR_CUFFT;
+    k_scale_complex<<<grid_n(n), 256, 0, st>>>((double2*)cfield, n, scale);
+  } else {
+    k_real_to_complex<<<grid_n(n), 256, 0, st>>>(
+        (const float*)rfield, (float2*)cfield, n, 1.0f);
+    if (cufftExecC2C(h, (cufftComplex*)cfield, (cufftComplex*)cfield,
+                     CUFFT_FORWARD) != CUFFT_SUCCESS)
+      return FPM_ERR_CUFFT;
+    k_scale_complex<<<grid_n(n), 256, 0, st>>>((float2*)cfield, n,
+                                                (float)scale);
+  }
+  return launch_ok();
+}
+
+extern "C" int fpm_c2r3d(const void* cfield, void* rfield, int batch, int nx,
+                         int ny, int nz, double scale, int double_precision,
+                         void* stream) {
+  if (!rfield || !cfield || batch < 1 || nx < 1 || ny < 1 || nz < 1)
+    return FPM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t n = (int64_t)batch * nx * ny * nz;
+  cufftHandle h;
+  FPM_TRY(c2c_plan(batch, nx, ny, nz, double_precision, &h));
+  if (cufftSetStream(h, st) != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  const size_t bytes = (size_t)n * (double_precision ? 16 : 8);
+  void* tmp = nullptr;
+  FPM_CUDA(cudaMallocAsync(&tmp, bytes, st));
+  int rc = FPM_OK;
+  if (double_precision) {
+    if (cufftExecZ2Z(h, (cufftDoubleComplex*)cfield, (cufftDoubleComplex*)tmp,
+                     CUFFT_INVERSE) != CUFFT_SUCCESS)
+      rc = FPM_ERR_CUFFT;
+    else
+      k_complex_real<<<grid_n(n), 256, 0, st>>>((const double2*)tmp,
+                                                 (double*)rfield, n, scale);
+  } else {
+    if (cufftExecC2C(h, (cufftComplex*)cfield, (cufftComplex*)tmp,
+                     CUFFT_INVERSE) != CUFFT_SUCCESS)
+      rc = FPM_ERR_CUFFT;
+    else
+      k_complex_real<<<grid_n(n), 256, 0, st>>>(
+          (const float2*)tmp, (float*)rfield, n, (float)scale);
+  }
+  cudaFreeAsync(tmp, st);
+  if (rc != FPM_OK) return rc;
+  return launch_ok();
+}

@@ -1,0 +1,214 @@
+/*
+ * flowpm_b200 -- C ABI of the B200 particle-mesh library (libflowpm_b200.so).
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (passed as void*), is stream-ordered, performs no host synchronisation
+ * unless stated, and returns FPM_OK (0) or one of the FPM_ERR_* codes; it
+ * never exits, aborts or traps.  The caller owns every buffer it passes; the
+ * library owns only what fpm_plan_create allocates (cuFFT plans, the mesh
+ * work buffers and a device status word), released by fpm_plan_destroy.
+ *
+ * Conventions (those of the reference, flowpm/utils.py and flowpm/tfpm.py):
+ *   meshes            float32, (batch, nx, ny, nz), z fastest;
+ *   particle arrays   float32, (batch, npart, 3) in mesh units;
+ *   nbody state       kept as displacement d from the Lagrangian lattice
+ *                     q = (i, j, k) of particle index (i*ny + j)*nz + k
+ *                     (absolute position X = q + d), momentum p, force f,
+ *                     each (total_particles, 3).
+ */
+#ifndef FLOWPM_B200_H
+#define FLOWPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  FPM_OK = 0,
+  FPM_ERR_ARG = 1,        /* bad shape, size or null pointer            */
+  FPM_ERR_ALIGN = 2,      /* pointer not aligned as required            */
+  FPM_ERR_OOM = 3,        /* device allocation failed                   */
+  FPM_ERR_CUDA = 4,       /* a CUDA runtime call failed                 */
+  FPM_ERR_CUFFT = 5,      /* a cuFFT call failed                        */
+  FPM_ERR_NONFINITE = 6,  /* device status: non-finite particle state   */
+  FPM_ERR_STATE = 7,      /* call out of order (e.g. missing workspace) */
+  FPM_ERR_UNSUPPORTED = 8 /* valid request this build does not handle   */
+};
+
+/* Device status bits accumulated by the kernels of a plan. */
+enum {
+  FPM_STATUS_NONFINITE_POS = 1, /* a particle position was NaN or inf */
+  FPM_STATUS_NONFINITE_MOM = 2  /* a momentum or force was NaN or inf */
+};
+
+/* Plan option flags (fpm_plan_create). */
+enum {
+  FPM_PLAN_CIC_DECONV = 1u << 0, /* divide the force by the CIC window
+                                    prod_d sinc^2(k_d / 2pi)
+                                    (flowpm/kernels.py:137 cic_compensation);
+                                    off in the reference force              */
+  FPM_PLAN_LPT = 1u << 1,        /* also allocate the LPT / linear-field
+                                    buffers on the particle lattice         */
+  FPM_PLAN_GRAD_ORDER0 = 1u << 2 /* gradient i*k (order 0) instead of the
+                                    4-point finite difference (order 1)   */
+};
+
+/* nbody flags (fpm_nbody). */
+enum {
+  FPM_NBODY_INTERMEDIATE = 1u << 0 /* write the state after every step */
+};
+
+typedef struct fpm_plan fpm_plan;
+
+/* Library version (major*10000 + minor*100 + patch) and error text. */
+int fpm_version(void);
+const char* fpm_error_string(int code);
+
+/* Number of CUDA kernels this library has launched since it was loaded
+ * (its own kernels; cuFFT's are not counted). */
+int64_t fpm_launch_count(void);
+
+/* ---------------------------------------------------------------------
+ * Stand-alone CIC operators.
+ * ------------------------------------------------------------------ */
+
+/* mesh[b] += CIC deposit of part[b] with weights weight[b] (or 1 when
+ * weight is NULL).  Replaces flowpm/utils.py:32-91 cic_paint
+ * (tf.scatter_nd over 8 neighbours, mod-N periodic wrap). */
+int fpm_cic_paint(float* mesh, int batch, int nx, int ny, int nz,
+                  const float* part, int64_t npart, const float* weight,
+                  void* stream);
+
+/* out[b, p] = sum over the 8 CIC neighbours of mesh[b] * weight.
+ * Replaces flowpm/utils.py:163-210 cic_readout (tf.gather_nd). */
+int fpm_cic_readout(const float* mesh, int batch, int nx, int ny, int nz,
+                    const float* part, int64_t npart, float* out,
+                    void* stream);
+
+/* Neighbour cells and weights of each particle, in the reference's
+ * neighbour order (flowpm/utils.py:66-67): idx[p*8 + c] is the flat cell
+ * (ix*ny + iy)*nz + iz, w[p*8 + c] the CIC weight.  Exposed so that cell
+ * indices and neighbour sets can be compared bit for bit. */
+int fpm_cic_neighbours(int nx, int ny, int nz, const float* part,
+                       int64_t npart, int32_t* idx, float* w, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Full-spectrum FFTs behind flowpm/utils.py:213 r2c3d and :244 c2r3d:
+ *   fpm_r2c3d: out = FFT3(complex(in)) * scale            (r2c3d: 1/norm)
+ *   fpm_c2r3d: out = Re(sum_k in_k e^{+ikx}) * scale      (c2r3d: norm/N^3)
+ * over the three innermost axes of (batch, nx, ny, nz) arrays.
+ * double_precision selects float64 / complex128 buffers.  Plans are cached
+ * inside the library per device and shape (created on first use);
+ * fpm_c2r3d takes a temporary buffer from the stream-ordered allocator.
+ * ------------------------------------------------------------------ */
+int fpm_r2c3d(const void* rfield, void* cfield, int batch, int nx, int ny,
+              int nz, double scale, int double_precision, void* stream);
+int fpm_c2r3d(const void* cfield, void* rfield, int batch, int nx, int ny,
+              int nz, double scale, int double_precision, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Plans: one set of simulations advanced together.  dims holds, for each
+ * simulation, {nx, ny, nz, pm_nc_factor}: the particle lattice (= the
+ * linear-field mesh, flowpm/tfpm.py:148) and the force-mesh factor
+ * (flowpm/tfpm.py:317 pm_nc_factor).  Consecutive simulations with equal
+ * dims share batched cuFFT plans.  Particle arrays of the plan are the
+ * simulations' arrays concatenated in order.
+ * ------------------------------------------------------------------ */
+int fpm_plan_create(fpm_plan** plan, int nsims, const int32_t* dims,
+                    double r_split, unsigned flags);
+int fpm_plan_destroy(fpm_plan* plan);
+/* Total particles of the plan and bytes of device memory it holds. */
+int fpm_plan_info(const fpm_plan* plan, int64_t* total_particles,
+                  int64_t* device_bytes);
+/* Copy the device status word to *status and clear it (synchronises the
+ * stream). */
+int fpm_plan_status(fpm_plan* plan, int32_t* status, void* stream);
+
+/* Per-kernel timing: while enabled, fpm_nbody_run records a CUDA event
+ * pair around every launch of the fused step kernel (kind 0), the Fourier
+ * force kernel (kind 1) and the initial paint (kind 2) on the call's
+ * stream.  fpm_plan_profile_read waits for the last event, returns the
+ * summed device time and the number of timed launches of `kind`, and
+ * resets that kind.  Not for use under CUDA graph capture. */
+int fpm_plan_profile(fpm_plan* plan, int enable);
+int fpm_plan_profile_read(fpm_plan* plan, int kind, double* total_ms,
+                          int64_t* launches);
+
+/* Force on every particle at positions q + disp:
+ * flowpm/tfpm.py:317-366 force() = paint at X*B, /nbar, r2c, Green's
+ * function * 4-point gradient * force_fac[s] (1.5 Omega_m in the
+ * reference), c2r, readout at X*B, /B.  force has the layout of disp. */
+int fpm_force(fpm_plan* plan, const float* disp, const double* force_fac,
+              float* force, void* stream);
+
+/* KDK leapfrog of flowpm/tfpm.py:425-503 for every simulation of the
+ * plan.  coefs holds, per simulation s and step i < nsteps[s], the three
+ * FP64 prefactors {kick_start, drift, kick_end} at
+ * coefs[(s*max_steps + i)*3 + 0..2]:
+ *   kick_start_i = kick(a_i, a_i, ah_i), drift_i = drift(a_i, ah_i, a_i+1),
+ *   kick_end_i   = kick(ah_i, a_i+1, a_i+1)   (flowpm/tfpm.py:273-314).
+ * disp and mom are updated in place; force receives the force at the
+ * final positions.  With FPM_NBODY_INTERMEDIATE, inter (max_steps x 3 x
+ * total_particles x 3 floats) receives (X = q + d, p, f) after each step. */
+int fpm_nbody(fpm_plan* plan, float* disp, float* mom, float* force,
+              int max_steps, const int32_t* nsteps, const double* coefs,
+              const double* force_fac, float* inter, unsigned flags,
+              void* stream);
+
+/* fpm_nbody in two parts: fpm_nbody_set_steps uploads the step tables
+ * (host arrays; synchronises the stream once), fpm_nbody_run launches the
+ * whole leapfrog with kernels and cuFFT executions only, so that it can be
+ * captured into a CUDA graph and replayed. */
+int fpm_nbody_set_steps(fpm_plan* plan, int max_steps, const int32_t* nsteps,
+                        const double* coefs, const double* force_fac,
+                        void* stream);
+int fpm_nbody_run(fpm_plan* plan, float* disp, float* mom, float* force,
+                  float* inter, unsigned flags, void* stream);
+
+/* 2LPT initial conditions, flowpm/tfpm.py:148-180 lpt_init: from the real
+ * linear field (the plan's lattice meshes concatenated) compute the 1LPT
+ * and 2LPT displacements at the lattice points and
+ *   d = D1 psi1 + D2 psi2, p = c[2] D1 psi1 + c[3] D2 psi2,
+ *   f = c[4] D1 psi1 + c[5] D2 psi2
+ * with coef[s*6 + 0..5] = {D1, D2, a^2 f1 E, a^2 f2 E, a^2 E gf / D1,
+ * a^2 E gf2 / D2}.  order 1 skips the 2LPT term.  Needs FPM_PLAN_LPT. */
+int fpm_lpt_init(fpm_plan* plan, const float* linear, const double* coef,
+                 int order, float* disp, float* mom, float* force,
+                 void* stream);
+
+/* Gaussian white noise N(0, sqrt(N^3)) per cell on every simulation's
+ * lattice (Philox4x32-10 counter RNG + Box-Muller), then
+ * linear = c2r(r2c(white) * amp), flowpm/tfpm.py:15-63 linear_field.
+ * amp is the half-spectrum amplitude sqrt(P(|k|) / V) per simulation
+ * (lattice half spectra concatenated, nx*ny*(nz/2+1) each).  white may be
+ * NULL; when it is not NULL and generate == 0 it is read instead of
+ * generated.  Needs FPM_PLAN_LPT. */
+int fpm_linear_field(fpm_plan* plan, const float* amp, uint64_t seed,
+                     int generate, float* white, float* linear,
+                     void* stream);
+
+/* out = in + sign * q for every particle of a uniform batch of lattices
+ * (batch, nx*ny*nz, 3): sign -1 turns absolute positions X into lattice
+ * displacements, +1 turns displacements back into X = q + d (the
+ * reference's X = DX + Q, flowpm/tfpm.py:179).  in may equal out. */
+int fpm_lattice_shift(const float* in, float* out, int batch, int nx, int ny,
+                      int nz, int sign, void* stream);
+
+/* y = y + a * x with the two roundings of the reference's kick and drift
+ * updates (update = fac * F; state = state + update, flowpm/tfpm.py:287-292,
+ * :309-314). */
+int fpm_saxpy(float* y, const float* x, float a, int64_t n, void* stream);
+
+/* Gaussian white noise alone: out[e] = stddev * N(0,1) for e < n with the
+ * generator of fpm_linear_field (counter = element index). */
+int fpm_white_noise(float* out, int64_t n, uint64_t seed, double stddev,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLOWPM_B200_H */

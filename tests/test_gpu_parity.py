@@ -1,0 +1,288 @@
+"""Parity of the CUDA path (through the C ABI) with the reference: golden
+fixtures from the reference's own source and the CPU oracle on the same
+inputs.  Bars: cell indices / neighbour sets bit-exact; CIC values at
+FP32 rounding; final density rel-L2 <= 1e-4; P(k) per bin <= 1e-4; the
+error against the FP64 oracle is printed for every trajectory result."""
+import numpy as np
+import pytest
+import torch
+from numpy.testing import assert_allclose
+
+from conftest import golden, pk_table, rel_l2
+from oracle import background as obg
+from oracle import pm as opm
+from oracle import rng as orng
+
+pytestmark = pytest.mark.gpu
+ALT = dict(Omega_c=0.30, Omega_b=0.045, h=0.70, sigma8=0.75, n_s=0.96)
+
+
+@pytest.fixture(scope='module')
+def fpm(cuda):
+  import flowpm_b200
+  return flowpm_b200
+
+
+def host(t):
+  return t.detach().cpu().numpy()
+
+
+# --------------------------------------------------------------------------
+# CIC operators
+# --------------------------------------------------------------------------
+def test_cic_paint_readout_golden(fpm):
+  z = golden('cic')
+  m = fpm.cic_paint(np.zeros((2, 16, 16, 16), np.float32), z['pos'],
+                    z['wts'])
+  assert_allclose(host(m), z['paint_w'], atol=1e-6)
+  m = fpm.cic_paint(np.zeros((2, 16, 16, 16), np.float32), z['pos'])
+  assert_allclose(host(m), z['paint_1'], atol=1e-6)
+  r = fpm.cic_readout(z['base'], z['pos'])
+  assert_allclose(host(r), z['readout'], rtol=1e-6)
+  m = fpm.cic_paint(np.zeros((1, 8, 6, 10), np.float32), z['pos_rect'])
+  assert_allclose(host(m), z['paint_rect'], atol=1e-6)
+  r = fpm.cic_readout(z['base_rect'], z['pos_rect'])
+  assert_allclose(host(r), z['readout_rect'], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize('nc', [[16, 16, 16], [8, 6, 10], [128, 128, 128]])
+def test_cic_neighbours_bit_exact(fpm, nc):
+  rng = np.random.default_rng(7)
+  n = 20000
+  pos = (rng.random((n, 3)) * 3 - 1) * np.array(nc)
+  # faces, integer points, the wrap at N - eps, huge and negative values
+  pos[:6] = [[0, 0, 0], [nc[0] - 1e-5, 0.5, 1.0], [-1e-7, 3.0, 2.0],
+             [nc[0], nc[1], nc[2]], [-nc[0] * 7.25, 1e4, -3e3],
+             [0.999999, 1.0000001, 2.5]]
+  pos = pos.astype(np.float32)
+  idx, w = fpm.utils.cic_neighbours(pos, nc)
+  t = torch.tensor(pos).reshape(1, -1, 3)
+  ref = opm._neighbours(t, nc)
+  ref_idx = np.stack([f.numpy()[0] for _, f in ref], axis=1)
+  ref_w = np.stack([k.numpy()[0] for k, _ in ref], axis=1)
+  assert np.array_equal(host(idx).astype(np.int64), ref_idx)
+  assert np.array_equal(host(w), ref_w)
+
+
+def test_cic_empty_and_batched(fpm):
+  mesh = torch.full((3, 8, 8, 8), 2.0, device='cuda')
+  out = fpm.cic_paint(mesh, torch.zeros((3, 0, 3), device='cuda'))
+  assert torch.equal(out, mesh)
+  r = fpm.cic_readout(mesh, torch.zeros((3, 0, 3), device='cuda'))
+  assert r.shape == (3, 0)
+
+
+def test_cic_large_properties(fpm):
+  """128^3 mesh, 2 x 2^21 particles: mass conservation, readout of a
+  constant and of a linear ramp, and agreement with the oracle."""
+  g = torch.Generator(device='cpu').manual_seed(3)
+  B, n, N = 2, 1 << 21, 128
+  pos = torch.rand((B, n, 3), generator=g) * N
+  w = torch.rand((B, n), generator=g)
+  m = fpm.cic_paint(torch.zeros((B, N, N, N)), pos, w)
+  assert_allclose(host(m.double().sum(dim=(1, 2, 3))),
+                  w.double().sum(dim=1).numpy(), rtol=1e-6)
+  ref = opm.cic_paint(torch.zeros((B, N, N, N)), pos, w)
+  assert_allclose(host(m), ref.numpy(), atol=2e-5)
+  r = fpm.cic_readout(torch.full((B, N, N, N), 3.5), pos)
+  assert_allclose(host(r), 3.5, rtol=1e-6)
+  ramp = torch.arange(N, dtype=torch.float32).reshape(1, 1, 1, N).expand(
+      B, N, N, N).contiguous()
+  inner = pos.clone()
+  inner[..., 2] = inner[..., 2].clamp(0, N - 1.01)
+  r = fpm.cic_readout(ramp, inner)
+  assert_allclose(host(r), inner[..., 2].numpy(), atol=2e-5)
+
+
+def test_fft_pair(fpm):
+  z = golden('cic')
+  c = fpm.r2c3d(torch.tensor(z['rt_in']), dtype=torch.complex128)
+  assert_allclose(host(c), z['rt_k'], rtol=1e-9, atol=1e-9)
+  r = fpm.c2r3d(c, dtype=torch.float64)
+  assert_allclose(host(r), z['rt_in'], rtol=1e-9)
+  r32 = fpm.c2r3d(fpm.r2c3d(torch.tensor(z['rt_in'], dtype=torch.float32)))
+  assert_allclose(host(r32), z['rt_in'], rtol=1e-4, atol=1e-3)
+
+
+# --------------------------------------------------------------------------
+# Initial conditions
+# --------------------------------------------------------------------------
+def test_white_noise_generator(fpm):
+  w = fpm.white_noise([8, 8, 10], batch_size=3, seed=12345, type='real')
+  ref = orng.white_noise(3 * 640, 12345, stddev=640**0.5)
+  assert_allclose(host(w).ravel(), ref, rtol=1e-6, atol=1e-6)
+  big = host(fpm.white_noise(64, batch_size=2, seed=1, type='real')).ravel()
+  big /= 64**1.5
+  assert abs(big.mean()) < 5e-3 and abs(big.std() - 1) < 5e-3
+
+
+@pytest.mark.parametrize('nc,bs', [(16, 50.), (32, 100.)])
+def test_linear_field_golden(fpm, nc, bs):
+  z = golden('lpt')
+  lin = fpm.linear_field(nc, bs, pk_table(), white=z['n%d_white' % nc])
+  ref = z['n%d_linear' % nc]
+  assert_allclose(host(lin), ref, atol=1e-5 * np.abs(ref).max())
+
+
+def test_linear_field_seeded(fpm):
+  a = fpm.linear_field(32, 100., pk_table(), batch_size=2, seed=9)
+  b = fpm.linear_field(32, 100., pk_table(), batch_size=2, seed=9)
+  assert torch.equal(a, b)
+  white = orng.white_noise(2 * 32**3, 9, stddev=32**1.5).reshape(
+      2, 32, 32, 32)
+  ref = opm.linear_field_from_white(torch.tensor(white), 100., pk_table())
+  assert_allclose(host(a), ref.numpy(), atol=1e-5 * float(ref.abs().max()))
+
+
+@pytest.mark.parametrize('nc,order', [(16, 1), (16, 2), (32, 2)])
+def test_lpt_init_golden(fpm, nc, order):
+  z = golden('lpt')
+  c = fpm.cosmology.Planck15()
+  s = host(fpm.lpt_init(c, z['n%d_linear' % nc], 0.1, order=order))
+  ref = z['n%d_init_o%d' % (nc, order)]
+  assert_allclose(s, ref, atol=3e-5 * np.abs(ref).max(axis=(1, 2, 3),
+                                                      keepdims=True).max())
+
+
+def test_lpt_init_rectangular_alt_cosmology(fpm):
+  z = golden('nbody')
+  c = fpm.cosmology.Planck15(**ALT)
+  s = host(fpm.lpt_init(c, z['rect_linear'], 0.1, order=2))
+  assert_allclose(s, z['rect_init'], atol=1e-5)
+
+
+# --------------------------------------------------------------------------
+# Force, kick, drift, nbody
+# --------------------------------------------------------------------------
+def test_force_kick_drift_golden(fpm):
+  z, l = golden('nbody'), golden('lpt')
+  c = fpm.cosmology.Planck15()
+  s0 = l['n16_init_o1']
+  f = host(fpm.tfpm.force(c, s0, 16))
+  assert_allclose(f, z['n16_force'], atol=2e-5)
+  assert_allclose(host(fpm.tfpm.kick(c, s0, 0.1, 0.1, 0.12)), z['n16_kick'],
+                  atol=2e-6)
+  assert_allclose(host(fpm.tfpm.drift(c, s0, 0.1, 0.12, 0.15)),
+                  z['n16_drift'], atol=2e-6)
+
+
+def _fp64_oracle_state(state0, stages, nc, cosmo_kw=None, pm_nc_factor=1):
+  b64 = obg.Background(cosmo_kw or {}, dtype=np.float64)
+  s = torch.tensor(state0, dtype=torch.float64)
+  return opm.nbody(b64, s, stages, nc, pm_nc_factor=pm_nc_factor).numpy()
+
+
+def test_nbody_16_golden(fpm, capsys):
+  z, l = golden('nbody'), golden('lpt')
+  c = fpm.cosmology.Planck15()
+  stages = z['stages']
+  st = host(fpm.nbody(c, l['n16_init_o1'], stages, 16))
+  assert_allclose(st, z['n16_b1_final'], atol=1e-4)
+  st2 = host(fpm.nbody(c, l['n16_init_o1'], stages, 16, pm_nc_factor=2))
+  assert_allclose(st2, z['n16_b2_final'], atol=1e-4)
+  inter = fpm.nbody(c, l['n16_init_o1'], stages[:4], 16,
+                    return_intermediate_states=True)
+  assert [a for a, _ in inter] == list(z['n16_inter_a'])
+  assert_allclose(np.stack([host(s) for _, s in inter]), z['n16_inter'],
+                  atol=2e-5)
+  ref64 = _fp64_oracle_state(l['n16_init_o1'], stages, 16)
+  with capsys.disabled():
+    print('\n  nbody 16^3: max |X - X_fp64| = %.2e cells (reference FP32: '
+          '%.2e)' % (np.abs(st[0] - ref64[0]).max(),
+                     np.abs(z['n16_b1_final'][0] - ref64[0]).max()))
+
+
+def test_nbody_rectangular_golden(fpm):
+  z = golden('nbody')
+  c = fpm.cosmology.Planck15(**ALT)
+  s0 = fpm.lpt_init(c, z['rect_linear'], 0.1, order=2)
+  st = host(fpm.nbody(c, s0, z['stages'], [8, 8, 24]))
+  assert_allclose(st, z['rect_final'], atol=1e-4)
+
+
+def _pk(field, bs):
+  kb, p = opm.power_spectrum(torch.tensor(field, dtype=torch.float64),
+                             kmin=0.1, dk=0.05, boxsize=np.array([bs] * 3))
+  return p.numpy()
+
+
+def test_nbody_32_density_and_pk(fpm, capsys):
+  """C1 configuration (32^3, box 100, Planck15, 2LPT at a0=0.1, 10 stages):
+  final density within 1e-4 relative L2 and P(k) within 1e-4 per bin of
+  the reference."""
+  z, l = golden('nbody'), golden('lpt')
+  c = fpm.cosmology.Planck15()
+  stages = z['stages']
+  s0 = fpm.lpt_init(c, l['n32_linear'], 0.1, order=2)
+  st = fpm.nbody(c, s0, stages, 32)
+  rho = host(fpm.cic_paint(torch.zeros((1, 32, 32, 32)), st[0]))
+  err = rel_l2(rho, z['n32_rho'])
+  assert err <= 1e-4, err
+  pk, pk_ref = _pk(rho, 100.), _pk(z['n32_rho'], 100.)
+  pk_err = float(np.max(np.abs(pk - pk_ref) / np.abs(pk_ref)))
+  assert pk_err <= 1e-4, pk_err
+  ref64 = _fp64_oracle_state(l['n32_init_o2'], stages, 32)
+  rho64 = opm.cic_paint(torch.zeros((1, 32, 32, 32), dtype=torch.float64),
+                        torch.tensor(ref64[0])).numpy()
+  with capsys.disabled():
+    print('\n  nbody 32^3: density rel-L2 vs reference %.2e, vs FP64 %.2e '
+          '(reference vs FP64 %.2e); P(k) max rel %.2e' %
+          (err, rel_l2(rho, rho64), rel_l2(z['n32_rho'], rho64), pk_err))
+
+
+def test_nbody_status_nonfinite(fpm):
+  l = golden('lpt')
+  c = fpm.cosmology.Planck15()
+  s = l['n16_init_o1'].copy()
+  s[0, 0, 5, 1] = np.nan
+  with pytest.raises(fpm._lib.FlowPMError):
+    fpm.nbody(c, s, [0.1, 0.2], 16)
+  # the plan and the context stay usable
+  st = fpm.nbody(c, l['n16_init_o1'], [0.1, 0.2], 16)
+  assert torch.isfinite(st).all()
+
+
+def test_batched_uneven_plan(fpm):
+  """Simulations of different sizes, cosmologies and step counts advanced
+  by one plan match the same simulations run one at a time."""
+  from flowpm_b200 import _lib, tfbackground
+  from flowpm_b200._plans import Plan
+  rng = np.random.default_rng(11)
+  sims = [(16, dict(Omega_c=0.25, sigma8=0.8), 5),
+          (16, dict(Omega_c=0.32, sigma8=0.72), 3),
+          (8, dict(Omega_c=0.22, sigma8=0.88), 4),
+          (32, {}, 6)]
+  maxT = max(t for _, _, t in sims)
+  dims, disp, mom, coefs, ffac, nsteps = [], [], [], [], [], []
+  singles = []
+  for n, kw, T in sims:
+    c = fpm.cosmology.Planck15(**kw)
+    lin = rng.standard_normal((1, n, n, n)).astype(np.float32) * 0.3
+    s0 = fpm.lpt_init(c, lin, 0.1, order=2)
+    stages = np.linspace(0.1, 1.0, T + 1)
+    singles.append(host(fpm.nbody(c, s0, stages, n)))
+    dims.append((n, n, n, 1))
+    disp.append(fpm.tfpm._to_disp(s0[0], [n] * 3).reshape(-1, 3))
+    mom.append(s0[1].reshape(-1, 3))
+    co = np.zeros((maxT, 3))
+    co[:T] = tfbackground.nbody_coefficients(c, stages)
+    coefs.append(co)
+    ffac.append(1.5 * c.Omega_m)
+    nsteps.append(T)
+  plan = Plan(dims)
+  d = torch.cat(disp).contiguous()
+  p = torch.cat(mom).contiguous()
+  f = torch.empty_like(d)
+  _lib.call('fpm_nbody', plan.handle, _lib.ptr(d), _lib.ptr(p), _lib.ptr(f),
+            maxT, _lib.ivec(nsteps), _lib.dvec(np.concatenate(coefs).ravel()),
+            _lib.dvec(ffac), None, 0, _lib.stream_ptr())
+  off = 0
+  for (n, _, _), ref in zip(sims, singles):
+    npart = n**3
+    X = d[off:off + npart] + torch.tensor(
+        opm.lattice([n] * 3, 1)[0].numpy(), device='cuda')
+    assert_allclose(host(X), ref[0, 0], atol=1e-4)
+    assert_allclose(host(p[off:off + npart]), ref[1, 0], atol=1e-4)
+    assert_allclose(host(f[off:off + npart]), ref[2, 0], atol=1e-4)
+    off += npart
+  assert plan.status() == 0
