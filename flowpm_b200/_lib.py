@@ -48,7 +48,28 @@ SIGNATURES = {
     'fpm_nbody_set_steps': (c_int, [c_void_p, c_int, P_int32, P_double,
                                     P_double, c_void_p]),
     'fpm_nbody_run': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p,
-                              c_void_p, c_uint, c_void_p]),
+                              c_void_p, c_uint, c_void_p, c_int, c_void_p]),
+    'fpm_nbody_adjoint': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p,
+                                  c_void_p, c_void_p, c_void_p, c_void_p,
+                                  c_int, c_void_p]),
+    'fpm_graph_capture_nbody': (c_int, [c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_uint, c_void_p,
+                                        c_int, ctypes.POINTER(c_void_p)]),
+    'fpm_graph_capture_adjoint': (c_int, [c_void_p, c_void_p, c_void_p,
+                                          c_void_p, c_void_p, c_void_p,
+                                          c_void_p, c_void_p, c_int,
+                                          ctypes.POINTER(c_void_p)]),
+    'fpm_graph_launch': (c_int, [c_void_p, c_void_p]),
+    'fpm_graph_destroy': (c_int, [c_void_p]),
+    'fpm_lpt_adjoint': (c_int, [c_void_p, c_void_p, P_double, c_int,
+                                c_void_p, c_void_p, c_void_p, c_void_p,
+                                c_void_p]),
+    'fpm_cic_paint_adjoint': (c_int, [c_void_p, c_int, c_int, c_int, c_int,
+                                      c_void_p, c_int64, c_void_p, c_void_p,
+                                      c_void_p, c_void_p]),
+    'fpm_cic_readout_adjoint': (c_int, [c_void_p, c_int, c_int, c_int, c_int,
+                                        c_void_p, c_int64, c_void_p, c_void_p,
+                                        c_void_p, c_void_p]),
     'fpm_lpt_init': (c_int, [c_void_p, c_void_p, P_double, c_int, c_void_p,
                              c_void_p, c_void_p, c_void_p]),
     'fpm_linear_field': (c_int, [c_void_p, c_void_p, c_uint64, c_int,
@@ -63,9 +84,11 @@ SIGNATURES = {
 # Constants of include/flowpm_b200.h.
 FPM_OK = 0
 FPM_ERR_NONFINITE = 6
+FPM_ERR_STATE = 7
 FPM_PLAN_CIC_DECONV = 1
 FPM_PLAN_LPT = 2
 FPM_PLAN_GRAD_ORDER0 = 4
+FPM_PLAN_ADJOINT = 8
 FPM_NBODY_INTERMEDIATE = 1
 FPM_STATUS_NONFINITE_POS = 1
 FPM_STATUS_NONFINITE_MOM = 2

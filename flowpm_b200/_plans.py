@@ -27,6 +27,8 @@ class Plan(object):
     _lib.call('fpm_plan_info', h, ctypes.byref(np_tot), ctypes.byref(nbytes))
     self.total_particles = np_tot.value
     self.device_bytes = nbytes.value
+    self._work = None
+    self._graphs = {}
 
   @property
   def nsims(self):
@@ -39,7 +41,39 @@ class Plan(object):
               stream or _lib.stream_ptr())
     return v.value
 
+  def work(self):
+    """Persistent (disp, mom, force) buffers of the plan, (total_np, 3)."""
+    if self._work is None:
+      shape = (self.total_particles, 3)
+      self._work = tuple(
+          torch.empty(shape, dtype=torch.float32, device='cuda')
+          for _ in range(3))
+    return self._work
+
+  def nbody_graph(self, max_steps):
+    """CUDA graph of one leapfrog run of ``max_steps`` on the work buffers
+    (captured once per step count; the step tables are read at replay)."""
+    g = self._graphs.get(('nbody', max_steps))
+    if g is None:
+      d, p, f = self.work()
+      g = ctypes.c_void_p()
+      _lib.call('fpm_graph_capture_nbody', self.handle, _lib.ptr(d),
+                _lib.ptr(p), _lib.ptr(f), None, 0, None, 0, ctypes.byref(g))
+      self._graphs[('nbody', max_steps)] = g
+    return g
+
+  def launch_nbody(self, max_steps, stream):
+    """Replay the leapfrog graph (recaptured if the step tables moved)."""
+    code = _lib.lib.fpm_graph_launch(self.nbody_graph(max_steps), stream)
+    if code == _lib.FPM_ERR_STATE:
+      _lib.lib.fpm_graph_destroy(self._graphs.pop(('nbody', max_steps)))
+      code = _lib.lib.fpm_graph_launch(self.nbody_graph(max_steps), stream)
+    _lib.check('fpm_graph_launch', code)
+
   def close(self):
+    for g in getattr(self, '_graphs', {}).values():
+      _lib.lib.fpm_graph_destroy(g)
+    self._graphs = {}
     if getattr(self, 'handle', None) is not None and self.handle.value:
       _lib.lib.fpm_plan_destroy(self.handle)
       self.handle = None

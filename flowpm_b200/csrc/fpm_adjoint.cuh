@@ -1,0 +1,47 @@
+// Launch wrappers of the adjoint kernels (fpm_adjoint.cu).
+#pragma once
+
+#include "fpm_kernels.cuh"
+
+namespace fpm {
+
+struct AdjArgs {
+  float* disp;            // (total_np, 3) displacement, reconstructed in place
+  float* mom;             // (total_np, 3) momentum, reconstructed in place
+  float* lam_x;           // (total_np, 3) dL/dX
+  float* lam_p;           // (total_np, 3) dL/dp
+  float* fpart;           // (total_np, 3) force at the current position
+  const float* lam_f;     // (total_np, 3) dL/dF at the final position or null
+  const float* fmesh;     // forward force meshes at the current position
+  const float* lrho;      // adjoint density mesh of the previous position
+  float* lmesh;           // three adjoint force meshes (scatter target)
+  float* rho;             // density target of the paint
+  const float* coefs;     // (nsims, max_steps, 3) {kick_start, drift, kick_end}
+  const float* ffac;      // (nsims)
+  const int32_t* nsteps;  // (nsims)
+  const float* ckpt;      // checkpoint slots (d, p) or null
+  int ckpt_every;
+  int32_t* status;
+  int64_t total_np;
+  int max_steps;
+  int it;
+};
+
+void launch_adj_drift_paint(const SimDev* sims, int nsims, int64_t nchunks,
+                            const AdjArgs& a, cudaStream_t st);
+void launch_adj_vjp(const SimDev* sims, int nsims, int64_t nchunks,
+                    const AdjArgs& a, cudaStream_t st);
+void launch_adj_fourier(const SimDev* sims, int nsims, int64_t nchunks,
+                        const float2* lk, float2* out, AxisTabs tabs,
+                        double r_split2, int deconv, cudaStream_t st);
+void launch_lpt_adj_particles(const SimDev* sims, int nsims, int64_t nchunks,
+                              const float* ld, const float* lp,
+                              const float* lf, const float* coef, float* psi1,
+                              int m1, float* psi2, int m2, cudaStream_t st);
+void launch_lpt_adj_fourier(const SimDev* sims, int nsims, int64_t nchunks,
+                            const float2* in, int nin, float2* out,
+                            AxisTabs tabs, cudaStream_t st);
+void launch_lpt_adj_phi(const SimDev* sims, int nsims, int64_t nchunks,
+                        const float* ls, float* phi9, cudaStream_t st);
+
+}  // namespace fpm

@@ -126,6 +126,103 @@ __device__ __forceinline__ bool finite3(float a, float b, float c) {
   return isfinite(a) && isfinite(b) && isfinite(c);
 }
 
+// ---------------------------------------------------------------------------
+// Particle / mode helpers shared by the step and adjoint kernels
+// ---------------------------------------------------------------------------
+// Lattice coordinates of particle `local` of a sim (index (i*ny + j)*nz + k,
+// the order of np.indices(nc).reshape(3, -1).T at flowpm/tfpm.py:162).
+__device__ __forceinline__ void lattice_ijk(const SimDev& S, int64_t local,
+                                            int& i, int& j, int& k) {
+  const int64_t t = local / S.nz;
+  k = (int)(local - t * S.nz);
+  i = (int)(t / S.ny);
+  j = (int)(t - (int64_t)i * S.ny);
+}
+
+// Position in force-mesh units: (q + d) * bf, as the reference's
+// state[0] * pm_nc_factor with state[0] = q + d.
+__device__ __forceinline__ float3 mesh_pos(const SimDev& S, int i, int j,
+                                           int k, float3 d) {
+  const float b = (float)S.bf;
+  float3 x;
+  x.x = __fmul_rn(__fadd_rn((float)i, d.x), b);
+  x.y = __fmul_rn(__fadd_rn((float)j, d.y), b);
+  x.z = __fmul_rn(__fadd_rn((float)k, d.z), b);
+  return x;
+}
+
+__device__ __forceinline__ void paint8(float* __restrict__ m, int my, int mz,
+                                       const Axis& ax, const Axis& ay,
+                                       const Axis& az) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
+    const float w = cic_w(ax, ay, az, cx, cy, cz);
+    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
+              iz = cz ? az.i1 : az.i0;
+    red_add(m + ((int64_t)ix * my + iy) * mz + iz, w);
+  }
+}
+
+// Deposit s * W at the 8 neighbours.
+__device__ __forceinline__ void paint_scaled(float* __restrict__ m, int my,
+                                             int mz, const Axis& ax,
+                                             const Axis& ay, const Axis& az,
+                                             float s) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
+    const float w = cic_w(ax, ay, az, cx, cy, cz);
+    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
+              iz = cz ? az.i1 : az.i0;
+    red_add(m + ((int64_t)ix * my + iy) * mz + iz, __fmul_rn(s, w));
+  }
+}
+
+// Readout of the three force components at the same 8 neighbours.
+__device__ __forceinline__ float3 readout3(const float* __restrict__ f0,
+                                           int64_t mcells, int my, int mz,
+                                           const Axis& ax, const Axis& ay,
+                                           const Axis& az) {
+  float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
+    const float w = cic_w(ax, ay, az, cx, cy, cz);
+    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
+              iz = cz ? az.i1 : az.i0;
+    const int64_t o = ((int64_t)ix * my + iy) * mz + iz;
+    r0 = __fadd_rn(r0, __fmul_rn(__ldg(f0 + o), w));
+    r1 = __fadd_rn(r1, __fmul_rn(__ldg(f0 + mcells + o), w));
+    r2 = __fadd_rn(r2, __fmul_rn(__ldg(f0 + 2 * mcells + o), w));
+  }
+  return make_float3(r0, r1, r2);
+}
+
+__device__ __forceinline__ float3 ld3(const float* p, int64_t g) {
+  return make_float3(p[3 * g], p[3 * g + 1], p[3 * g + 2]);
+}
+__device__ __forceinline__ void st3(float* p, int64_t g, float3 v) {
+  p[3 * g] = v.x;
+  p[3 * g + 1] = v.y;
+  p[3 * g + 2] = v.z;
+}
+// a + s * b with the two roundings of the reference (update = fac * F,
+// state = state + update).
+__device__ __forceinline__ float3 axpy(float3 a, float s, float3 b) {
+  return make_float3(__fadd_rn(a.x, __fmul_rn(s, b.x)),
+                     __fadd_rn(a.y, __fmul_rn(s, b.y)),
+                     __fadd_rn(a.z, __fmul_rn(s, b.z)));
+}
+
+__device__ __forceinline__ void mode_ijl(int64_t local, int ny, int nzh,
+                                         int& i, int& j, int& l) {
+  const int64_t t = local / nzh;
+  l = (int)(local - t * nzh);
+  i = (int)(t / ny);
+  j = (int)(t - (int64_t)i * ny);
+}
+
 inline unsigned grid_for(int64_t chunks) {
   int64_t g = chunks < 1 ? 1 : chunks;
   const int64_t cap = (int64_t)kNumSMs * 16;

@@ -23,6 +23,8 @@ struct StepArgs {
   const float* ffac;       // (nsims) force prefactor (1.5 Omega_m)
   const int32_t* nsteps;   // (nsims)
   int32_t* status;         // device status word
+  float* ckpt;             // checkpoint slots (d, p) or null
+  int ckpt_every;          // position j is saved in slot j / ckpt_every
   int64_t total_np;
   int max_steps;
   int it;                  // global iteration 0..max_steps

@@ -16,7 +16,7 @@
 #include <tuple>
 #include <vector>
 
-#include "fpm_kernels.cuh"
+#include "fpm_adjoint.cuh"
 
 using namespace fpm;
 
@@ -27,8 +27,10 @@ constexpr int kProfKinds = 3;  // 0 step, 1 fourier force, 2 initial paint
 
 struct Run {
   int first, count;        // simulations [first, first + count)
-  cufftHandle r2c = 0, c2r3 = 0;                   // force mesh
+  cufftHandle r2c = 0, c2r3 = 0;     // force mesh
+  cufftHandle r2c3 = 0, c2r1 = 0;    // force mesh, adjoint
   cufftHandle lr2c = 0, lc2r9 = 0, lc2r3 = 0, lc2r1 = 0;  // lattice
+  cufftHandle lr2c3 = 0, lr2c9 = 0;  // lattice, adjoint
 };
 
 template <typename T>
@@ -69,6 +71,10 @@ struct fpm_plan {
   float2* lspec9 = nullptr;
   float* lreal9 = nullptr;
   float* lreal3 = nullptr;
+  // adjoint buffers (FPM_PLAN_ADJOINT)
+  float* lmesh = nullptr;   // 3 adjoint force meshes
+  float* lrho = nullptr;    // adjoint density mesh
+  float* fpart = nullptr;   // per-particle force of the reverse sweep
   // parameters
   float* d_coefs = nullptr;
   int coef_cap = 0;     // steps capacity of d_coefs
@@ -80,6 +86,7 @@ struct fpm_plan {
   void* work = nullptr;
   size_t device_bytes = 0;
   bool steps_set = false;
+  int64_t coef_gen = 0;   // bumped whenever d_coefs is reallocated
   // optional per-kernel timing (fpm_plan_profile)
   bool profile = false;
   std::vector<cudaEvent_t> ev[kProfKinds];
@@ -104,7 +111,8 @@ void prof_mark(fpm_plan* p, int kind, cudaStream_t st) {
 
 void destroy_handles(fpm_plan* p) {
   for (auto& r : p->runs) {
-    cufftHandle* hs[] = {&r.r2c, &r.c2r3, &r.lr2c, &r.lc2r9, &r.lc2r3, &r.lc2r1};
+    cufftHandle* hs[] = {&r.r2c,   &r.c2r3,  &r.r2c3,  &r.c2r1, &r.lr2c,
+                         &r.lc2r9, &r.lc2r3, &r.lc2r1, &r.lr2c3, &r.lr2c9};
     for (cufftHandle* h : hs)
       if (*h) {
         cufftDestroy(*h);
@@ -120,7 +128,8 @@ void free_all(fpm_plan* p) {
   void* bufs[] = {p->d_sims, p->d_kk,   p->d_grad,  p->d_win,   p->rho,
                   p->dk,     p->fk,     p->fmesh,   p->lreal1,  p->lspec1,
                   p->lspec9, p->lreal9, p->lreal3,  p->d_coefs, p->d_nsteps,
-                  p->d_ffac, p->d_lcoef, p->d_status, p->work};
+                  p->d_ffac, p->d_lcoef, p->d_status, p->work,
+                  p->lmesh,  p->lrho,   p->fpart};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -327,13 +336,24 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
   int rc = FPM_OK;
   size_t ws = 0;
   const bool lpt = (flags & FPM_PLAN_LPT) != 0;
+  const bool adj = (flags & FPM_PLAN_ADJOINT) != 0;
   for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
     if (rc == FPM_OK)
       rc = make_plan(&r.r2c, S.mx, S.my, S.mz, CUFFT_R2C, r.count, &ws);
     if (rc == FPM_OK)
       rc = make_plan(&r.c2r3, S.mx, S.my, S.mz, CUFFT_C2R, 3 * r.count, &ws);
+    if (adj) {
+      if (rc == FPM_OK)
+        rc = make_plan(&r.r2c3, S.mx, S.my, S.mz, CUFFT_R2C, 3 * r.count, &ws);
+      if (rc == FPM_OK)
+        rc = make_plan(&r.c2r1, S.mx, S.my, S.mz, CUFFT_C2R, r.count, &ws);
+    }
     if (lpt) {
+      if (rc == FPM_OK)
+        rc = make_plan(&r.lr2c3, S.nx, S.ny, S.nz, CUFFT_R2C, 3 * r.count, &ws);
+      if (rc == FPM_OK)
+        rc = make_plan(&r.lr2c9, S.nx, S.ny, S.nz, CUFFT_R2C, 9 * r.count, &ws);
       if (rc == FPM_OK)
         rc = make_plan(&r.lr2c, S.nx, S.ny, S.nz, CUFFT_R2C, r.count, &ws);
       if (rc == FPM_OK)
@@ -367,6 +387,11 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
     p->lreal9 = dalloc<float>(9 * p->total_l, tot, ok);
     p->lreal3 = dalloc<float>(3 * p->total_l, tot, ok);
   }
+  if (adj) {
+    p->lmesh = dalloc<float>(3 * p->total_m, tot, ok);
+    p->lrho = dalloc<float>(p->total_m, tot, ok);
+    p->fpart = dalloc<float>(3 * p->total_np, tot, ok);
+  }
   p->d_nsteps = dalloc<int32_t>(nsims, tot, ok);
   p->d_ffac = dalloc<float>(nsims, tot, ok);
   p->d_lcoef = dalloc<float>(6 * (size_t)nsims, tot, ok);
@@ -382,7 +407,8 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
     return FPM_ERR_OOM;
   }
   for (auto& r : p->runs) {
-    cufftHandle hs[] = {r.r2c, r.c2r3, r.lr2c, r.lc2r9, r.lc2r3, r.lc2r1};
+    cufftHandle hs[] = {r.r2c,   r.c2r3,  r.r2c3,  r.c2r1, r.lr2c,
+                        r.lc2r9, r.lc2r3, r.lc2r1, r.lr2c3, r.lr2c9};
     for (cufftHandle h : hs)
       if (h && cufftSetWorkArea(h, p->work) != CUFFT_SUCCESS) rc = FPM_ERR_CUFFT;
   }
@@ -471,6 +497,7 @@ extern "C" int fpm_nbody_set_steps(fpm_plan* p, int max_steps,
       return FPM_ERR_OOM;
     }
     p->coef_cap = max_steps;
+    p->coef_gen++;
     p->device_bytes += sizeof(float) * 3 * (size_t)p->nsims * max_steps;
   }
   if (max_steps > 0) {
@@ -491,8 +518,9 @@ extern "C" int fpm_nbody_set_steps(fpm_plan* p, int max_steps,
 
 extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
                              float* force, float* inter, unsigned flags,
-                             void* stream) {
-  if (!p || !disp || !mom || !force) return FPM_ERR_ARG;
+                             float* ckpt, int ckpt_every, void* stream) {
+  if (!p || !disp || !mom || !force || (ckpt && ckpt_every < 1))
+    return FPM_ERR_ARG;
   if (!p->steps_set) return FPM_ERR_STATE;
   if ((flags & FPM_NBODY_INTERMEDIATE) && !inter) return FPM_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
@@ -507,6 +535,8 @@ extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
   a.ffac = p->d_ffac;
   a.nsteps = p->d_nsteps;
   a.status = p->d_status;
+  a.ckpt = ckpt;
+  a.ckpt_every = ckpt ? ckpt_every : 1;
   a.total_np = p->total_np;
   a.max_steps = p->max_steps;
   FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
@@ -531,7 +561,66 @@ extern "C" int fpm_nbody(fpm_plan* p, float* disp, float* mom, float* force,
                          const double* coefs, const double* force_fac,
                          float* inter, unsigned flags, void* stream) {
   FPM_TRY(fpm_nbody_set_steps(p, max_steps, nsteps, coefs, force_fac, stream));
-  return fpm_nbody_run(p, disp, mom, force, inter, flags, stream);
+  return fpm_nbody_run(p, disp, mom, force, inter, flags, nullptr, 0, stream);
+}
+
+extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
+                                 const float* force, float* lam_x,
+                                 float* lam_p, const float* lam_f,
+                                 const float* ckpt, int ckpt_every,
+                                 void* stream) {
+  if (!p || !disp || !mom || !force || !lam_x || !lam_p ||
+      (ckpt && ckpt_every < 1))
+    return FPM_ERR_ARG;
+  if (!(p->flags & FPM_PLAN_ADJOINT) || !p->steps_set) return FPM_ERR_STATE;
+  cudaStream_t st = (cudaStream_t)stream;
+  FPM_CUDA(cudaMemcpyAsync(p->fpart, force, sizeof(float) * 3 * p->total_np,
+                           cudaMemcpyDeviceToDevice, st));
+  AdjArgs a;
+  a.disp = disp;
+  a.mom = mom;
+  a.lam_x = lam_x;
+  a.lam_p = lam_p;
+  a.fpart = p->fpart;
+  a.lam_f = lam_f;
+  a.fmesh = p->fmesh;
+  a.lrho = p->lrho;
+  a.lmesh = p->lmesh;
+  a.rho = p->rho;
+  a.coefs = p->d_coefs;
+  a.ffac = p->d_ffac;
+  a.nsteps = p->d_nsteps;
+  a.ckpt = ckpt;
+  a.ckpt_every = ckpt ? ckpt_every : 1;
+  a.status = p->d_status;
+  a.total_np = p->total_np;
+  a.max_steps = p->max_steps;
+  const double r2 = p->r_split * p->r_split;
+  const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
+  for (int it = p->max_steps; it >= 0; --it) {
+    a.it = it;
+    FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
+    launch_adj_drift_paint(p->d_sims, p->nsims, p->ch_p, a, st);
+    FPM_TRY(launch_ok());
+    FPM_TRY(force_meshes(p, st, false));
+    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, sizeof(float) * 3 * p->total_m, st));
+    launch_adj_vjp(p->d_sims, p->nsims, p->ch_p, a, st);
+    FPM_TRY(launch_ok());
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      FPM_TRY(exec_r2c(r.r2c3, p->lmesh + 3 * S.m_off, p->fk + 3 * S.s_off, st));
+    }
+    launch_adj_fourier(p->d_sims, p->nsims, p->ch_s, p->fk, p->dk, tabs_of(p),
+                       r2, deconv, st);
+    FPM_TRY(launch_ok());
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      FPM_TRY(exec_c2r(r.c2r1, p->dk + S.s_off, p->lrho + S.m_off, st));
+    }
+  }
+  a.it = -1;
+  launch_adj_drift_paint(p->d_sims, p->nsims, p->ch_p, a, st);
+  return launch_ok();
 }
 
 extern "C" int fpm_lpt_init(fpm_plan* p, const float* linear,
@@ -583,6 +672,77 @@ extern "C" int fpm_lpt_init(fpm_plan* p, const float* linear,
                        p->d_lcoef, disp, mom, force, st);
   FPM_TRY(launch_ok());
   // The coefficient upload reads a host vector that dies with this call.
+  FPM_CUDA(cudaStreamSynchronize(st));
+  return FPM_OK;
+}
+
+extern "C" int fpm_lpt_adjoint(fpm_plan* p, const float* linear,
+                               const double* coef, int order,
+                               const float* lam_disp, const float* lam_mom,
+                               const float* lam_force, float* lam_linear,
+                               void* stream) {
+  if (!p || !linear || !coef || !lam_disp || !lam_linear ||
+      (order != 1 && order != 2))
+    return FPM_ERR_ARG;
+  if (!(p->flags & FPM_PLAN_LPT)) return FPM_ERR_STATE;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<float> c(6 * (size_t)p->nsims);
+  for (size_t i = 0; i < c.size(); ++i) c[i] = (float)coef[i];
+  FPM_CUDA(cudaMemcpyAsync(p->d_lcoef, c.data(), sizeof(float) * c.size(),
+                           cudaMemcpyHostToDevice, st));
+  if (order == 2) {
+    // recompute the second-derivative meshes phi_ij of the forward
+    FPM_CUDA(cudaMemcpyAsync(p->lreal1, linear, sizeof(float) * p->total_l,
+                             cudaMemcpyDeviceToDevice, st));
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      FPM_TRY(exec_r2c(r.lr2c, p->lreal1 + S.l_off, p->lspec1 + S.ls_off, st));
+    }
+    launch_lpt_fourier(p->d_sims, p->nsims, p->ch_ls, p->lspec1, p->lspec9, 0,
+                       tabs_of(p), st);
+    FPM_TRY(launch_ok());
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      FPM_TRY(exec_c2r(r.lc2r9, p->lspec9 + 9 * S.ls_off,
+                       p->lreal9 + 9 * S.l_off, st));
+    }
+  } else {
+    for (const SimDev& S : p->sims)
+      FPM_CUDA(cudaMemsetAsync(p->lreal9 + 9 * S.l_off + 3 * S.np, 0,
+                               sizeof(float) * 6 * S.np, st));
+  }
+  launch_lpt_adj_particles(p->d_sims, p->nsims, p->ch_p, lam_disp, lam_mom,
+                           lam_force, p->d_lcoef, p->lreal9, 9,
+                           order == 2 ? p->lreal3 : nullptr, 3, st);
+  FPM_TRY(launch_ok());
+  if (order == 2) {
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      FPM_TRY(exec_r2c(r.lr2c3, p->lreal3 + 3 * S.l_off,
+                       p->lspec9 + 3 * S.ls_off, st));
+    }
+    launch_lpt_adj_fourier(p->d_sims, p->nsims, p->ch_ls, p->lspec9, 3,
+                           p->lspec1, tabs_of(p), st);
+    FPM_TRY(launch_ok());
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      FPM_TRY(exec_c2r(r.lc2r1, p->lspec1 + S.ls_off, p->lreal1 + S.l_off, st));
+    }
+    launch_lpt_adj_phi(p->d_sims, p->nsims, p->ch_l, p->lreal1, p->lreal9, st);
+    FPM_TRY(launch_ok());
+  }
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_r2c(r.lr2c9, p->lreal9 + 9 * S.l_off,
+                     p->lspec9 + 9 * S.ls_off, st));
+  }
+  launch_lpt_adj_fourier(p->d_sims, p->nsims, p->ch_ls, p->lspec9, 9,
+                         p->lspec1, tabs_of(p), st);
+  FPM_TRY(launch_ok());
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_c2r(r.lc2r1, p->lspec1 + S.ls_off, lam_linear + S.l_off, st));
+  }
   FPM_CUDA(cudaStreamSynchronize(st));
   return FPM_OK;
 }
@@ -653,6 +813,98 @@ extern "C" int fpm_plan_profile_read(fpm_plan* p, int kind, double* total_ms,
   *total_ms = t;
   *launches = (int64_t)n;
   p->ev_used[kind] = 0;
+  return FPM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CUDA graphs of the leapfrog and of its adjoint
+// ---------------------------------------------------------------------------
+struct fpm_graph {
+  fpm_plan* plan = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int max_steps = 0;
+  int64_t coef_gen = 0;
+};
+
+namespace {
+
+template <typename F>
+int capture(fpm_plan* p, fpm_graph** out, F&& body) {
+  if (!p || !out) return FPM_ERR_ARG;
+  if (!p->steps_set) return FPM_ERR_STATE;
+  *out = nullptr;
+  cudaStream_t cs;
+  FPM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  const bool prof = p->profile;
+  p->profile = false;
+  cudaGraph_t g = nullptr;
+  int rc = FPM_OK;
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) !=
+      cudaSuccess) {
+    rc = FPM_ERR_CUDA;
+  } else {
+    rc = body(cs);
+    if (cudaStreamEndCapture(cs, &g) != cudaSuccess && rc == FPM_OK)
+      rc = FPM_ERR_CUDA;
+  }
+  p->profile = prof;
+  cudaGraphExec_t exec = nullptr;
+  if (rc == FPM_OK && cudaGraphInstantiate(&exec, g, 0) != cudaSuccess)
+    rc = FPM_ERR_CUDA;
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  if (rc != FPM_OK) {
+    cudaGetLastError();
+    return rc;
+  }
+  fpm_graph* gr = new (std::nothrow) fpm_graph();
+  if (!gr) {
+    cudaGraphExecDestroy(exec);
+    return FPM_ERR_OOM;
+  }
+  gr->plan = p;
+  gr->exec = exec;
+  gr->max_steps = p->max_steps;
+  gr->coef_gen = p->coef_gen;
+  *out = gr;
+  return FPM_OK;
+}
+
+}  // namespace
+
+extern "C" int fpm_graph_capture_nbody(fpm_plan* p, float* disp, float* mom,
+                                       float* force, float* inter,
+                                       unsigned flags, float* ckpt,
+                                       int ckpt_every, fpm_graph** out) {
+  return capture(p, out, [&](cudaStream_t cs) {
+    return fpm_nbody_run(p, disp, mom, force, inter, flags, ckpt, ckpt_every,
+                         cs);
+  });
+}
+
+extern "C" int fpm_graph_capture_adjoint(fpm_plan* p, float* disp, float* mom,
+                                         const float* force, float* lam_x,
+                                         float* lam_p, const float* lam_f,
+                                         const float* ckpt, int ckpt_every,
+                                         fpm_graph** out) {
+  return capture(p, out, [&](cudaStream_t cs) {
+    return fpm_nbody_adjoint(p, disp, mom, force, lam_x, lam_p, lam_f, ckpt,
+                             ckpt_every, cs);
+  });
+}
+
+extern "C" int fpm_graph_launch(fpm_graph* g, void* stream) {
+  if (!g || !g->exec) return FPM_ERR_ARG;
+  if (g->plan->max_steps != g->max_steps || g->plan->coef_gen != g->coef_gen)
+    return FPM_ERR_STATE;
+  FPM_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  return FPM_OK;
+}
+
+extern "C" int fpm_graph_destroy(fpm_graph* g) {
+  if (!g) return FPM_ERR_ARG;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  delete g;
   return FPM_OK;
 }
 

@@ -11,6 +11,7 @@ boundary.  Background prefactors are FP64 (``tfbackground``).
 import numpy as np
 import torch
 
+from . import _autograd
 from . import _lib
 from . import tfbackground as bg
 from ._plans import get_plan
@@ -102,13 +103,16 @@ def linear_field(nc, boxsize, pk, kvec=None, batch_size=1, seed=None,
 
 def lpt_init(cosmo, linear, a, order=2, kvec=None, name='LPTInit'):
   """1LPT / 2LPT initial state (3, batch, npart, 3) from a real linear field
-  (batch, nx, ny, nz) at scale factor ``a`` (flowpm/tfpm.py:148-180)."""
+  (batch, nx, ny, nz) at scale factor ``a`` (flowpm/tfpm.py:148-180).
+  Differentiable in ``linear`` (fpm_lpt_adjoint)."""
   assert order in (1, 2)
   linear = as_cuda(linear)
   if linear.dim() != 4:
     raise ValueError('linear must be (batch, nx, ny, nz)')
   B, nx, ny, nz = linear.shape
   _check_kvec(kvec, [nx, ny, nz])
+  if _autograd.needs_grad(linear):
+    return _autograd.LptInit.apply(linear, cosmo, a, order)
   np_ = nx * ny * nz
   plan = get_plan([(nx, ny, nz, 1)] * B, flags=_lib.FPM_PLAN_LPT)
   coef = np.tile(bg.lpt_coefficients(cosmo, a), B)
@@ -180,11 +184,16 @@ def drift(cosmo, state, ai, ac, af, name='Drift', **kwargs):
 
 def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
           return_intermediate_states=False, pgdparams=None, name='NBody',
-          check_finite=True):
+          check_finite=True, checkpoint_every=None):
   """Integrate ``state`` across ``stages`` with the FastPM KDK leapfrog
   (flowpm/tfpm.py:425-503): one force at stages[0], then per step
   kick / drift / force / kick.  Returns the final state (3, B, Np, 3) or,
   with ``return_intermediate_states``, the list of (a_i, state_i).
+
+  Differentiable in ``state``: the backward is the reverse-time adjoint
+  (fpm_nbody_adjoint), which rebuilds the trajectory from the final state;
+  ``checkpoint_every = k`` stores (d, p) every k steps in the forward and
+  resets the rebuilt trajectory there, bounding its FP32 drift.
 
   With ``check_finite`` the device status word is read at the end and a
   non-finite particle state raises ``FlowPMError``."""
@@ -197,25 +206,40 @@ def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
     return state
   B = state.shape[1]
   T = len(stages) - 1
+  if _autograd.needs_grad(state):
+    if return_intermediate_states:
+      raise NotImplementedError(
+          'gradients through intermediate states are not supported')
+    out = _autograd.NBody.apply(state, cosmo, stages, nc, pm_nc_factor,
+                                checkpoint_every)
+    if check_finite:
+      plan = get_plan([tuple(nc) + (int(pm_nc_factor),)] * B,
+                      flags=_lib.FPM_PLAN_ADJOINT)
+      if plan.status():
+        raise _lib.FlowPMError('nbody', _lib.FPM_ERR_NONFINITE)
+    return out
   plan = get_plan([tuple(nc) + (int(pm_nc_factor),)] * B)
   coefs = np.tile(bg.nbody_coefficients(cosmo, stages)[None], (B, 1, 1))
   st = _lib.stream_ptr()
-  d = _to_disp(state[0], nc)
-  p = state[1].clone()
-  f = torch.empty_like(p)
+  _lib.call('fpm_nbody_set_steps', plan.handle, T, _lib.ivec([T] * B),
+            _lib.dvec(coefs.ravel()), _lib.dvec([1.5 * cosmo.Omega_m] * B), st)
+  d, p, f = plan.work()
+  _lib.call('fpm_lattice_shift', _lib.ptr(state[0]), _lib.ptr(d), B, nc[0],
+            nc[1], nc[2], -1, st)
+  p.copy_(state[1].reshape(-1, 3))
   inter = None
-  flags = 0
   if return_intermediate_states and T > 0:
     inter = torch.empty((T, 3) + tuple(state.shape[1:]), dtype=torch.float32,
                         device=state.device)
-    flags = _lib.FPM_NBODY_INTERMEDIATE
-  _lib.call('fpm_nbody', plan.handle, _lib.ptr(d), _lib.ptr(p), _lib.ptr(f),
-            T, _lib.ivec([T] * B), _lib.dvec(coefs.ravel()),
-            _lib.dvec([1.5 * cosmo.Omega_m] * B), _lib.ptr(inter), flags, st)
+    _lib.call('fpm_nbody_run', plan.handle, _lib.ptr(d), _lib.ptr(p),
+              _lib.ptr(f), _lib.ptr(inter), _lib.FPM_NBODY_INTERMEDIATE, None,
+              0, st)
+  else:
+    plan.launch_nbody(T, st)
   out = torch.empty_like(state)
-  _to_pos(d, nc, out[0])
-  out[1].copy_(p)
-  out[2].copy_(f)
+  _to_pos(d.reshape(state[0].shape), nc, out[0])
+  out[1].copy_(p.reshape(state[1].shape))
+  out[2].copy_(f.reshape(state[2].shape))
   if check_finite:
     status = plan.status(st)
     if status:

@@ -9,6 +9,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import _autograd
 
 __all__ = ['cic_paint', 'cic_readout', 'cic_neighbours', 'r2c3d', 'c2r3d',
            'white_noise', 'compensate_cic']
@@ -36,7 +37,8 @@ def cic_paint(mesh, part, weight=None, name='CiCPaint'):
 
   mesh: (batch, nx, ny, nz); part: (batch, npart, 3) (or any shape with a
   trailing 3 that flattens to it) in mesh units; weight: (batch, npart) or
-  None.  Returns mesh + the CIC deposit; neighbours wrap periodically."""
+  None.  Returns mesh + the CIC deposit; neighbours wrap periodically.
+  Differentiable in mesh, part and weight (fpm_cic_paint_adjoint)."""
   mesh = as_cuda(mesh)
   _check_mesh(mesh)
   B, nx, ny, nz = mesh.shape
@@ -45,6 +47,8 @@ def cic_paint(mesh, part, weight=None, name='CiCPaint'):
   w = None
   if weight is not None:
     w = as_cuda(weight).reshape(B, npart)
+  if _autograd.needs_grad(mesh, part, w):
+    return _autograd.CicPaint.apply(mesh, part, w)
   out = mesh.clone()
   _lib.call('fpm_cic_paint', _lib.ptr(out), B, nx, ny, nz, _lib.ptr(part),
             npart, _lib.ptr(w), _lib.stream_ptr())
@@ -53,12 +57,15 @@ def cic_paint(mesh, part, weight=None, name='CiCPaint'):
 
 def cic_readout(mesh, part, name='CiCReadout'):
   """Read the mesh out at particle positions (flowpm/utils.py:163-210).
-  Returns (batch, npart)."""
+  Returns (batch, npart); differentiable in mesh and part
+  (fpm_cic_readout_adjoint)."""
   mesh = as_cuda(mesh)
   _check_mesh(mesh)
   B, nx, ny, nz = mesh.shape
   part = as_cuda(part).reshape(B, -1, 3)
   npart = part.shape[1]
+  if _autograd.needs_grad(mesh, part):
+    return _autograd.CicReadout.apply(mesh, part)
   out = torch.empty((B, npart), dtype=torch.float32, device=mesh.device)
   _lib.call('fpm_cic_readout', _lib.ptr(mesh), B, nx, ny, nz, _lib.ptr(part),
             npart, _lib.ptr(out), _lib.stream_ptr())

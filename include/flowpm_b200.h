@@ -52,8 +52,10 @@ enum {
                                     off in the reference force              */
   FPM_PLAN_LPT = 1u << 1,        /* also allocate the LPT / linear-field
                                     buffers on the particle lattice         */
-  FPM_PLAN_GRAD_ORDER0 = 1u << 2 /* gradient i*k (order 0) instead of the
+  FPM_PLAN_GRAD_ORDER0 = 1u << 2, /* gradient i*k (order 0) instead of the
                                     4-point finite difference (order 1)   */
+  FPM_PLAN_ADJOINT = 1u << 3     /* also allocate the adjoint buffers and
+                                    cuFFT plans (fpm_nbody_adjoint)         */
 };
 
 /* nbody flags (fpm_nbody). */
@@ -62,6 +64,7 @@ enum {
 };
 
 typedef struct fpm_plan fpm_plan;
+typedef struct fpm_graph fpm_graph;
 
 /* Library version (major*10000 + minor*100 + patch) and error text. */
 int fpm_version(void);
@@ -87,6 +90,21 @@ int fpm_cic_paint(float* mesh, int batch, int nx, int ny, int nz,
 int fpm_cic_readout(const float* mesh, int batch, int nx, int ny, int nz,
                     const float* part, int64_t npart, float* out,
                     void* stream);
+
+/* Adjoint of fpm_cic_paint: lam_part = weight * sum_c lam_mesh[c] grad W,
+ * lam_weight = sum_c lam_mesh[c] W (either output may be NULL).  The CIC
+ * weight derivative follows d|x|/dx = sign(x), sign(0) = 0. */
+int fpm_cic_paint_adjoint(const float* lam_mesh, int batch, int nx, int ny,
+                          int nz, const float* part, int64_t npart,
+                          const float* weight, float* lam_part,
+                          float* lam_weight, void* stream);
+
+/* Adjoint of fpm_cic_readout: lam_mesh += scatter of lam_out with the CIC
+ * weights; lam_part = lam_out * sum_c mesh[c] grad W (either may be NULL). */
+int fpm_cic_readout_adjoint(const float* mesh, int batch, int nx, int ny,
+                            int nz, const float* part, int64_t npart,
+                            const float* lam_out, float* lam_mesh,
+                            float* lam_part, void* stream);
 
 /* Neighbour cells and weights of each particle, in the reference's
  * neighbour order (flowpm/utils.py:66-67): idx[p*8 + c] is the flat cell
@@ -166,7 +184,29 @@ int fpm_nbody_set_steps(fpm_plan* plan, int max_steps, const int32_t* nsteps,
                         const double* coefs, const double* force_fac,
                         void* stream);
 int fpm_nbody_run(fpm_plan* plan, float* disp, float* mom, float* force,
-                  float* inter, unsigned flags, void* stream);
+                  float* inter, unsigned flags, float* ckpt, int ckpt_every,
+                  void* stream);
+
+/* Checkpoints: when ckpt is not NULL, fpm_nbody_run stores the state
+ * (disp, mom) at every position j (after the closing kick of step j-1,
+ * j = 0 the initial state) with j % ckpt_every == 0 in slot j / ckpt_every
+ * of ckpt, each slot 2 x total_particles x 3 floats (disp then mom). */
+
+/* Reverse-time adjoint of fpm_nbody_run (the FastPM adjoint method):
+ * given the final state (disp, mom, force = the outputs of the forward run)
+ * and the cotangents lam_x = dL/dX, lam_p = dL/dp, lam_f = dL/dF (may be
+ * NULL) at the final positions, integrate the leapfrog backwards --
+ * rebuilding positions and momenta from the final state instead of storing
+ * the trajectory, and resetting them to the checkpoints where ckpt is given
+ * -- while propagating the cotangents through every kick, drift and force
+ * (paint adjoint = gather with CIC weight derivatives, readout adjoint =
+ * scatter, Fourier force adjoint = conjugate transfer function).  On return
+ * lam_x, lam_p hold dL/dX_0, dL/dp_0 and disp, mom the rebuilt initial
+ * state.  Needs FPM_PLAN_ADJOINT and fpm_nbody_set_steps. */
+int fpm_nbody_adjoint(fpm_plan* plan, float* disp, float* mom,
+                      const float* force, float* lam_x, float* lam_p,
+                      const float* lam_f, const float* ckpt, int ckpt_every,
+                      void* stream);
 
 /* 2LPT initial conditions, flowpm/tfpm.py:148-180 lpt_init: from the real
  * linear field (the plan's lattice meshes concatenated) compute the 1LPT
@@ -178,6 +218,32 @@ int fpm_nbody_run(fpm_plan* plan, float* disp, float* mom, float* force,
 int fpm_lpt_init(fpm_plan* plan, const float* linear, const double* coef,
                  int order, float* disp, float* mom, float* force,
                  void* stream);
+
+/* CUDA graphs: capture one fpm_nbody_run (or fpm_nbody_adjoint) with the
+ * given buffers into an executable graph, then replay it with
+ * fpm_graph_launch on any stream, with one launch instead of ~10 per
+ * leapfrog step.  The graph reads the plan's step tables at replay time,
+ * so fpm_nbody_set_steps may change their values, but a call that changes
+ * max_steps (or reallocates the tables) makes fpm_graph_launch return
+ * FPM_ERR_STATE.  Capture runs on a private stream and executes nothing.
+ * The graph must be destroyed before its plan. */
+int fpm_graph_capture_nbody(fpm_plan* plan, float* disp, float* mom,
+                            float* force, float* inter, unsigned flags,
+                            float* ckpt, int ckpt_every, fpm_graph** graph);
+int fpm_graph_capture_adjoint(fpm_plan* plan, float* disp, float* mom,
+                              const float* force, float* lam_x, float* lam_p,
+                              const float* lam_f, const float* ckpt,
+                              int ckpt_every, fpm_graph** graph);
+int fpm_graph_launch(fpm_graph* graph, void* stream);
+int fpm_graph_destroy(fpm_graph* graph);
+
+/* Vector-Jacobian product of fpm_lpt_init with respect to the linear
+ * field: lam_linear = d/d(linear) of sum(lam_disp . d + lam_mom . p +
+ * lam_force . f) (lam_mom, lam_force may be NULL).  Synchronises the
+ * stream.  Needs FPM_PLAN_LPT. */
+int fpm_lpt_adjoint(fpm_plan* plan, const float* linear, const double* coef,
+                    int order, const float* lam_disp, const float* lam_mom,
+                    const float* lam_force, float* lam_linear, void* stream);
 
 /* Gaussian white noise N(0, sqrt(N^3)) per cell on every simulation's
  * lattice (Philox4x32-10 counter RNG + Box-Muller), then

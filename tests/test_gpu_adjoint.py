@@ -1,0 +1,161 @@
+"""Gradients of the CUDA path: the hand-written adjoints (CIC paint / readout,
+LPT, reverse-time nbody) against the oracle's autograd -- the stand-in for
+the reference's TensorFlow tape gradient -- and against central finite
+differences of the FP64 oracle.  Bar: 1e-3 relative."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from oracle import background as obg
+from oracle import pm as opm
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def fpm(cuda):
+  import flowpm_b200
+  return flowpm_b200
+
+
+def host(t):
+  return t.detach().cpu().numpy()
+
+
+def test_paint_readout_adjoint(fpm):
+  rng = np.random.default_rng(5)
+  B, n, N = 2, 3000, 16
+  pos = rng.random((B, n, 3)) * N
+  pos[0, :4] = [[3, 4, 5], [0, 0, 0], [15, 2.5, 7], [7.5, 8, 9.25]]
+  w = rng.random((B, n))
+  M = rng.standard_normal((B, N, N, N))
+  mesh = rng.standard_normal((B, N, N, N))
+  r = rng.standard_normal((B, n))
+
+  def ours():
+    x = torch.tensor(pos, dtype=torch.float32, device='cuda',
+                     requires_grad=True)
+    ww = torch.tensor(w, dtype=torch.float32, device='cuda',
+                      requires_grad=True)
+    m = torch.tensor(mesh, dtype=torch.float32, device='cuda',
+                     requires_grad=True)
+    l1 = (fpm.cic_paint(torch.zeros((B, N, N, N), device='cuda'), x, ww) *
+          torch.tensor(M, dtype=torch.float32, device='cuda')).sum()
+    l2 = (fpm.cic_readout(m, x) *
+          torch.tensor(r, dtype=torch.float32, device='cuda')).sum()
+    gx1, gw = torch.autograd.grad(l1, (x, ww))
+    gm, gx2 = torch.autograd.grad(l2, (m, x))
+    return [host(t) for t in (gx1, gw, gm, gx2)]
+
+  def oracle():
+    x = torch.tensor(pos, dtype=torch.float64, requires_grad=True)
+    ww = torch.tensor(w, dtype=torch.float64, requires_grad=True)
+    m = torch.tensor(mesh, dtype=torch.float64, requires_grad=True)
+    l1 = (opm.cic_paint(torch.zeros((B, N, N, N), dtype=torch.float64), x,
+                        ww) * torch.tensor(M)).sum()
+    l2 = (opm.cic_readout(m, x) * torch.tensor(r)).sum()
+    gx1, gw = torch.autograd.grad(l1, (x, ww))
+    gm, gx2 = torch.autograd.grad(l2, (m, x))
+    return [t.numpy() for t in (gx1, gw, gm, gx2)]
+
+  for a, b in zip(ours(), oracle()):
+    assert rel_l2(a, b) < 1e-5
+
+
+@pytest.mark.parametrize('order', [1, 2])
+def test_lpt_adjoint(fpm, order):
+  rng = np.random.default_rng(order)
+  N = 16
+  lin = (rng.standard_normal((2, N, N, N)) * 0.5)
+  R = rng.standard_normal((3, 2, N**3, 3))
+  c = fpm.cosmology.Planck15()
+  x = torch.tensor(lin, dtype=torch.float32, device='cuda',
+                   requires_grad=True)
+  s = fpm.lpt_init(c, x, 0.1, order=order)
+  (g,) = torch.autograd.grad(
+      (s * torch.tensor(R, dtype=torch.float32, device='cuda')).sum(), x)
+  b64 = obg.Background({}, dtype=np.float64)
+  xo = torch.tensor(lin, requires_grad=True)
+  so = opm.lpt_init(b64, xo, 0.1, order=order)
+  (go,) = torch.autograd.grad((so * torch.tensor(R)).sum(), xo)
+  assert rel_l2(host(g), go.numpy()) < 1e-4
+
+
+def _chi2_ours(fpm, lin, target, stages, nc, pm_nc_factor=1, ckpt=None):
+  c = fpm.cosmology.Planck15()
+  x = torch.tensor(lin, dtype=torch.float32, device='cuda',
+                   requires_grad=True)
+  s0 = fpm.lpt_init(c, x, stages[0], order=2)
+  st = fpm.nbody(c, s0, stages, nc, pm_nc_factor=pm_nc_factor,
+                 checkpoint_every=ckpt)
+  rho = fpm.cic_paint(torch.zeros((1,) + tuple(nc), device='cuda'), st[0])
+  loss = ((rho - torch.tensor(target, dtype=torch.float32,
+                              device='cuda'))**2).sum()
+  (g,) = torch.autograd.grad(loss, x)
+  return float(loss), host(g)
+
+
+def _chi2_oracle(lin, target, stages, nc, pm_nc_factor=1, grad=True):
+  b64 = obg.Background({}, dtype=np.float64)
+  x = torch.tensor(lin, dtype=torch.float64, requires_grad=grad)
+  s0 = opm.lpt_init(b64, x, stages[0], order=2)
+  st = opm.nbody(b64, s0, stages, nc, pm_nc_factor=pm_nc_factor)
+  rho = opm.cic_paint(torch.zeros((1,) + tuple(nc), dtype=torch.float64),
+                      st[0])
+  loss = ((rho - torch.tensor(target))**2).sum()
+  if not grad:
+    return float(loss), None
+  (g,) = torch.autograd.grad(loss, x)
+  return float(loss), g.numpy()
+
+
+@pytest.mark.parametrize('pm_nc_factor,ckpt', [(1, None), (2, None), (1, 2)])
+def test_nbody_adjoint_vs_tape(fpm, capsys, pm_nc_factor, ckpt):
+  """d chi^2 / d linear field through lpt_init -> nbody -> cic_paint."""
+  rng = np.random.default_rng(21)
+  nc = [16, 16, 16]
+  lin = rng.standard_normal([1] + nc) * 0.6
+  stages = np.linspace(0.1, 1.0, 6)
+  rho0 = _rho_oracle(lin, stages, nc, pm_nc_factor)
+  target = rho0 + rng.standard_normal(rho0.shape)
+  lo, go = _chi2_oracle(lin, target, stages, nc, pm_nc_factor)
+  l, g = _chi2_ours(fpm, lin, target, stages, nc, pm_nc_factor, ckpt)
+  err = rel_l2(g, go)
+  with capsys.disabled():
+    print('\n  adjoint vs FP64 tape gradient (B=%d, ckpt=%s): rel-L2 %.2e, '
+          'loss %.6g vs %.6g' % (pm_nc_factor, ckpt, err, l, lo))
+  assert err < 1e-3
+
+
+def _rho_oracle(lin, stages, nc, pm_nc_factor=1):
+  b64 = obg.Background({}, dtype=np.float64)
+  s0 = opm.lpt_init(b64, torch.tensor(lin), stages[0], order=2)
+  st = opm.nbody(b64, s0, stages, nc, pm_nc_factor=pm_nc_factor)
+  return opm.cic_paint(torch.zeros((1,) + tuple(nc), dtype=torch.float64),
+                       st[0]).numpy()
+
+
+def test_nbody_adjoint_vs_finite_differences(fpm, capsys):
+  """Directional derivatives of chi^2 along random directions: adjoint
+  gradient vs central differences of the FP64 oracle."""
+  rng = np.random.default_rng(8)
+  nc = [16, 16, 16]
+  lin = rng.standard_normal([1] + nc) * 0.6
+  stages = np.linspace(0.1, 1.0, 6)
+  target = _rho_oracle(lin, stages, nc) + rng.standard_normal([1] + nc)
+  _, g = _chi2_ours(fpm, lin, target, stages, nc)
+  errs = []
+  for _ in range(4):
+    u = rng.standard_normal(lin.shape)
+    u /= np.linalg.norm(u)
+    eps = 1e-4
+    lp, _ = _chi2_oracle(lin + eps * u, target, stages, nc, grad=False)
+    lm, _ = _chi2_oracle(lin - eps * u, target, stages, nc, grad=False)
+    fd = (lp - lm) / (2 * eps)
+    ad = float(np.sum(g * u))
+    errs.append(abs(ad - fd) / abs(fd))
+  with capsys.disabled():
+    print('\n  adjoint vs FP64 central differences: max rel %.2e' %
+          max(errs))
+  assert max(errs) < 1e-3

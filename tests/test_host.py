@@ -162,7 +162,9 @@ def test_capi_rejects_bad_arguments(fpm):
   assert L.fpm_plan_create(ctypes.byref(h), 1, dims, 0.0, 0) == 1
   assert L.fpm_plan_create(ctypes.byref(h), 0, dims, 0.0, 0) == 1
   assert L.fpm_plan_destroy(None) == 1
-  assert L.fpm_nbody_run(None, None, None, None, None, 0, None) == 1
+  assert L.fpm_nbody_run(None, None, None, None, None, 0, None, 0, None) == 1
+  assert L.fpm_nbody_adjoint(None, None, None, None, None, None, None, None,
+                             0, None) == 1
 
 
 def test_product_does_not_import_oracle():
