@@ -69,7 +69,7 @@ __device__ __forceinline__ float3 gather_grad(const float* __restrict__ m,
 //   lam_ph = lam_p + dr lam_x
 // then paint x_it (also for the sims starting their reverse sweep, it == T).
 // it = -1: only the final gather at position 0.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                   AdjArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -127,7 +127,7 @@ k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       if (a.it < 0) continue;
       const float3 x = mesh_pos(S, i, j, k, d);
       if (!finite3(x.x, x.y, x.z)) atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
-      paint8(m, S.my, S.mz, cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
+      paint8(m, S.mx, S.my, S.mz, cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
              cic_axis(x.z, S.mz));
     }
   }
@@ -138,7 +138,7 @@ k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 // cotangent v = (ks_it + ke_{it-1}) lam_p (+ lam_F at the last position):
 //   lam_x += fac * sum_c grad W * (v . f[c])            (readout weights)
 //   lam_f[c] += (fac / B) * v * W                       (scatter)
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
           AdjArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -324,7 +324,7 @@ k_cic_readout_adjoint(const float* __restrict__ mesh, int nx, int ny, int nz,
     if (lmesh) {
       const Axis ax = cic_axis(y.x, nx), ay = cic_axis(y.y, ny),
                  az = cic_axis(y.z, nz);
-      paint_scaled(lmesh + b * ncell, ny, nz, ax, ay, az, lo);
+      paint_scaled(lmesh + b * ncell, nx, ny, nz, ax, ay, az, lo);
     }
   }
 }

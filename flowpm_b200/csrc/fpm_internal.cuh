@@ -122,6 +122,40 @@ __device__ __forceinline__ void red_add(float* p, float v) {
   asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }
 
+// Tuning knobs of the particle kernels (compile-time).
+// Measured on B200 at 128^3: 3 blocks (80 registers) beats 2 (128
+// registers) and 4 (64 registers, spills); the v4 pair reduction is slower
+// than two scalar reductions (33 vs 49 us for 2^21 particles).
+#ifndef FPM_STEP_MINBLOCKS
+#define FPM_STEP_MINBLOCKS 3   // resident blocks of 256 threads per SM
+#endif
+#ifndef FPM_PAINT_VEC
+#define FPM_PAINT_VEC 0        // z-adjacent neighbour pairs as one v4 add
+#endif
+
+// m[e] += a, m[e + 1] += b as one 16-byte vector reduction when both lie
+// in the same aligned float4 and that float4 lies inside m[0, n) (three
+// quarters of the pairs), else as two scalar reductions.
+__device__ __forceinline__ void red_add_pair(float* m, int64_t n, int64_t e,
+                                             float a, float b) {
+#if FPM_PAINT_VEC
+  const int lane = (int)(((uintptr_t)(m + e) >> 2) & 3);
+  if (lane != 3 && e >= lane && e - lane + 4 <= n) {
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (lane == 0) { v.x = a; v.y = b; }
+    else if (lane == 1) { v.y = a; v.z = b; }
+    else { v.z = a; v.w = b; }
+    float* base = m + e - lane;
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(base),
+                 "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+    return;
+  }
+#endif
+  red_add(m + e, a);
+  red_add(m + e + 1, b);
+}
+
 __device__ __forceinline__ bool finite3(float a, float b, float c) {
   return isfinite(a) && isfinite(b) && isfinite(c);
 }
@@ -151,31 +185,48 @@ __device__ __forceinline__ float3 mesh_pos(const SimDev& S, int i, int j,
   return x;
 }
 
-__device__ __forceinline__ void paint8(float* __restrict__ m, int my, int mz,
-                                       const Axis& ax, const Axis& ay,
+__device__ __forceinline__ void paint8(float* __restrict__ m, int mx, int my,
+                                       int mz, const Axis& ax, const Axis& ay,
                                        const Axis& az) {
+  const bool adj = az.i1 == az.i0 + 1;
+  const int64_t n = (int64_t)mx * my * mz;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
-    const float w = cic_w(ax, ay, az, cx, cy, cz);
-    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
-              iz = cz ? az.i1 : az.i0;
-    red_add(m + ((int64_t)ix * my + iy) * mz + iz, w);
+  for (int q = 0; q < 4; ++q) {
+    const int cx = q & 1, cy = q >> 1;
+    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0;
+    const float wxy = __fmul_rn(cx ? ax.w1 : ax.w0, cy ? ay.w1 : ay.w0);
+    const int64_t row = ((int64_t)ix * my + iy) * mz;
+    const float w0 = __fmul_rn(wxy, az.w0), w1 = __fmul_rn(wxy, az.w1);
+    if (adj) {
+      red_add_pair(m, n, row + az.i0, w0, w1);
+    } else {
+      red_add(m + row + az.i0, w0);
+      red_add(m + row + az.i1, w1);
+    }
   }
 }
 
 // Deposit s * W at the 8 neighbours.
-__device__ __forceinline__ void paint_scaled(float* __restrict__ m, int my,
-                                             int mz, const Axis& ax,
+__device__ __forceinline__ void paint_scaled(float* __restrict__ m, int mx,
+                                             int my, int mz, const Axis& ax,
                                              const Axis& ay, const Axis& az,
                                              float s) {
+  const bool adj = az.i1 == az.i0 + 1;
+  const int64_t n = (int64_t)mx * my * mz;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
-    const float w = cic_w(ax, ay, az, cx, cy, cz);
-    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
-              iz = cz ? az.i1 : az.i0;
-    red_add(m + ((int64_t)ix * my + iy) * mz + iz, __fmul_rn(s, w));
+  for (int q = 0; q < 4; ++q) {
+    const int cx = q & 1, cy = q >> 1;
+    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0;
+    const float wxy = __fmul_rn(cx ? ax.w1 : ax.w0, cy ? ay.w1 : ay.w0);
+    const int64_t row = ((int64_t)ix * my + iy) * mz;
+    const float w0 = __fmul_rn(s, __fmul_rn(wxy, az.w0));
+    const float w1 = __fmul_rn(s, __fmul_rn(wxy, az.w1));
+    if (adj) {
+      red_add_pair(m, n, row + az.i0, w0, w1);
+    } else {
+      red_add(m + row + az.i0, w0);
+      red_add(m + row + az.i1, w1);
+    }
   }
 }
 

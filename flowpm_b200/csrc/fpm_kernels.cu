@@ -14,7 +14,7 @@ namespace fpm {
 // Particle kernels
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_paint_lattice(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                 const float* __restrict__ disp, float* __restrict__ rho,
                 int32_t* status) {
@@ -31,13 +31,13 @@ k_paint_lattice(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       const float3 d = ld3(disp, S.p_off + local);
       const float3 x = mesh_pos(S, i, j, k, d);
       if (!finite3(x.x, x.y, x.z)) atomicOr(status, FPM_STATUS_NONFINITE_POS);
-      paint8(m, S.my, S.mz, cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
+      paint8(m, S.mx, S.my, S.mz, cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
              cic_axis(x.z, S.mz));
     }
   }
 }
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
        StepArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -101,13 +101,13 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       const float3 xn = mesh_pos(S, i, j, k, d);
       if (!finite3(xn.x, xn.y, xn.z))
         atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
-      paint8(m, S.my, S.mz, cic_axis(xn.x, S.mx), cic_axis(xn.y, S.my),
+      paint8(m, S.mx, S.my, S.mz, cic_axis(xn.x, S.mx), cic_axis(xn.y, S.my),
              cic_axis(xn.z, S.mz));
     }
   }
 }
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_force_readout(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                 const float* __restrict__ disp,
                 const float* __restrict__ fmesh,
