@@ -14,6 +14,7 @@ from . import tfbackground as background
 from . import tfpower
 from .utils import cic_paint, cic_readout, r2c3d, c2r3d, white_noise
 from .tfpm import nbody, linear_field, lpt_init
+from .pk import power_spectrum
 from ._plans import clear_plans
 
 __version__ = '0.1.0'

@@ -77,6 +77,11 @@ SIGNATURES = {
     'fpm_lattice_shift': (c_int, [c_void_p, c_void_p, c_int, c_int, c_int,
                                   c_int, c_int, c_void_p]),
     'fpm_saxpy': (c_int, [c_void_p, c_void_p, c_float, c_int64, c_void_p]),
+    'fpm_pk_bin': (c_int, [c_void_p, c_int, c_int, c_int, c_int, P_double,
+                           c_double, c_double, c_int, c_void_p, c_void_p]),
+    'fpm_power_spectrum': (c_int, [c_void_p, c_int, c_int, c_int, c_int,
+                                   P_double, c_double, c_double, c_int,
+                                   c_void_p, c_void_p]),
     'fpm_white_noise': (c_int, [c_void_p, c_int64, c_uint64, c_double,
                                 c_void_p]),
 }

@@ -268,6 +268,29 @@ int fpm_lattice_shift(const float* in, float* out, int batch, int nx, int ny,
  * :309-314). */
 int fpm_saxpy(float* y, const float* x, float a, int64_t n, void* stream);
 
+/* ---------------------------------------------------------------------
+ * Power spectrum, the estimator of flowpm/pk.py:7-103 (power_spectrum):
+ * P[b][i] = sum W |F|^2 / sum W over the modes with
+ * numpy.digitize(|k|, edges) == i + 1, times prod(boxsize) / ncell^2, for
+ * i < nedges - 1, where edges[n] = kmin + n * dk, F the unnormalised FFT
+ * of the field and W the reference's mode weights (1 on the z planes 0 and
+ * nz - 1 of the full spectrum, 2 elsewhere).  boxsize holds 3 doubles;
+ * power is (batch, nedges - 1) floats.
+ * ------------------------------------------------------------------ */
+
+/* From the unnormalised R2C half spectrum (batch, nx, ny, nz/2 + 1) of the
+ * field.  Takes its bin accumulators (2 x batch x (nedges + 1) doubles)
+ * from the stream-ordered allocator. */
+int fpm_pk_bin(const void* delta_k, int batch, int nx, int ny, int nz,
+               const double* boxsize, double kmin, double dk, int nedges,
+               float* power, void* stream);
+
+/* From the real field (batch, nx, ny, nz): R2C (cached cuFFT plan) then
+ * fpm_pk_bin. */
+int fpm_power_spectrum(const float* field, int batch, int nx, int ny, int nz,
+                       const double* boxsize, double kmin, double dk,
+                       int nedges, float* power, void* stream);
+
 /* Gaussian white noise alone: out[e] = stddev * N(0,1) for e < n with the
  * generator of fpm_linear_field (counter = element index). */
 int fpm_white_noise(float* out, int64_t n, uint64_t seed, double stddev,

@@ -286,3 +286,27 @@ def test_batched_uneven_plan(fpm):
     assert_allclose(host(f[off:off + npart]), ref[2, 0], atol=1e-4)
     off += npart
   assert plan.status() == 0
+
+
+# --------------------------------------------------------------------------
+# Power spectrum (flowpm/pk.py)
+# --------------------------------------------------------------------------
+def test_power_spectrum_golden(fpm):
+  z = golden('pk')
+  for tag in ['rho32', 'lin16']:
+    bs = float(z[tag + '_boxsize'])
+    kb, p = fpm.power_spectrum(z[tag + '_field'], kmin=0.1, dk=0.05,
+                               boxsize=np.array([bs] * 3))
+    assert_allclose(kb, z[tag + '_k'], rtol=1e-12)
+    assert_allclose(host(p), z[tag + '_pk'], rtol=2e-5)
+
+
+def test_power_spectrum_batched_rectangular(fpm):
+  rng = np.random.default_rng(4)
+  f = rng.standard_normal((3, 8, 12, 16)).astype(np.float32)
+  box = np.array([40., 60., 80.])
+  kb, p = fpm.power_spectrum(f, kmin=0.05, dk=0.02, boxsize=box)
+  kb_o, p_o = opm.power_spectrum(torch.tensor(f, dtype=torch.float64),
+                                 kmin=0.05, dk=0.02, boxsize=box)
+  assert_allclose(kb, kb_o, rtol=1e-12)
+  assert_allclose(host(p), p_o.numpy(), rtol=1e-5)
