@@ -79,6 +79,9 @@ SIGNATURES = {
     'fpm_saxpy': (c_int, [c_void_p, c_void_p, c_float, c_int64, c_void_p]),
     'fpm_pk_bin': (c_int, [c_void_p, c_int, c_int, c_int, c_int, P_double,
                            c_double, c_double, c_int, c_void_p, c_void_p]),
+    'fpm_pk_bin_noalloc': (c_int, [c_void_p, c_int, c_int, c_int, c_int,
+                                   P_double, c_double, c_double, c_int,
+                                   c_void_p, c_void_p]),
     'fpm_power_spectrum': (c_int, [c_void_p, c_int, c_int, c_int, c_int,
                                    P_double, c_double, c_double, c_int,
                                    c_void_p, c_void_p]),
@@ -90,6 +93,7 @@ SIGNATURES = {
 FPM_OK = 0
 FPM_ERR_NONFINITE = 6
 FPM_ERR_STATE = 7
+FPM_ERR_LIMIT = 9
 FPM_PLAN_CIC_DECONV = 1
 FPM_PLAN_LPT = 2
 FPM_PLAN_GRAD_ORDER0 = 4

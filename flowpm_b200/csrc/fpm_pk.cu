@@ -221,3 +221,69 @@ extern "C" int fpm_power_spectrum(const float* field, int batch, int nx,
   cudaFreeAsync(spec, st);
   return rc;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of fpm_pk_bin.
+//
+// Some callers cannot let a library allocate device memory: applications
+// that hand all of a GPU's memory to their own pool or arena (where a
+// cudaMalloc / cudaMallocAsync from a library fails or fragments it), and
+// latency-critical loops that forbid allocation after start-up because an
+// allocation can synchronise the device.  For them the bin accumulators of
+// the power spectrum live in a fixed file-scope device array instead of
+// stream-ordered scratch.  The array is part of this library's module, so
+// every GPU that loads the library holds it (128 KiB) until the process
+// exits.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double
+    g_pk_static_scratch[FPM_PK_NOALLOC_MAX_DOUBLES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+double* g_static_ptr[kMaxDevices] = {};
+
+// Device address of g_pk_static_scratch on the current device.  On host,
+// the name g_pk_static_scratch is only a stand-in for the device symbol,
+// so its device address is looked up once per device (with that device
+// current) and cached.
+int static_scratch(double** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return FPM_ERR_CUDA;
+  if (dev < 0 || dev >= kMaxDevices) return FPM_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_pk_static_scratch) != cudaSuccess ||
+        !p) {
+      cudaGetLastError();
+      return FPM_ERR_CUDA;
+    }
+    g_static_ptr[dev] = (double*)p;
+  }
+  *out = g_static_ptr[dev];
+  return FPM_OK;
+}
+
+}  // namespace
+
+extern "C" int fpm_pk_bin_noalloc(const void* delta_k, int batch, int nx,
+                                  int ny, int nz, const double* boxsize,
+                                  double kmin, double dk, int nedges,
+                                  float* power, void* stream) {
+  int rc = pk_check(delta_k, batch, nx, ny, nz, boxsize, dk, nedges, power);
+  if (rc != FPM_OK) return rc;
+  const int64_t n = 2 * (int64_t)batch * (nedges + 1);
+  if (n > FPM_PK_NOALLOC_MAX_DOUBLES) return FPM_ERR_LIMIT;
+  double* scratch = nullptr;
+  rc = static_scratch(&scratch);
+  if (rc != FPM_OK) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // The array keeps the previous call's sums: clear the part this call uses.
+  if (cudaMemsetAsync(scratch, 0, n * sizeof(double), st) != cudaSuccess)
+    return FPM_ERR_CUDA;
+  const PkGeom g = pk_geom(nx, ny, nz, boxsize, kmin, dk, nedges);
+  return pk_launch((const float2*)delta_k, batch, g, scratch,
+                   boxsize[0] * boxsize[1] * boxsize[2], power, st);
+}

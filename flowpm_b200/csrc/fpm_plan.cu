@@ -250,6 +250,8 @@ extern "C" const char* fpm_error_string(int code) {
     case FPM_ERR_NONFINITE: return "non-finite particle state";
     case FPM_ERR_STATE: return "call out of order";
     case FPM_ERR_UNSUPPORTED: return "unsupported request";
+    case FPM_ERR_LIMIT:
+      return "request exceeds the fixed scratch of an allocation-free entry";
     default: return "unknown error";
   }
 }

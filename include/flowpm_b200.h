@@ -35,7 +35,9 @@ enum {
   FPM_ERR_CUFFT = 5,      /* a cuFFT call failed                        */
   FPM_ERR_NONFINITE = 6,  /* device status: non-finite particle state   */
   FPM_ERR_STATE = 7,      /* call out of order (e.g. missing workspace) */
-  FPM_ERR_UNSUPPORTED = 8 /* valid request this build does not handle   */
+  FPM_ERR_UNSUPPORTED = 8, /* valid request this build does not handle  */
+  FPM_ERR_LIMIT = 9        /* request larger than the fixed scratch of an
+                              allocation-free entry point                  */
 };
 
 /* Device status bits accumulated by the kernels of a plan. */
@@ -284,6 +286,29 @@ int fpm_saxpy(float* y, const float* x, float a, int64_t n, void* stream);
 int fpm_pk_bin(const void* delta_k, int batch, int nx, int ny, int nz,
                const double* boxsize, double kmin, double dk, int nedges,
                float* power, void* stream);
+
+/* Capacity, in doubles, of the fixed device array behind
+ * fpm_pk_bin_noalloc: 2 * batch * (nedges + 1) must not exceed it. */
+#define FPM_PK_NOALLOC_MAX_DOUBLES 16384
+
+/* fpm_pk_bin without any device allocation.  No counterpart in the
+ * reference.  For callers that cannot let a library allocate device memory:
+ * applications that give all of a GPU's memory to their own pool or arena,
+ * so that a cudaMalloc / cudaMallocAsync from here would fail or fragment
+ * it, and loops that forbid allocation after start-up because allocating
+ * can synchronise the device.  The bin sums live in a fixed 128 KiB array
+ * inside this library (FPM_PK_NOALLOC_MAX_DOUBLES doubles), which every GPU
+ * that loads the library holds until the process exits; requests with
+ * 2 * batch * (nedges + 1) above that return FPM_ERR_LIMIT.  The caller
+ * passes the inputs and the output as for fpm_pk_bin.  The first call on a
+ * device looks up the array's device address (once per device) -- make
+ * that first call before any stream capture.  All calls share the one
+ * array and each clears the part it uses before summing, so calls whose
+ * execution overlaps on the GPU (several streams, several host threads)
+ * race; order them on one stream. */
+int fpm_pk_bin_noalloc(const void* delta_k, int batch, int nx, int ny, int nz,
+                       const double* boxsize, double kmin, double dk,
+                       int nedges, float* power, void* stream);
 
 /* From the real field (batch, nx, ny, nz): R2C (cached cuFFT plan) then
  * fpm_pk_bin. */
