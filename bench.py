@@ -53,6 +53,9 @@ def parse():
   ap.add_argument('--impl', default='flowpm_b200',
                   choices=['flowpm_b200', 'reference'])
   ap.add_argument('--no-cpu-baseline', action='store_true')
+  ap.add_argument('--no-extras', action='store_true',
+                  help='skip the C4 (forward + adjoint) and C3 (batched) '
+                  'measurements')
   return ap.parse_args()
 
 
@@ -221,6 +224,233 @@ def run_reference(args, rank, world):
               'd2h_bytes_per_step': 0},
   }
   print(json.dumps(line))
+
+
+def _pk_interp(cosmo):
+  from flowpm_b200 import tfpower
+  kk = np.logspace(-4, 2, 4096)
+  pk = tfpower.linear_matter_power(cosmo, kk)
+  return lambda k: np.interp(np.log(np.maximum(k, 1e-30)), np.log(kk), pk,
+                             left=0.0)
+
+
+def _timed(fn, reps, flush):
+  """Device time (ms) of fn() per call, L2 flushed before every call."""
+  ts = []
+  for _ in range(reps):
+    flush.fill_(1.0)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    fn()
+    e1.record()
+    torch.cuda.synchronize()
+    ts.append(e0.elapsed_time(e1))
+  return float(np.median(ts))
+
+
+def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5,
+                        fd_dirs=32):
+  """Config C4: 128^3, 20 steps, chi^2 of the final CIC density against
+  (that density + N(0, 1) noise); gradient with respect to the initial
+  linear field.  Timed step = forward leapfrog (graph, checkpoints every
+  `ckpt`) + loss gradient + reverse-time adjoint (graph).  The gradient is
+  also checked against central differences of the same FP32 pipeline along
+  `fd_dirs` random directions of the linear field."""
+  from flowpm_b200 import _lib, tfbackground
+  from flowpm_b200._plans import get_plan
+  cosmo = fpm.cosmology.Planck15()
+  nc = [n] * 3
+  np_ = n**3
+  st = _lib.stream_ptr()
+  lin = fpm.linear_field(nc, BOX, _pk_interp(cosmo), seed=4242)
+  stages = np.linspace(A0, 1.0, steps + 1)
+  plan = get_plan([tuple(nc) + (1,)], flags=_lib.FPM_PLAN_ADJOINT)
+  coefs = tfbackground.nbody_coefficients(cosmo, stages)
+  _lib.call('fpm_nbody_set_steps', plan.handle, steps, _lib.ivec([steps]),
+            _lib.dvec(coefs.ravel()), _lib.dvec([1.5 * cosmo.Omega_m]), st)
+  s0 = fpm.lpt_init(cosmo, lin, A0, order=2)
+  d0 = fpm.tfpm._to_disp(s0[0], nc).reshape(-1, 3).contiguous()
+  p0 = s0[1].reshape(-1, 3).contiguous().clone()
+  d, p, f = torch.empty_like(d0), torch.empty_like(p0), torch.empty_like(d0)
+  lx, lp = torch.empty_like(d0), torch.empty_like(d0)
+  X = torch.empty_like(d0)
+  rho = torch.empty((1,) + tuple(nc), device='cuda')
+  g = torch.empty_like(rho)
+  nslot = steps // ckpt + 1
+  ck = torch.empty((nslot, 2, np_, 3), device='cuda')
+  gf, ga = _lib.ctypes.c_void_p(), _lib.ctypes.c_void_p()
+  _lib.call('fpm_graph_capture_nbody', plan.handle, _lib.ptr(d), _lib.ptr(p),
+            _lib.ptr(f), None, 0, _lib.ptr(ck), ckpt, _lib.ctypes.byref(gf))
+  _lib.call('fpm_graph_capture_adjoint', plan.handle, _lib.ptr(d),
+            _lib.ptr(p), _lib.ptr(f), _lib.ptr(lx), _lib.ptr(lp), None,
+            _lib.ptr(ck), ckpt, _lib.ctypes.byref(ga))
+
+  def forward():
+    d.copy_(d0)
+    p.copy_(p0)
+    _lib.call('fpm_graph_launch', gf, st)
+    _lib.call('fpm_lattice_shift', _lib.ptr(d), _lib.ptr(X), 1, n, n, n, 1,
+              st)
+    rho.zero_()
+    _lib.call('fpm_cic_paint', _lib.ptr(rho), 1, n, n, n, _lib.ptr(X), np_,
+              None, st)
+
+  forward()
+  gen = torch.Generator(device='cuda').manual_seed(77)
+  target = rho + torch.randn(rho.shape, generator=gen, device='cuda')
+
+  def step():
+    forward()
+    # dL/drho = 2 (rho - target); dL/dX by the paint adjoint
+    g.copy_(rho)
+    _lib.call('fpm_saxpy', _lib.ptr(g), _lib.ptr(target), -1.0, g.numel(), st)
+    _lib.call('fpm_cic_paint_adjoint', _lib.ptr(g), 1, n, n, n, _lib.ptr(X),
+              np_, None, _lib.ptr(lx), None, st)
+    _lib.call('fpm_saxpy', _lib.ptr(lx), _lib.ptr(lx), 1.0, lx.numel(), st)
+    lp.zero_()
+    _lib.call('fpm_graph_launch', ga, st)
+
+  for _ in range(3):
+    step()
+  ms = _timed(step, reps, flush)
+  ms_fwd = _timed(forward, reps, flush)
+  # gradient with respect to the linear field (LPT adjoint)
+  step()
+  coef = tfbackground.lpt_coefficients(cosmo, A0)
+  glin = torch.empty_like(lin)
+  _lib.call('fpm_lpt_adjoint', get_plan([tuple(nc) + (1,)],
+                                        flags=_lib.FPM_PLAN_LPT).handle,
+            _lib.ptr(lin), _lib.dvec(coef), 2, _lib.ptr(lx), _lib.ptr(lp),
+            None, _lib.ptr(glin), st)
+  grad = glin.double().cpu().numpy().ravel()
+
+  def loss(field):
+    s = fpm.lpt_init(cosmo, field, A0, order=2)
+    d0.copy_(fpm.tfpm._to_disp(s[0], nc).reshape(-1, 3))
+    p0.copy_(s[1].reshape(-1, 3))
+    forward()
+    return float(((rho.double() - target.double())**2).sum())
+
+  rng = np.random.default_rng(5)
+  fd = {}
+  lin_std = float(lin.std())
+  for rel in (1e-3, 1e-2):
+    errs = []
+    for _ in range(fd_dirs):
+      u = torch.tensor(rng.standard_normal(lin.shape), dtype=torch.float32,
+                       device='cuda')
+      eps = rel * lin_std
+      lpl = loss(lin + eps * u)
+      lmi = loss(lin - eps * u)
+      fdv = (lpl - lmi) / (2 * eps)
+      ad = float(np.dot(grad, u.double().cpu().numpy().ravel()))
+      errs.append(abs(ad - fdv) / max(abs(fdv), 1e-30))
+    fd['eps_%g' % rel] = {'median_rel': float(np.median(errs)),
+                          'max_rel': float(np.max(errs))}
+  _lib.lib.fpm_graph_destroy(gf)
+  _lib.lib.fpm_graph_destroy(ga)
+  upd = float(np_) * steps
+  return {
+      'workload': 'C4: 128^3, 20 KDK steps, chi^2(final CIC density, '
+                  'density + N(0,1)), reverse-time adjoint, checkpoint every '
+                  '%d' % ckpt,
+      'value': upd / (ms * 1e-3),
+      'unit': 'particle-updates/s (forward + adjoint)',
+      'ms_per_step': ms,
+      'forward_ms': ms_fwd,
+      'adjoint_over_forward': (ms - ms_fwd) / ms_fwd,
+      'grad_vs_fp32_central_differences': fd,
+      'fd_directions': fd_dirs,
+  }
+
+
+def measure_batched(fpm, flush, reps):
+  """Config C3: 8 x 32^3 + 8 x 64^3 + 4 x 128^3 simulations, per-sim
+  Omega_c ~ U[0.20, 0.35], sigma8 ~ U[0.70, 0.90], 10-20 steps each, in one
+  plan and one CUDA graph, against the plain path (one simulation at a time,
+  no graph)."""
+  from flowpm_b200 import _lib, tfbackground
+  from flowpm_b200._plans import Plan, get_plan
+  rng = np.random.default_rng(2024)
+  spec = [(32, 100.)] * 8 + [(64, 100.)] * 8 + [(128, 200.)] * 4
+  sims = []
+  for i, (n, box) in enumerate(spec):
+    c = fpm.cosmology.Planck15(Omega_c=float(rng.uniform(0.20, 0.35)),
+                               sigma8=float(rng.uniform(0.70, 0.90)))
+    sims.append((n, box, c, int(rng.integers(10, 21)), 500 + i))
+  maxT = max(s[3] for s in sims)
+  st = _lib.stream_ptr()
+  d0s, p0s, coefs, ffac, nsteps, dims = [], [], [], [], [], []
+  for n, box, c, T, seed in sims:
+    lin = fpm.linear_field(n, box, _pk_interp(c), seed=seed)
+    s0 = fpm.lpt_init(c, lin, A0, order=2)
+    d0s.append(fpm.tfpm._to_disp(s0[0], [n] * 3).reshape(-1, 3))
+    p0s.append(s0[1].reshape(-1, 3).contiguous())
+    co = np.zeros((maxT, 3))
+    co[:T] = tfbackground.nbody_coefficients(c, np.linspace(A0, 1.0, T + 1))
+    coefs.append(co)
+    ffac.append(1.5 * c.Omega_m)
+    nsteps.append(T)
+    dims.append((n, n, n, 1))
+  # batched: one plan, one graph
+  plan = Plan(dims)
+  _lib.call('fpm_nbody_set_steps', plan.handle, maxT, _lib.ivec(nsteps),
+            _lib.dvec(np.concatenate(coefs).ravel()), _lib.dvec(ffac), st)
+  D0, P0 = torch.cat(d0s).contiguous(), torch.cat(p0s).contiguous()
+  D, P, F = torch.empty_like(D0), torch.empty_like(P0), torch.empty_like(D0)
+  gr = _lib.ctypes.c_void_p()
+  _lib.call('fpm_graph_capture_nbody', plan.handle, _lib.ptr(D), _lib.ptr(P),
+            _lib.ptr(F), None, 0, None, 0, _lib.ctypes.byref(gr))
+
+  def batched():
+    D.copy_(D0)
+    P.copy_(P0)
+    _lib.call('fpm_graph_launch', gr, st)
+
+  # plain: one simulation at a time through fpm_nbody, no graph
+  singles = []
+  for i, (n, box, c, T, seed) in enumerate(sims):
+    sp = get_plan([(n, n, n, 1)])
+    singles.append((sp, d0s[i], p0s[i], torch.empty_like(d0s[i]),
+                    torch.empty_like(p0s[i]), torch.empty_like(d0s[i]),
+                    coefs[i][:T].ravel(), T, ffac[i]))
+
+  def plain():
+    for sp, d0, p0, d, p, f, co, T, ff in singles:
+      d.copy_(d0)
+      p.copy_(p0)
+      _lib.call('fpm_nbody', sp.handle, _lib.ptr(d), _lib.ptr(p), _lib.ptr(f),
+                T, _lib.ivec([T]), _lib.dvec(co), _lib.dvec([ff]), None, 0, st)
+
+  batched()
+  plain()
+  torch.cuda.synchronize()
+  # same answer both ways
+  off, err = 0, 0.0
+  for sp, d0, p0, d, p, f, co, T, ff in singles:
+    m = d.shape[0]
+    err = max(err, float((D[off:off + m] - d).abs().max()))
+    off += m
+  tb = _timed(batched, reps, flush)
+  tp = _timed(plain, reps, flush)
+  _lib.lib.fpm_graph_destroy(gr)
+  plan.close()
+  nsim = len(sims)
+  return {
+      'workload': 'C3: 8x32^3 + 8x64^3 + 4x128^3, per-sim cosmology, 10-20 '
+                  'steps each',
+      'value': nsim / (tb * 1e-3),
+      'unit': 'sims/s',
+      'plain_sims_per_s': nsim / (tp * 1e-3),
+      'speedup_vs_plain': tp / tb,
+      'batched_ms': tb,
+      'plain_ms': tp,
+      'particles': int(sum(n**3 for n, *_ in sims)),
+      'particle_updates_per_s': float(
+          sum(n**3 * T for n, _, _, T, _ in sims)) / (tb * 1e-3),
+      'max_abs_diff_batched_vs_plain': err,
+  }
 
 
 def main():
@@ -406,6 +636,9 @@ def main():
       'kernel_ms_per_step': kt,
       'clocks': clk.summary(),
   }
+  if world == 1 and not args.no_extras:
+    line['fwd_adjoint'] = measure_fwd_adjoint(fpm, flush, max(args.steps, 3))
+    line['batched'] = measure_batched(fpm, flush, max(args.steps, 3))
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     line['cpu_baseline'] = cpu_baseline()
   _lib.lib.fpm_graph_destroy(graph)
