@@ -42,6 +42,9 @@ WORKLOAD = ('C2: forward PM, 128^3 particles / 128^3 mesh, box 200 Mpc/h, '
 # force meshes (12 Nc) + paint the density (4 Nc) = 64 B per particle.
 STEP_BYTES_PER_PART = 124
 KERNEL_BYTES_PER_PART = 64
+# DRAM bytes (read + write) of one k_step launch at 128^3, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum = 84.0 + 8.4 MB).
+KSTEP_TRAFFIC_BYTES_128 = 92.4e6
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -53,6 +56,8 @@ def parse():
   ap.add_argument('--impl', default='flowpm_b200',
                   choices=['flowpm_b200', 'reference'])
   ap.add_argument('--no-cpu-baseline', action='store_true')
+  ap.add_argument('--c5', action='store_true',
+                  help='also measure the 2 x 512^3 forward + adjoint config')
   ap.add_argument('--no-extras', action='store_true',
                   help='skip the C4 (forward + adjoint) and C3 (batched) '
                   'measurements')
@@ -453,6 +458,144 @@ def measure_batched(fpm, flush, reps):
   }
 
 
+def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
+  """Config C5: two 512^3 simulations (different seeds and cosmologies),
+  box 1000 Mpc/h, 30 steps, forward + reverse-time adjoint with a
+  checkpoint every 5 steps, in one plan.  Reports forward and
+  forward+adjoint particle-updates/s, the per-kernel device time of the
+  forward (event pairs around every launch) and the HBM roofline fraction
+  of the paint, step (readout + kick + drift + paint) and Fourier kernels."""
+  from flowpm_b200 import _lib, tfbackground
+  from flowpm_b200._plans import Plan, clear_plans
+  box = 1000.0
+  cosmos = [fpm.cosmology.Planck15(),
+            fpm.cosmology.Planck15(Omega_c=0.27, sigma8=0.78)]
+  seeds = [5120, 5121]
+  nc = [n] * 3
+  np_ = n**3
+  st = _lib.stream_ptr()
+  d0s, p0s = [], []
+  for c, seed in zip(cosmos, seeds):
+    lin = fpm.linear_field(nc, box, _pk_interp(c), seed=seed)
+    s0 = fpm.lpt_init(c, lin, A0, order=2)
+    d0s.append(fpm.tfpm._to_disp(s0[0], nc).reshape(-1, 3))
+    p0s.append(s0[1].reshape(-1, 3).clone())
+    del lin, s0
+  clear_plans()
+  torch.cuda.empty_cache()
+  D0, P0 = torch.cat(d0s), torch.cat(p0s)
+  del d0s, p0s
+  stages = np.linspace(A0, 1.0, steps + 1)
+  plan = Plan([tuple(nc) + (1,)] * 2, flags=_lib.FPM_PLAN_ADJOINT)
+  coefs = np.concatenate(
+      [tfbackground.nbody_coefficients(c, stages) for c in cosmos])
+  ffac = [1.5 * c.Omega_m for c in cosmos]
+  _lib.call('fpm_nbody_set_steps', plan.handle, steps, _lib.ivec([steps] * 2),
+            _lib.dvec(coefs.ravel()), _lib.dvec(ffac), st)
+  D, P, F = torch.empty_like(D0), torch.empty_like(P0), torch.empty_like(D0)
+  LX, LP = torch.empty_like(D0), torch.empty_like(D0)
+  X = torch.empty_like(D0)
+  ck = torch.empty((steps // ckpt + 1, 2) + tuple(D0.shape), device='cuda')
+  rho = torch.empty((2,) + tuple(nc), device='cuda')
+  g = torch.empty_like(rho)
+  gf, ga = _lib.ctypes.c_void_p(), _lib.ctypes.c_void_p()
+  _lib.call('fpm_graph_capture_nbody', plan.handle, _lib.ptr(D), _lib.ptr(P),
+            _lib.ptr(F), None, 0, _lib.ptr(ck), ckpt, _lib.ctypes.byref(gf))
+  _lib.call('fpm_graph_capture_adjoint', plan.handle, _lib.ptr(D),
+            _lib.ptr(P), _lib.ptr(F), _lib.ptr(LX), _lib.ptr(LP), None,
+            _lib.ptr(ck), ckpt, _lib.ctypes.byref(ga))
+
+  def forward():
+    D.copy_(D0)
+    P.copy_(P0)
+    _lib.call('fpm_graph_launch', gf, st)
+
+  def density():
+    _lib.call('fpm_lattice_shift', _lib.ptr(D), _lib.ptr(X), 2, n, n, n, 1,
+              st)
+    rho.zero_()
+    _lib.call('fpm_cic_paint', _lib.ptr(rho), 2, n, n, n, _lib.ptr(X), np_,
+              None, st)
+
+  forward()
+  density()
+  gen = torch.Generator(device='cuda').manual_seed(99)
+  target = rho + torch.randn(rho.shape, generator=gen, device='cuda')
+  status = plan.status(st)
+
+  def fwd_adj():
+    forward()
+    density()
+    g.copy_(rho)
+    _lib.call('fpm_saxpy', _lib.ptr(g), _lib.ptr(target), -1.0, g.numel(), st)
+    _lib.call('fpm_cic_paint_adjoint', _lib.ptr(g), 2, n, n, n, _lib.ptr(X),
+              np_, None, _lib.ptr(LX), None, st)
+    _lib.call('fpm_saxpy', _lib.ptr(LX), _lib.ptr(LX), 1.0, LX.numel(), st)
+    LP.zero_()
+    _lib.call('fpm_graph_launch', ga, st)
+
+  fwd_adj()
+  t_fwd = _timed(forward, reps, flush)
+  t_all = _timed(fwd_adj, reps, flush)
+  status |= plan.status(st)
+  # per-kernel device time of one forward run, GPU kept busy while enqueued
+  _lib.call('fpm_plan_profile', plan.handle, 1)
+  D.copy_(D0)
+  P.copy_(P0)
+  torch.cuda._sleep(100_000_000)
+  _lib.call('fpm_nbody_run', plan.handle, _lib.ptr(D), _lib.ptr(P),
+            _lib.ptr(F), None, 0, None, 0, st)
+  torch.cuda.synchronize()
+  kt = {}
+  for kind, name in [(0, 'step'), (1, 'fourier'), (2, 'paint')]:
+    tot, cnt = _lib.c_double(), _lib.c_int64()
+    _lib.call('fpm_plan_profile_read', plan.handle, kind,
+              _lib.ctypes.byref(tot), _lib.ctypes.byref(cnt))
+    kt[name] = (tot.value / max(cnt.value, 1), cnt.value)
+  _lib.call('fpm_plan_profile', plan.handle, 0)
+  kb, pk = fpm.power_spectrum(rho, kmin=0.01, dk=0.01, boxsize=[box] * 3)
+  peak, peak_kind = peaks()
+  tot_np, nc_tot = 2 * np_, 2 * np_
+  # algorithmic bytes per launch: step 64 B / particle (Np = Nc), paint
+  # 12 Np + 4 Nc, Fourier read 8 B x half modes + write 3 x 8 B x half modes
+  # + zero 4 Nc
+  half = 2 * n * n * (n // 2 + 1)
+  kbytes = {
+      'step': KERNEL_BYTES_PER_PART * tot_np,
+      'paint': 12 * tot_np + 4 * nc_tot,
+      'fourier': 8 * half + 24 * half + 4 * nc_tot,
+  }
+  roof = {}
+  for k, (ms, cnt) in kt.items():
+    gbs = kbytes[k] / (ms * 1e-3) / 1e9
+    roof[k] = {'avg_launch_ms': ms, 'launches': cnt,
+               'algorithmic_bytes': kbytes[k], 'achieved_gbs': gbs,
+               'frac': gbs / peak}
+  _lib.lib.fpm_graph_destroy(gf)
+  _lib.lib.fpm_graph_destroy(ga)
+  dev_gb = (plan.device_bytes + 7 * D0.numel() * 4 + ck.numel() * 4 +
+            3 * rho.numel() * 4) / 1e9
+  plan.close()
+  upd = 2.0 * np_ * steps
+  return {
+      'workload': 'C5: 2 x 512^3, box 1000 Mpc/h, 30 KDK steps, forward + '
+                  'reverse-time adjoint, checkpoint every %d, different '
+                  'seeds and cosmologies' % ckpt,
+      'forward_value': upd / (t_fwd * 1e-3),
+      'value': upd / (t_all * 1e-3),
+      'unit': 'particle-updates/s (forward + adjoint)',
+      'forward_ms': t_fwd,
+      'forward_adjoint_ms': t_all,
+      'sims_per_s_forward_adjoint': 2 / (t_all * 1e-3),
+      'kernel_roofline': roof,
+      'peak_gbs': peak,
+      'peak_kind': peak_kind,
+      'status': status,
+      'device_gb': dev_gb,
+      'pk_final_first_bins': [float(v) for v in pk[0, :8].cpu()],
+  }
+
+
 def main():
   args = parse()
   rank, world, local = dist_env()
@@ -624,7 +767,7 @@ def main():
           'peak_kind': peak_kind,
           'unit': 'GB/s',
           'frac': achieved / peak,
-          'traffic': None,
+          'traffic': KSTEP_TRAFFIC_BYTES_128 if N_MESH == 128 else None,
           'algorithmic_bytes_per_launch': kbytes,
           'avg_launch_ms': step_ms,
       },
@@ -639,6 +782,8 @@ def main():
   if world == 1 and not args.no_extras:
     line['fwd_adjoint'] = measure_fwd_adjoint(fpm, flush, max(args.steps, 3))
     line['batched'] = measure_batched(fpm, flush, max(args.steps, 3))
+  if world == 1 and args.c5:
+    line['large'] = measure_large(fpm, flush)
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     line['cpu_baseline'] = cpu_baseline()
   _lib.lib.fpm_graph_destroy(graph)
