@@ -398,20 +398,20 @@ def measure_batched(fpm, flush, reps):
     ffac.append(1.5 * c.Omega_m)
     nsteps.append(T)
     dims.append((n, n, n, 1))
-  # batched: one plan, one graph
-  plan = Plan(dims)
-  _lib.call('fpm_nbody_set_steps', plan.handle, maxT, _lib.ivec(nsteps),
-            _lib.dvec(np.concatenate(coefs).ravel()), _lib.dvec(ffac), st)
-  D0, P0 = torch.cat(d0s).contiguous(), torch.cat(p0s).contiguous()
-  D, P, F = torch.empty_like(D0), torch.empty_like(P0), torch.empty_like(D0)
-  gr = _lib.ctypes.c_void_p()
-  _lib.call('fpm_graph_capture_nbody', plan.handle, _lib.ptr(D), _lib.ptr(P),
-            _lib.ptr(F), None, 0, None, 0, _lib.ctypes.byref(gr))
+  # batched: one plan, one graph (public batch API)
+  runner = fpm.BatchRunner([dict(nc=n, cosmo=c, stages=np.linspace(
+      A0, 1.0, T + 1)) for n, box, c, T, seed in sims])
+  states = []
+  for i, (n, box, c, T, seed) in enumerate(sims):
+    s = torch.empty((3, 1, n**3, 3), device='cuda')
+    _lib.call('fpm_lattice_shift', _lib.ptr(d0s[i]), _lib.ptr(s[0]), 1, n, n,
+              n, 1, st)
+    s[1, 0].copy_(p0s[i])
+    states.append(s)
 
   def batched():
-    D.copy_(D0)
-    P.copy_(P0)
-    _lib.call('fpm_graph_launch', gr, st)
+    runner.load(states)
+    runner.run()
 
   # plain: one simulation at a time through fpm_nbody, no graph
   singles = []
@@ -432,15 +432,17 @@ def measure_batched(fpm, flush, reps):
   plain()
   torch.cuda.synchronize()
   # same answer both ways
-  off, err = 0, 0.0
-  for sp, d0, p0, d, p, f, co, T, ff in singles:
-    m = d.shape[0]
-    err = max(err, float((D[off:off + m] - d).abs().max()))
-    off += m
+  err = 0.0
+  for res, (sp, d0, p0, d, p, f, co, T, ff) in zip(runner.results(),
+                                                   singles):
+    n = round(d.shape[0]**(1 / 3))
+    x = torch.empty_like(d)
+    _lib.call('fpm_lattice_shift', _lib.ptr(d), _lib.ptr(x), 1, n, n, n, 1,
+              st)
+    err = max(err, float((res[0, 0] - x).abs().max()))
   tb = _timed(batched, reps, flush)
   tp = _timed(plain, reps, flush)
-  _lib.lib.fpm_graph_destroy(gr)
-  plan.close()
+  runner.close()
   nsim = len(sims)
   return {
       'workload': 'C3: 8x32^3 + 8x64^3 + 4x128^3, per-sim cosmology, 10-20 '

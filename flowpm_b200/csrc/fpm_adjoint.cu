@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                   AdjArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const int s = find_sim(sims, nsims, ch, kPart);
+    const int s = find_sim(sims, nsims, ch, kTraverse);
     const SimDev S = sims[s];
     const int T = a.nsteps[s];
     if (a.it > T) continue;
@@ -88,14 +88,13 @@ k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float* ckd =
         ck ? a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3
            : nullptr;
-    const int64_t base = (ch - S.ch_p) * kChunk + threadIdx.x;
+    const int64_t rel = ch - traverse_first(S);
 #pragma unroll 1
     for (int item = 0; item < kItems; ++item) {
-      const int64_t local = base + item * kThreads;
-      if (local >= S.np) break;
-      const int64_t g = S.p_off + local;
       int i, j, k;
-      lattice_ijk(S, local, i, j, k);
+      int64_t local;
+      if (!traverse_particle(S, rel, item, i, j, k, local)) continue;
+      const int64_t g = S.p_off + local;
       float3 d = ld3(a.disp, g);
       if (a.it < T) {
         const float3 gg = gather_grad(lr, S.mx, S.my, S.mz,
@@ -142,7 +141,7 @@ __global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
           AdjArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const int s = find_sim(sims, nsims, ch, kPart);
+    const int s = find_sim(sims, nsims, ch, kTraverse);
     const SimDev S = sims[s];
     const int T = a.nsteps[s];
     if (a.it > T) continue;
@@ -163,14 +162,13 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
         ck ? a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3 +
                  a.total_np * 3
            : nullptr;
-    const int64_t base = (ch - S.ch_p) * kChunk + threadIdx.x;
+    const int64_t rel = ch - traverse_first(S);
 #pragma unroll 1
     for (int item = 0; item < kItems; ++item) {
-      const int64_t local = base + item * kThreads;
-      if (local >= S.np) break;
-      const int64_t g = S.p_off + local;
       int i, j, k;
-      lattice_ijk(S, local, i, j, k);
+      int64_t local;
+      if (!traverse_particle(S, rel, item, i, j, k, local)) continue;
+      const int64_t g = S.p_off + local;
       const float3 d = ld3(a.disp, g);
       const float3 lp = ld3(a.lam_p, g);
       float3 v = make_float3(cv * lp.x, cv * lp.y, cv * lp.z);

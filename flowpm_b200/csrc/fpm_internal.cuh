@@ -14,6 +14,9 @@ constexpr int kChunk = kThreads * kItems;
 constexpr int kNumSMs = 148;     // B200
 
 // One simulation of a plan, as the device kernels see it.
+// Lattice blocks: kBI x kBJ x kBK = kChunk particles, z fastest.
+constexpr int kBI = 8, kBJ = 8, kBK = 16;
+
 struct SimDev {
   int nx, ny, nz;        // particle lattice (= linear-field mesh)
   int bf;                // force mesh factor
@@ -33,6 +36,9 @@ struct SimDev {
   int64_t ch_m;          // first force-mesh chunk
   int64_t ch_l;          // first lattice-cell chunk
   int64_t ch_ls;         // first lattice-spectrum chunk
+  int64_t ch_b;          // first lattice-block chunk
+  int nbi, nbj, nbk;     // lattice blocks per axis
+  int pad2_;
 };
 
 // Per-axis Fourier tables.  For an axis of n cells and index i,
@@ -46,7 +52,9 @@ struct AxisTabs {
   const float* win;
 };
 
-enum ChunkKind { kPart = 0, kSpec = 1, kMesh = 2, kLat = 3, kLatSpec = 4 };
+enum ChunkKind {
+  kPart = 0, kSpec = 1, kMesh = 2, kLat = 3, kLatSpec = 4, kBlock = 5
+};
 
 __device__ __forceinline__ int64_t chunk_first(const SimDev& s, int kind) {
   switch (kind) {
@@ -54,6 +62,7 @@ __device__ __forceinline__ int64_t chunk_first(const SimDev& s, int kind) {
     case kSpec: return s.ch_s;
     case kMesh: return s.ch_m;
     case kLat: return s.ch_l;
+    case kBlock: return s.ch_b;
     default: return s.ch_ls;
   }
 }
@@ -123,6 +132,9 @@ __device__ __forceinline__ void red_add(float* p, float v) {
 }
 
 // Tuning knobs of the particle kernels (compile-time).
+#ifndef FPM_STEP_BLOCKED
+#define FPM_STEP_BLOCKED 1  // k_step walks 8x8x16 lattice blocks
+#endif
 // Measured on B200 at 128^3: 3 blocks (80 registers) beats 2 (128
 // registers) and 4 (64 registers, spills); the v4 pair reduction is slower
 // than two scalar reductions (33 vs 49 us for 2^21 particles).
@@ -272,6 +284,46 @@ __device__ __forceinline__ void mode_ijl(int64_t local, int ny, int nzh,
   l = (int)(local - t * nzh);
   i = (int)(t / ny);
   j = (int)(t - (int64_t)i * ny);
+}
+
+// Particle t (0 <= t < kChunk) of lattice block `blk` of a sim: lattice
+// coordinates, flat particle index, and whether it exists (edge blocks).
+__device__ __forceinline__ bool block_particle(const SimDev& S, int64_t blk,
+                                               int t, int& i, int& j, int& k,
+                                               int64_t& local) {
+  const int bk = (int)(blk % S.nbk);
+  const int64_t r = blk / S.nbk;
+  const int bj = (int)(r % S.nbj), bi = (int)(r / S.nbj);
+  i = bi * kBI + t / (kBJ * kBK);
+  j = bj * kBJ + (t / kBK) % kBJ;
+  k = bk * kBK + t % kBK;
+  local = ((int64_t)i * S.ny + j) * S.nz + k;
+  return i < S.nx && j < S.ny && k < S.nz;
+}
+
+// Chunk kind and particle enumeration of the particle kernels that gather
+// from or scatter to the meshes (lattice blocks when FPM_STEP_BLOCKED, else
+// 1024 consecutive particles).
+constexpr int kTraverse = FPM_STEP_BLOCKED ? kBlock : kPart;
+
+__device__ __forceinline__ int64_t traverse_first(const SimDev& S) {
+  return FPM_STEP_BLOCKED ? S.ch_b : S.ch_p;
+}
+
+// Item `item` (0 <= item < kItems) of this thread in chunk `rel` (relative
+// to the sim's first chunk): lattice coordinates and flat particle index;
+// false when the particle does not exist.
+__device__ __forceinline__ bool traverse_particle(const SimDev& S, int64_t rel,
+                                                  int item, int& i, int& j,
+                                                  int& k, int64_t& local) {
+#if FPM_STEP_BLOCKED
+  return block_particle(S, rel, threadIdx.x + item * kThreads, i, j, k, local);
+#else
+  local = rel * kChunk + threadIdx.x + item * kThreads;
+  if (local >= S.np) return false;
+  lattice_ijk(S, local, i, j, k);
+  return true;
+#endif
 }
 
 inline unsigned grid_for(int64_t chunks) {

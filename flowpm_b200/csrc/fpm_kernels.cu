@@ -19,15 +19,14 @@ k_paint_lattice(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                 const float* __restrict__ disp, float* __restrict__ rho,
                 int32_t* status) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const SimDev S = sims[find_sim(sims, nsims, ch, kPart)];
-    const int64_t base = (ch - S.ch_p) * kChunk + threadIdx.x;
+    const SimDev S = sims[find_sim(sims, nsims, ch, kTraverse)];
+    const int64_t rel = ch - traverse_first(S);
     float* m = rho + S.m_off;
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
-      const int64_t local = base + it * kThreads;
-      if (local >= S.np) break;
       int i, j, k;
-      lattice_ijk(S, local, i, j, k);
+      int64_t local;
+      if (!traverse_particle(S, rel, it, i, j, k, local)) continue;
       const float3 d = ld3(disp, S.p_off + local);
       const float3 x = mesh_pos(S, i, j, k, d);
       if (!finite3(x.x, x.y, x.z)) atomicOr(status, FPM_STATUS_NONFINITE_POS);
@@ -41,7 +40,7 @@ __global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
        StepArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const int s = find_sim(sims, nsims, ch, kPart);
+    const int s = find_sim(sims, nsims, ch, kTraverse);
     const SimDev S = sims[s];
     const int T = a.nsteps[s];
     if (a.it > T) continue;  // this sim has finished
@@ -55,14 +54,13 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
     const float* f0 = a.fmesh + 3 * S.m_off;
     float* m = a.rho + S.m_off;
-    const int64_t base = (ch - S.ch_p) * kChunk + threadIdx.x;
+    const int64_t rel = ch - traverse_first(S);
 #pragma unroll 1
     for (int it = 0; it < kItems; ++it) {
-      const int64_t local = base + it * kThreads;
-      if (local >= S.np) break;
-      const int64_t g = S.p_off + local;
       int i, j, k;
-      lattice_ijk(S, local, i, j, k);
+      int64_t local;
+      if (!traverse_particle(S, rel, it, i, j, k, local)) continue;
+      const int64_t g = S.p_off + local;
       float3 d = ld3(a.disp, g);
       float3 p = ld3(a.mom, g);
       const float3 x = mesh_pos(S, i, j, k, d);
@@ -113,19 +111,18 @@ k_force_readout(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                 const float* __restrict__ fmesh,
                 const float* __restrict__ ffac, float* __restrict__ force) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const int s = find_sim(sims, nsims, ch, kPart);
+    const int s = find_sim(sims, nsims, ch, kTraverse);
     const SimDev S = sims[s];
     const float fac = ffac[s];
     const float invb = 1.0f / (float)S.bf;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
     const float* f0 = fmesh + 3 * S.m_off;
-    const int64_t base = (ch - S.ch_p) * kChunk + threadIdx.x;
+    const int64_t rel = ch - traverse_first(S);
     for (int it = 0; it < kItems; ++it) {
-      const int64_t local = base + it * kThreads;
-      if (local >= S.np) break;
-      const int64_t g = S.p_off + local;
       int i, j, k;
-      lattice_ijk(S, local, i, j, k);
+      int64_t local;
+      if (!traverse_particle(S, rel, it, i, j, k, local)) continue;
+      const int64_t g = S.p_off + local;
       const float3 x = mesh_pos(S, i, j, k, ld3(disp, g));
       float3 f = readout3(f0, mcells, S.my, S.mz, cic_axis(x.x, S.mx),
                           cic_axis(x.y, S.my), cic_axis(x.z, S.mz));
@@ -149,9 +146,11 @@ __global__ void __launch_bounds__(kThreads)
 k_fourier_force(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                 const float2* __restrict__ dk, float2* __restrict__ fk,
                 float* __restrict__ rho_zero, AxisTabs tabs, double r2,
-                int deconv) {
+                int deconv, const int32_t* __restrict__ nsteps, int pos) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const SimDev S = sims[find_sim(sims, nsims, ch, kSpec)];
+    const int s = find_sim(sims, nsims, ch, kSpec);
+    if (nsteps && pos > nsteps[s]) continue;  // finished simulation
+    const SimDev S = sims[s];
     const int64_t nmodes = (int64_t)S.mx * S.my * S.mzh;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
     // 1 / (nbar N^3) with nbar = Np / N^3 = 1 / bf^3.
@@ -410,10 +409,11 @@ void launch_paint_lattice(const SimDev* sims, int nsims, int64_t nchunks,
 void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
                           const float2* dk, float2* fk, float* rho_zero,
                           AxisTabs tabs, double r_split2, int deconv,
-                          cudaStream_t st) {
+                          const int32_t* nsteps, int pos, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_fourier_force<<<grid_for(nchunks), kThreads, 0, st>>>(
-      sims, nsims, nchunks, dk, fk, rho_zero, tabs, r_split2, deconv);
+      sims, nsims, nchunks, dk, fk, rho_zero, tabs, r_split2, deconv, nsteps,
+      pos);
 }
 
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,

@@ -36,11 +36,12 @@ void launch_paint_lattice(const SimDev* sims, int nsims, int64_t nchunks,
                           cudaStream_t st);
 
 // R2C output -> three force spectra (Green's function * gradient, optional
-// CIC deconvolution and Gaussian long-range window); also zeroes rho.
+// CIC deconvolution and Gaussian long-range window); also zeroes rho.  With
+// nsteps, simulations with nsteps[s] < pos (finished) are skipped.
 void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
                           const float2* dk, float2* fk, float* rho_zero,
                           AxisTabs tabs, double r_split2, int deconv,
-                          cudaStream_t st);
+                          const int32_t* nsteps, int pos, cudaStream_t st);
 
 // Fused readout + kick(end) + kick(start) + drift + paint of one iteration.
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,

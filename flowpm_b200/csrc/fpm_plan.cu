@@ -8,6 +8,7 @@
 // a CUDA graph.
 #include <cufft.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -27,6 +28,11 @@ constexpr int kProfKinds = 3;  // 0 step, 1 fourier force, 2 initial paint
 
 struct Run {
   int first, count;        // simulations [first, first + count)
+  // Simulations of the run still active at leapfrog position it (a prefix
+  // when the run is ordered by non-increasing step count), and the batched
+  // cuFFT plans of each smaller active count.
+  std::vector<int> active;
+  std::map<int, cufftHandle> r2c_n, c2r3_n, r2c3_n, c2r1_n;
   cufftHandle r2c = 0, c2r3 = 0;     // force mesh
   cufftHandle r2c3 = 0, c2r1 = 0;    // force mesh, adjoint
   cufftHandle lr2c = 0, lc2r9 = 0, lc2r3 = 0, lc2r1 = 0;  // lattice
@@ -55,7 +61,7 @@ struct fpm_plan {
   std::vector<Run> runs;
   SimDev* d_sims = nullptr;
   int64_t total_np = 0, total_m = 0, total_s = 0, total_l = 0, total_ls = 0;
-  int64_t ch_p = 0, ch_s = 0, ch_m = 0, ch_l = 0, ch_ls = 0;
+  int64_t ch_p = 0, ch_s = 0, ch_m = 0, ch_l = 0, ch_ls = 0, ch_b = 0;
   // tables
   double* d_kk = nullptr;
   float* d_grad = nullptr;
@@ -87,6 +93,8 @@ struct fpm_plan {
   size_t device_bytes = 0;
   bool steps_set = false;
   int64_t coef_gen = 0;   // bumped whenever d_coefs is reallocated
+  int64_t sched_gen = 0;  // bumped whenever the active-prefix schedule moves
+  size_t work_bytes = 0;  // size of the shared cuFFT work area
   // optional per-kernel timing (fpm_plan_profile)
   bool profile = false;
   std::vector<cudaEvent_t> ev[kProfKinds];
@@ -96,6 +104,11 @@ struct fpm_plan {
 namespace {
 
 AxisTabs tabs_of(const fpm_plan* p) { return AxisTabs{p->d_kk, p->d_grad, p->d_win}; }
+
+// Chunks of the mesh-touching particle kernels (see kTraverse).
+int64_t traverse_chunks(const fpm_plan* p) {
+  return FPM_STEP_BLOCKED ? p->ch_b : p->ch_p;
+}
 
 // Record the next timing event of `kind` on st (no-op unless profiling).
 void prof_mark(fpm_plan* p, int kind, cudaStream_t st) {
@@ -111,6 +124,10 @@ void prof_mark(fpm_plan* p, int kind, cudaStream_t st) {
 
 void destroy_handles(fpm_plan* p) {
   for (auto& r : p->runs) {
+    for (auto* m : {&r.r2c_n, &r.c2r3_n, &r.r2c3_n, &r.c2r1_n}) {
+      for (auto& kv : *m) cufftDestroy(kv.second);
+      m->clear();
+    }
     cufftHandle* hs[] = {&r.r2c,   &r.c2r3,  &r.r2c3,  &r.c2r1, &r.lr2c,
                          &r.lc2r9, &r.lc2r3, &r.lc2r1, &r.lr2c3, &r.lr2c9};
     for (cufftHandle* h : hs)
@@ -204,23 +221,103 @@ int launch_ok() {
     if ((x) != cudaSuccess) return FPM_ERR_CUDA; \
   } while (0)
 
+// Simulations of run r active at position it (all when it < 0).
+int run_active(const Run& r, int it) {
+  if (it < 0 || it >= (int)r.active.size()) return r.count;
+  return r.active[it];
+}
+
+// Plan for `n` of the run's simulations: the full-run plan or the one of
+// the smaller active prefix.
+cufftHandle pick(const Run& r, int n, cufftHandle full,
+                 const std::map<int, cufftHandle>& m) {
+  if (n == r.count) return full;
+  auto it = m.find(n);
+  return it == m.end() ? full : it->second;
+}
+
 // Density of the current positions -> force meshes (paint must be done).
-int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho) {
+// At leapfrog position it (>= 0) only the active prefix of each run is
+// transformed.
+int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
   for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
-    FPM_TRY(exec_r2c(r.r2c, p->rho + S.m_off, p->dk + S.s_off, st));
+    const int n = run_active(r, it);
+    if (n == 0) continue;
+    FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->rho + S.m_off,
+                     p->dk + S.s_off, st));
   }
   prof_mark(p, 1, st);
   launch_fourier_force(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
                        zero_rho ? p->rho : nullptr, tabs_of(p),
                        p->r_split * p->r_split,
-                       (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0, st);
+                       (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0,
+                       it >= 0 ? p->d_nsteps : nullptr, it, st);
   prof_mark(p, 1, st);
   FPM_TRY(launch_ok());
   for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
-    FPM_TRY(exec_c2r(r.c2r3, p->fk + 3 * S.s_off, p->fmesh + 3 * S.m_off, st));
+    const int n = run_active(r, it);
+    if (n == 0) continue;
+    FPM_TRY(exec_c2r(pick(r, n, r.c2r3, r.c2r3_n), p->fk + 3 * S.s_off,
+                     p->fmesh + 3 * S.m_off, st));
   }
+  return FPM_OK;
+}
+
+// Per run and position, the active prefix of the run; batched cuFFT plans
+// for every prefix length used, sharing the plan's work area.
+int update_schedule(fpm_plan* p, int max_steps, const int32_t* nsteps,
+                    cudaStream_t st) {
+  bool changed = false;
+  const bool adj = (p->flags & FPM_PLAN_ADJOINT) != 0;
+  for (auto& r : p->runs) {
+    bool prefix = true;
+    for (int s = r.first + 1; s < r.first + r.count; ++s)
+      if (nsteps[s] > nsteps[s - 1]) prefix = false;
+    std::vector<int> act(max_steps + 1, r.count);
+    if (prefix)
+      for (int it = 0; it <= max_steps; ++it) {
+        int n = 0;
+        while (n < r.count && nsteps[r.first + n] >= it) ++n;
+        act[it] = n;
+      }
+    if (act != r.active) changed = true;
+    r.active = act;
+    const SimDev& S = p->sims[r.first];
+    for (int n : act) {
+      if (n == 0 || n == r.count || r.r2c_n.count(n)) continue;
+      size_t ws = 0;
+      cufftHandle a = 0, b = 0, c = 0, d = 0;
+      int rc = make_plan(&a, S.mx, S.my, S.mz, CUFFT_R2C, n, &ws);
+      if (rc == FPM_OK)
+        rc = make_plan(&b, S.mx, S.my, S.mz, CUFFT_C2R, 3 * n, &ws);
+      if (adj && rc == FPM_OK)
+        rc = make_plan(&c, S.mx, S.my, S.mz, CUFFT_R2C, 3 * n, &ws);
+      if (adj && rc == FPM_OK)
+        rc = make_plan(&d, S.mx, S.my, S.mz, CUFFT_C2R, n, &ws);
+      if (rc == FPM_OK && ws > p->work_bytes) rc = FPM_ERR_UNSUPPORTED;
+      for (cufftHandle h : {a, b, c, d})
+        if (rc == FPM_OK && h && cufftSetWorkArea(h, p->work) != CUFFT_SUCCESS)
+          rc = FPM_ERR_CUFFT;
+      if (rc != FPM_OK) {
+        for (cufftHandle h : {a, b, c, d})
+          if (h) cufftDestroy(h);
+        // fall back to full-run transforms for this run
+        std::fill(r.active.begin(), r.active.end(), r.count);
+        changed = true;
+        break;
+      }
+      r.r2c_n[n] = a;
+      r.c2r3_n[n] = b;
+      if (adj) {
+        r.r2c3_n[n] = c;
+        r.c2r1_n[n] = d;
+      }
+    }
+  }
+  (void)st;
+  if (changed) p->sched_gen++;
   return FPM_OK;
 }
 
@@ -303,6 +400,11 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
     S.ch_m = p->ch_m;
     S.ch_l = p->ch_l;
     S.ch_ls = p->ch_ls;
+    S.nbi = (S.nx + kBI - 1) / kBI;
+    S.nbj = (S.ny + kBJ - 1) / kBJ;
+    S.nbk = (S.nz + kBK - 1) / kBK;
+    S.ch_b = p->ch_b;
+    p->ch_b += (int64_t)S.nbi * S.nbj * S.nbk;
     p->ch_p += (S.np + kChunk - 1) / kChunk;
     p->ch_s += (ns + kChunk - 1) / kChunk;
     p->ch_m += (nm + kChunk - 1) / kChunk;
@@ -401,6 +503,7 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
   if (ws > 0) {
     if (ok && cudaMalloc(&p->work, ws) != cudaSuccess) ok = false;
     if (ok) tot += ws;
+    if (ok) p->work_bytes = ws;
   }
   if (!ok) {
     cudaGetLastError();
@@ -467,11 +570,11 @@ extern "C" int fpm_force(fpm_plan* p, const float* disp,
   cudaStream_t st = (cudaStream_t)stream;
   FPM_TRY(upload_ffac(p, force_fac, st));
   FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
-  launch_paint_lattice(p->d_sims, p->nsims, p->ch_p, disp, p->rho,
+  launch_paint_lattice(p->d_sims, p->nsims, traverse_chunks(p), disp, p->rho,
                        p->d_status, st);
   FPM_TRY(launch_ok());
   FPM_TRY(force_meshes(p, st, false));
-  launch_force_readout(p->d_sims, p->nsims, p->ch_p, disp, p->fmesh,
+  launch_force_readout(p->d_sims, p->nsims, traverse_chunks(p), disp, p->fmesh,
                        p->d_ffac, force, st);
   return launch_ok();
 }
@@ -513,6 +616,7 @@ extern "C" int fpm_nbody_set_steps(fpm_plan* p, int max_steps,
   FPM_TRY(upload_ffac(p, force_fac, st));
   // The uploads read pageable host vectors that die with this call.
   FPM_CUDA(cudaStreamSynchronize(st));
+  FPM_TRY(update_schedule(p, max_steps, nsteps, st));
   p->max_steps = max_steps;
   p->steps_set = true;
   return FPM_OK;
@@ -543,15 +647,15 @@ extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
   a.max_steps = p->max_steps;
   FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
   prof_mark(p, 2, st);
-  launch_paint_lattice(p->d_sims, p->nsims, p->ch_p, disp, p->rho,
+  launch_paint_lattice(p->d_sims, p->nsims, traverse_chunks(p), disp, p->rho,
                        p->d_status, st);
   prof_mark(p, 2, st);
   FPM_TRY(launch_ok());
   for (int it = 0; it <= p->max_steps; ++it) {
-    FPM_TRY(force_meshes(p, st, it < p->max_steps));
+    FPM_TRY(force_meshes(p, st, it < p->max_steps, it));
     a.it = it;
     prof_mark(p, 0, st);
-    launch_step(p->d_sims, p->nsims, p->ch_p, a, st);
+    launch_step(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     prof_mark(p, 0, st);
     FPM_TRY(launch_ok());
   }
@@ -602,26 +706,32 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   for (int it = p->max_steps; it >= 0; --it) {
     a.it = it;
     FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
-    launch_adj_drift_paint(p->d_sims, p->nsims, p->ch_p, a, st);
+    launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     FPM_TRY(launch_ok());
-    FPM_TRY(force_meshes(p, st, false));
+    FPM_TRY(force_meshes(p, st, false, it));
     FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, sizeof(float) * 3 * p->total_m, st));
-    launch_adj_vjp(p->d_sims, p->nsims, p->ch_p, a, st);
+    launch_adj_vjp(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     FPM_TRY(launch_ok());
     for (auto& r : p->runs) {
       const SimDev& S = p->sims[r.first];
-      FPM_TRY(exec_r2c(r.r2c3, p->lmesh + 3 * S.m_off, p->fk + 3 * S.s_off, st));
+      const int n = run_active(r, it);
+      if (n == 0) continue;
+      FPM_TRY(exec_r2c(pick(r, n, r.r2c3, r.r2c3_n), p->lmesh + 3 * S.m_off,
+                       p->fk + 3 * S.s_off, st));
     }
     launch_adj_fourier(p->d_sims, p->nsims, p->ch_s, p->fk, p->dk, tabs_of(p),
                        r2, deconv, st);
     FPM_TRY(launch_ok());
     for (auto& r : p->runs) {
       const SimDev& S = p->sims[r.first];
-      FPM_TRY(exec_c2r(r.c2r1, p->dk + S.s_off, p->lrho + S.m_off, st));
+      const int n = run_active(r, it);
+      if (n == 0) continue;
+      FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->dk + S.s_off,
+                       p->lrho + S.m_off, st));
     }
   }
   a.it = -1;
-  launch_adj_drift_paint(p->d_sims, p->nsims, p->ch_p, a, st);
+  launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
   return launch_ok();
 }
 
@@ -826,6 +936,7 @@ struct fpm_graph {
   cudaGraphExec_t exec = nullptr;
   int max_steps = 0;
   int64_t coef_gen = 0;
+  int64_t sched_gen = 0;
 };
 
 namespace {
@@ -868,6 +979,7 @@ int capture(fpm_plan* p, fpm_graph** out, F&& body) {
   gr->exec = exec;
   gr->max_steps = p->max_steps;
   gr->coef_gen = p->coef_gen;
+  gr->sched_gen = p->sched_gen;
   *out = gr;
   return FPM_OK;
 }
@@ -897,7 +1009,8 @@ extern "C" int fpm_graph_capture_adjoint(fpm_plan* p, float* disp, float* mom,
 
 extern "C" int fpm_graph_launch(fpm_graph* g, void* stream) {
   if (!g || !g->exec) return FPM_ERR_ARG;
-  if (g->plan->max_steps != g->max_steps || g->plan->coef_gen != g->coef_gen)
+  if (g->plan->max_steps != g->max_steps ||
+      g->plan->coef_gen != g->coef_gen || g->plan->sched_gen != g->sched_gen)
     return FPM_ERR_STATE;
   FPM_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
   return FPM_OK;
