@@ -179,10 +179,12 @@ __device__ __forceinline__ bool finite3(float a, float b, float c) {
 // the order of np.indices(nc).reshape(3, -1).T at flowpm/tfpm.py:162).
 __device__ __forceinline__ void lattice_ijk(const SimDev& S, int64_t local,
                                             int& i, int& j, int& k) {
-  const int64_t t = local / S.nz;
-  k = (int)(local - t * S.nz);
-  i = (int)(t / S.ny);
-  j = (int)(t - (int64_t)i * S.ny);
+  // per-simulation indices are < 2^31: 32-bit unsigned division
+  const unsigned l = (unsigned)local;
+  const unsigned t = l / (unsigned)S.nz;
+  k = (int)(l - t * (unsigned)S.nz);
+  i = (int)(t / (unsigned)S.ny);
+  j = (int)(t - (unsigned)i * (unsigned)S.ny);
 }
 
 // Position in force-mesh units: (q + d) * bf, as the reference's
@@ -197,25 +199,56 @@ __device__ __forceinline__ float3 mesh_pos(const SimDev& S, int i, int j,
   return x;
 }
 
+// The 8 CIC neighbours of one position as 4 (x, y) rows of 2 z cells, with
+// 32-bit offsets inside one simulation's mesh (meshes hold < 2^31 cells):
+// neighbour (cx, cy, cz) is m[row[cx + 2 cy] + (cz ? z1 : z0)] with weight
+// (wx * wy) * wz, the reference's product order.
+struct Cic8 {
+  unsigned row[4];
+  unsigned z0, z1;
+  float wxy[4];
+  float wz0, wz1;
+};
+
+__device__ __forceinline__ Cic8 cic8(const Axis& ax, const Axis& ay,
+                                     const Axis& az, int my, int mz) {
+  Cic8 c;
+  const unsigned x0 = (unsigned)ax.i0 * (unsigned)my;
+  const unsigned x1 = (unsigned)ax.i1 * (unsigned)my;
+  c.row[0] = (x0 + (unsigned)ay.i0) * (unsigned)mz;
+  c.row[1] = (x1 + (unsigned)ay.i0) * (unsigned)mz;
+  c.row[2] = (x0 + (unsigned)ay.i1) * (unsigned)mz;
+  c.row[3] = (x1 + (unsigned)ay.i1) * (unsigned)mz;
+  c.z0 = (unsigned)az.i0;
+  c.z1 = (unsigned)az.i1;
+  c.wxy[0] = __fmul_rn(ax.w0, ay.w0);
+  c.wxy[1] = __fmul_rn(ax.w1, ay.w0);
+  c.wxy[2] = __fmul_rn(ax.w0, ay.w1);
+  c.wxy[3] = __fmul_rn(ax.w1, ay.w1);
+  c.wz0 = az.w0;
+  c.wz1 = az.w1;
+  return c;
+}
+
+// Deposit s * W at the 8 neighbours (s = 1: plain paint).
+__device__ __forceinline__ void paint_cic8(float* __restrict__ m,
+                                           const Cic8& c, float s) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float w0 = __fmul_rn(c.wxy[q], c.wz0), w1 = __fmul_rn(c.wxy[q], c.wz1);
+    if (s != 1.f) {
+      w0 = __fmul_rn(s, w0);
+      w1 = __fmul_rn(s, w1);
+    }
+    red_add(m + c.row[q] + c.z0, w0);
+    red_add(m + c.row[q] + c.z1, w1);
+  }
+}
+
 __device__ __forceinline__ void paint8(float* __restrict__ m, int mx, int my,
                                        int mz, const Axis& ax, const Axis& ay,
                                        const Axis& az) {
-  const bool adj = az.i1 == az.i0 + 1;
-  const int64_t n = (int64_t)mx * my * mz;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int cx = q & 1, cy = q >> 1;
-    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0;
-    const float wxy = __fmul_rn(cx ? ax.w1 : ax.w0, cy ? ay.w1 : ay.w0);
-    const int64_t row = ((int64_t)ix * my + iy) * mz;
-    const float w0 = __fmul_rn(wxy, az.w0), w1 = __fmul_rn(wxy, az.w1);
-    if (adj) {
-      red_add_pair(m, n, row + az.i0, w0, w1);
-    } else {
-      red_add(m + row + az.i0, w0);
-      red_add(m + row + az.i1, w1);
-    }
-  }
+  paint_cic8(m, cic8(ax, ay, az, my, mz), 1.f);
 }
 
 // Deposit s * W at the 8 neighbours.
@@ -223,43 +256,37 @@ __device__ __forceinline__ void paint_scaled(float* __restrict__ m, int mx,
                                              int my, int mz, const Axis& ax,
                                              const Axis& ay, const Axis& az,
                                              float s) {
-  const bool adj = az.i1 == az.i0 + 1;
-  const int64_t n = (int64_t)mx * my * mz;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int cx = q & 1, cy = q >> 1;
-    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0;
-    const float wxy = __fmul_rn(cx ? ax.w1 : ax.w0, cy ? ay.w1 : ay.w0);
-    const int64_t row = ((int64_t)ix * my + iy) * mz;
-    const float w0 = __fmul_rn(s, __fmul_rn(wxy, az.w0));
-    const float w1 = __fmul_rn(s, __fmul_rn(wxy, az.w1));
-    if (adj) {
-      red_add_pair(m, n, row + az.i0, w0, w1);
-    } else {
-      red_add(m + row + az.i0, w0);
-      red_add(m + row + az.i1, w1);
-    }
-  }
+  paint_cic8(m, cic8(ax, ay, az, my, mz), s);
 }
 
-// Readout of the three force components at the same 8 neighbours.
+// Readout of the three force components (planes f0, f0 + mcells,
+// f0 + 2 mcells) at the same 8 neighbours.
+__device__ __forceinline__ float3 readout_cic8(const float* __restrict__ f0,
+                                               int64_t mcells,
+                                               const Cic8& c) {
+  const float* f1 = f0 + mcells;
+  const float* f2 = f1 + mcells;
+  float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const unsigned o0 = c.row[q] + c.z0, o1 = c.row[q] + c.z1;
+    const float w0 = __fmul_rn(c.wxy[q], c.wz0);
+    const float w1 = __fmul_rn(c.wxy[q], c.wz1);
+    r0 = __fadd_rn(r0, __fmul_rn(__ldg(f0 + o0), w0));
+    r1 = __fadd_rn(r1, __fmul_rn(__ldg(f1 + o0), w0));
+    r2 = __fadd_rn(r2, __fmul_rn(__ldg(f2 + o0), w0));
+    r0 = __fadd_rn(r0, __fmul_rn(__ldg(f0 + o1), w1));
+    r1 = __fadd_rn(r1, __fmul_rn(__ldg(f1 + o1), w1));
+    r2 = __fadd_rn(r2, __fmul_rn(__ldg(f2 + o1), w1));
+  }
+  return make_float3(r0, r1, r2);
+}
+
 __device__ __forceinline__ float3 readout3(const float* __restrict__ f0,
                                            int64_t mcells, int my, int mz,
                                            const Axis& ax, const Axis& ay,
                                            const Axis& az) {
-  float r0 = 0.f, r1 = 0.f, r2 = 0.f;
-#pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
-    const float w = cic_w(ax, ay, az, cx, cy, cz);
-    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
-              iz = cz ? az.i1 : az.i0;
-    const int64_t o = ((int64_t)ix * my + iy) * mz + iz;
-    r0 = __fadd_rn(r0, __fmul_rn(__ldg(f0 + o), w));
-    r1 = __fadd_rn(r1, __fmul_rn(__ldg(f0 + mcells + o), w));
-    r2 = __fadd_rn(r2, __fmul_rn(__ldg(f0 + 2 * mcells + o), w));
-  }
-  return make_float3(r0, r1, r2);
+  return readout_cic8(f0, mcells, cic8(ax, ay, az, my, mz));
 }
 
 __device__ __forceinline__ float3 ld3(const float* p, int64_t g) {
@@ -280,10 +307,11 @@ __device__ __forceinline__ float3 axpy(float3 a, float s, float3 b) {
 
 __device__ __forceinline__ void mode_ijl(int64_t local, int ny, int nzh,
                                          int& i, int& j, int& l) {
-  const int64_t t = local / nzh;
-  l = (int)(local - t * nzh);
-  i = (int)(t / ny);
-  j = (int)(t - (int64_t)i * ny);
+  const unsigned m = (unsigned)local;
+  const unsigned t = m / (unsigned)nzh;
+  l = (int)(m - t * (unsigned)nzh);
+  i = (int)(t / (unsigned)ny);
+  j = (int)(t - (unsigned)i * (unsigned)ny);
 }
 
 // Particle t (0 <= t < kChunk) of lattice block `blk` of a sim: lattice
@@ -291,10 +319,12 @@ __device__ __forceinline__ void mode_ijl(int64_t local, int ny, int nzh,
 __device__ __forceinline__ bool block_particle(const SimDev& S, int64_t blk,
                                                int t, int& i, int& j, int& k,
                                                int64_t& local) {
-  const int bk = (int)(blk % S.nbk);
-  const int64_t r = blk / S.nbk;
-  const int bj = (int)(r % S.nbj), bi = (int)(r / S.nbj);
-  i = bi * kBI + t / (kBJ * kBK);
+  const unsigned b = (unsigned)blk;
+  const unsigned r = b / (unsigned)S.nbk;
+  const int bk = (int)(b - r * (unsigned)S.nbk);
+  const unsigned bi = r / (unsigned)S.nbj;
+  const int bj = (int)(r - bi * (unsigned)S.nbj);
+  i = (int)bi * kBI + t / (kBJ * kBK);
   j = bj * kBJ + (t / kBK) % kBJ;
   k = bk * kBK + t % kBK;
   local = ((int64_t)i * S.ny + j) * S.nz + k;

@@ -52,7 +52,6 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float fac = a.ffac[s];
     const float invb = 1.0f / (float)S.bf;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
-    const float* f0 = a.fmesh + 3 * S.m_off;
     float* m = a.rho + S.m_off;
     const int64_t rel = ch - traverse_first(S);
 #pragma unroll 1
@@ -66,7 +65,8 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       const float3 x = mesh_pos(S, i, j, k, d);
       const Axis ax = cic_axis(x.x, S.mx), ay = cic_axis(x.y, S.my),
                  az = cic_axis(x.z, S.mz);
-      float3 f = readout3(f0, mcells, S.my, S.mz, ax, ay, az);
+      float3 f = readout_cic8(a.fmesh + 3 * S.m_off, mcells,
+                              cic8(ax, ay, az, S.my, S.mz));
       // force = readout * factor / pm_nc_factor (flowpm/tfpm.py:218, :356)
       f.x = __fmul_rn(__fmul_rn(f.x, fac), invb);
       f.y = __fmul_rn(__fmul_rn(f.y, fac), invb);
@@ -116,7 +116,6 @@ k_force_readout(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float fac = ffac[s];
     const float invb = 1.0f / (float)S.bf;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
-    const float* f0 = fmesh + 3 * S.m_off;
     const int64_t rel = ch - traverse_first(S);
     for (int it = 0; it < kItems; ++it) {
       int i, j, k;
@@ -124,8 +123,10 @@ k_force_readout(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       if (!traverse_particle(S, rel, it, i, j, k, local)) continue;
       const int64_t g = S.p_off + local;
       const float3 x = mesh_pos(S, i, j, k, ld3(disp, g));
-      float3 f = readout3(f0, mcells, S.my, S.mz, cic_axis(x.x, S.mx),
-                          cic_axis(x.y, S.my), cic_axis(x.z, S.mz));
+      float3 f = readout_cic8(
+          fmesh + 3 * S.m_off, mcells,
+          cic8(cic_axis(x.x, S.mx), cic_axis(x.y, S.my), cic_axis(x.z, S.mz),
+               S.my, S.mz));
       f.x = __fmul_rn(__fmul_rn(f.x, fac), invb);
       f.y = __fmul_rn(__fmul_rn(f.y, fac), invb);
       f.z = __fmul_rn(__fmul_rn(f.z, fac), invb);
@@ -194,6 +195,168 @@ k_fourier_force(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
         for (int64_t c = local; c < mcells; c += nmodes)
           rho_zero[S.m_off + c] = 0.f;
       }
+    }
+  }
+}
+
+// Potential spectrum phi_k = delta_k * pre * w(k) with w = lap (0 at k = 0)
+// times the optional Gaussian split and CIC deconvolution: the part of the
+// force transfer function common to the three components.  The 4-point
+// gradient i (8 sin k - sin 2k) / 6 of flowpm/kernels.py:72-76 is applied
+// afterwards in real space, where it is exactly the stencil
+// (8 (phi[x+1] - phi[x-1]) - (phi[x+2] - phi[x-2])) / 12 (k_stencil_grad).
+// Also zeroes rho for the next paint.  Used unchanged (rho_zero = null) for
+// the adjoint, the transfer function being real.
+__global__ void __launch_bounds__(kThreads)
+k_fourier_potential(const SimDev* __restrict__ sims, int nsims,
+                    int64_t nchunks, const float2* dk, float2* out,
+                    float* __restrict__ rho_zero,
+                    AxisTabs tabs, double r2, int deconv,
+                    const int32_t* __restrict__ nsteps, int pos) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kSpec);
+    if (nsteps && pos > nsteps[s]) continue;  // finished simulation
+    const SimDev S = sims[s];
+    const int64_t nmodes = (int64_t)S.mx * S.my * S.mzh;
+    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
+    const float pre = (float)((double)S.bf * S.bf * S.bf / (double)mcells);
+    const double* kkx = tabs.kk + S.tab;
+    const double* kky = kkx + S.mx;
+    const double* kkz = kky + S.my;
+    const float* wx = tabs.win + S.tab;
+    const float* wy = wx + S.mx;
+    const float* wz = wy + S.my;
+    const int64_t base = (ch - S.ch_s) * kChunk + threadIdx.x;
+    const float2* din = dk + S.s_off;
+    float2* o = out + S.s_off;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t local = base + it * kThreads;
+      if (local < nmodes) {
+        int i, j, l;
+        mode_ijl(local, S.my, S.mzh, i, j, l);
+        const double kk = kkx[i] + kky[j] + kkz[l];
+        float w = kk == 0.0 ? 0.f : (float)(1.0 / kk);
+        if (r2 != 0.0) w = __fmul_rn(w, (float)exp(-kk * r2));
+        if (deconv) w = __fmul_rn(w, __fmul_rn(__fmul_rn(wx[i], wy[j]), wz[l]));
+        float2 dv = din[local];
+        dv.x = __fmul_rn(dv.x, pre);
+        dv.y = __fmul_rn(dv.y, pre);
+        o[local] = make_float2(__fmul_rn(dv.x, w), __fmul_rn(dv.y, w));
+      }
+      if (rho_zero) {
+        for (int64_t c = local; c < mcells; c += nmodes)
+          rho_zero[S.m_off + c] = 0.f;
+      }
+    }
+  }
+}
+
+// 4-point central difference along one axis with periodic wrap:
+// (8 (f[+1] - f[-1]) - (f[+2] - f[-2])) / 12.
+__device__ __forceinline__ float stencil4(float m2, float m1, float p1,
+                                          float p2) {
+  return __fmul_rn(__fsub_rn(__fmul_rn(8.f, __fsub_rn(p1, m1)),
+                             __fsub_rn(p2, m2)),
+                   1.0f / 12.0f);
+}
+
+// Three force meshes f_d = D_d phi of each simulation (sim s: planes at
+// fmesh + 3 m_off + d mcells).  With nsteps, finished simulations skip.
+// 32-bit offsets inside a simulation's mesh.
+__global__ void __launch_bounds__(kThreads)
+k_stencil_grad(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+               const float* __restrict__ phi, float* __restrict__ fmesh,
+               const int32_t* __restrict__ nsteps, int pos) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kMesh);
+    if (nsteps && pos > nsteps[s]) continue;
+    const SimDev S = sims[s];
+    const unsigned my = S.my, mz = S.mz, mx = S.mx;
+    const unsigned sx = my * mz, mcells = mx * sx;
+    const float* f = phi + S.m_off;
+    float* o0 = fmesh + 3 * S.m_off;
+    float* o1 = o0 + mcells;
+    float* o2 = o1 + mcells;
+    const unsigned base = (unsigned)(ch - S.ch_m) * kChunk + threadIdx.x;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const unsigned c = base + it * kThreads;
+      if (c >= mcells) break;
+      const unsigned t = c / mz;
+      const unsigned z = c - t * mz;
+      const unsigned x = t / my;
+      const unsigned y = t - x * my;
+      const unsigned rx = c - x * sx;           // y * mz + z
+      const unsigned ry = c - y * mz;           // x * sx + z
+      const unsigned rz = c - z;                // x * sx + y * mz
+      const unsigned xm2 = (x >= 2 ? x - 2 : x + mx - 2) * sx;
+      const unsigned xm1 = (x >= 1 ? x - 1 : x + mx - 1) * sx;
+      const unsigned xp1 = (x + 1 < mx ? x + 1 : x + 1 - mx) * sx;
+      const unsigned xp2 = (x + 2 < mx ? x + 2 : x + 2 - mx) * sx;
+      const unsigned ym2 = (y >= 2 ? y - 2 : y + my - 2) * mz;
+      const unsigned ym1 = (y >= 1 ? y - 1 : y + my - 1) * mz;
+      const unsigned yp1 = (y + 1 < my ? y + 1 : y + 1 - my) * mz;
+      const unsigned yp2 = (y + 2 < my ? y + 2 : y + 2 - my) * mz;
+      const unsigned zm2 = z >= 2 ? z - 2 : z + mz - 2;
+      const unsigned zm1 = z >= 1 ? z - 1 : z + mz - 1;
+      const unsigned zp1 = z + 1 < mz ? z + 1 : z + 1 - mz;
+      const unsigned zp2 = z + 2 < mz ? z + 2 : z + 2 - mz;
+      o0[c] = stencil4(__ldg(f + xm2 + rx), __ldg(f + xm1 + rx),
+                       __ldg(f + xp1 + rx), __ldg(f + xp2 + rx));
+      o1[c] = stencil4(__ldg(f + ym2 + ry), __ldg(f + ym1 + ry),
+                       __ldg(f + yp1 + ry), __ldg(f + yp2 + ry));
+      o2[c] = stencil4(__ldg(f + rz + zm2), __ldg(f + rz + zm1),
+                       __ldg(f + rz + zp1), __ldg(f + rz + zp2));
+    }
+  }
+}
+
+// Adjoint of k_stencil_grad: lphi = sum_d D_d^T lf_d = -sum_d D_d lf_d
+// (the stencil is antisymmetric).
+__global__ void __launch_bounds__(kThreads)
+k_stencil_div(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+              const float* __restrict__ lf, float* __restrict__ lphi,
+              const int32_t* __restrict__ nsteps, int pos) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kMesh);
+    if (nsteps && pos > nsteps[s]) continue;
+    const SimDev S = sims[s];
+    const unsigned my = S.my, mz = S.mz, mx = S.mx;
+    const unsigned sx = my * mz, mcells = mx * sx;
+    const float* l0 = lf + 3 * S.m_off;
+    const float* l1 = l0 + mcells;
+    const float* l2 = l1 + mcells;
+    float* o = lphi + S.m_off;
+    const unsigned base = (unsigned)(ch - S.ch_m) * kChunk + threadIdx.x;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const unsigned c = base + it * kThreads;
+      if (c >= mcells) break;
+      const unsigned t = c / mz;
+      const unsigned z = c - t * mz;
+      const unsigned x = t / my;
+      const unsigned y = t - x * my;
+      const unsigned rx = c - x * sx, ry = c - y * mz, rz = c - z;
+      const unsigned xm2 = (x >= 2 ? x - 2 : x + mx - 2) * sx;
+      const unsigned xm1 = (x >= 1 ? x - 1 : x + mx - 1) * sx;
+      const unsigned xp1 = (x + 1 < mx ? x + 1 : x + 1 - mx) * sx;
+      const unsigned xp2 = (x + 2 < mx ? x + 2 : x + 2 - mx) * sx;
+      const unsigned ym2 = (y >= 2 ? y - 2 : y + my - 2) * mz;
+      const unsigned ym1 = (y >= 1 ? y - 1 : y + my - 1) * mz;
+      const unsigned yp1 = (y + 1 < my ? y + 1 : y + 1 - my) * mz;
+      const unsigned yp2 = (y + 2 < my ? y + 2 : y + 2 - my) * mz;
+      const unsigned zm2 = z >= 2 ? z - 2 : z + mz - 2;
+      const unsigned zm1 = z >= 1 ? z - 1 : z + mz - 1;
+      const unsigned zp1 = z + 1 < mz ? z + 1 : z + 1 - mz;
+      const unsigned zp2 = z + 2 < mz ? z + 2 : z + 2 - mz;
+      const float a = stencil4(__ldg(l0 + xm2 + rx), __ldg(l0 + xm1 + rx),
+                               __ldg(l0 + xp1 + rx), __ldg(l0 + xp2 + rx));
+      const float b = stencil4(__ldg(l1 + ym2 + ry), __ldg(l1 + ym1 + ry),
+                               __ldg(l1 + yp1 + ry), __ldg(l1 + yp2 + ry));
+      const float cz = stencil4(__ldg(l2 + rz + zm2), __ldg(l2 + rz + zm1),
+                                __ldg(l2 + rz + zp1), __ldg(l2 + rz + zp2));
+      o[c] = -((a + b) + cz);
     }
   }
 }
@@ -414,6 +577,33 @@ void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
   k_fourier_force<<<grid_for(nchunks), kThreads, 0, st>>>(
       sims, nsims, nchunks, dk, fk, rho_zero, tabs, r_split2, deconv, nsteps,
       pos);
+}
+
+void launch_fourier_potential(const SimDev* sims, int nsims, int64_t nchunks,
+                              const float2* dk, float2* out, float* rho_zero,
+                              AxisTabs tabs, double r_split2, int deconv,
+                              const int32_t* nsteps, int pos,
+                              cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_fourier_potential<<<grid_for(nchunks), kThreads, 0, st>>>(
+      sims, nsims, nchunks, dk, out, rho_zero, tabs, r_split2, deconv, nsteps,
+      pos);
+}
+
+void launch_stencil_grad(const SimDev* sims, int nsims, int64_t nchunks,
+                         const float* phi, float* fmesh, const int32_t* nsteps,
+                         int pos, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_stencil_grad<<<grid_for(nchunks), kThreads, 0, st>>>(
+      sims, nsims, nchunks, phi, fmesh, nsteps, pos);
+}
+
+void launch_stencil_div(const SimDev* sims, int nsims, int64_t nchunks,
+                        const float* lf, float* lphi, const int32_t* nsteps,
+                        int pos, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_stencil_div<<<grid_for(nchunks), kThreads, 0, st>>>(
+      sims, nsims, nchunks, lf, lphi, nsteps, pos);
 }
 
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,

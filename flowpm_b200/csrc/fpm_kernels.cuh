@@ -43,6 +43,22 @@ void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
                           AxisTabs tabs, double r_split2, int deconv,
                           const int32_t* nsteps, int pos, cudaStream_t st);
 
+// Potential spectrum delta_k * pre * w(k) (one output per sim, layout of
+// dk); also zeroes rho_zero when given.  The adjoint reuses it as is.
+void launch_fourier_potential(const SimDev* sims, int nsims, int64_t nchunks,
+                              const float2* dk, float2* out, float* rho_zero,
+                              AxisTabs tabs, double r_split2, int deconv,
+                              const int32_t* nsteps, int pos, cudaStream_t st);
+
+// f_d = D_d phi with the 4-point stencil (nchunks = mesh chunks), and its
+// adjoint lphi = -sum_d D_d lf_d.
+void launch_stencil_grad(const SimDev* sims, int nsims, int64_t nchunks,
+                         const float* phi, float* fmesh, const int32_t* nsteps,
+                         int pos, cudaStream_t st);
+void launch_stencil_div(const SimDev* sims, int nsims, int64_t nchunks,
+                        const float* lf, float* lphi, const int32_t* nsteps,
+                        int pos, cudaStream_t st);
+
 // Fused readout + kick(end) + kick(start) + drift + paint of one iteration.
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,
                  const StepArgs& a, cudaStream_t st);

@@ -71,6 +71,7 @@ struct fpm_plan {
   float2* dk = nullptr;
   float2* fk = nullptr;
   float* fmesh = nullptr;
+  float* phi = nullptr;     // potential mesh (stencil force path)
   // lattice buffers (FPM_PLAN_LPT)
   float* lreal1 = nullptr;
   float2* lspec1 = nullptr;
@@ -146,7 +147,7 @@ void free_all(fpm_plan* p) {
                   p->dk,     p->fk,     p->fmesh,   p->lreal1,  p->lspec1,
                   p->lspec9, p->lreal9, p->lreal3,  p->d_coefs, p->d_nsteps,
                   p->d_ffac, p->d_lcoef, p->d_status, p->work,
-                  p->lmesh,  p->lrho,   p->fpart};
+                  p->lmesh,  p->lrho,   p->fpart,   p->phi};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -236,10 +237,18 @@ cufftHandle pick(const Run& r, int n, cufftHandle full,
   return it == m.end() ? full : it->second;
 }
 
+// True for the default force path: potential spectrum, one C2R, and the
+// 4-point gradient as a real-space stencil.  The order-0 gradient i k has
+// no finite stencil and keeps three spectra and a batched C2R.
+bool stencil_path(const fpm_plan* p) {
+  return (p->flags & FPM_PLAN_GRAD_ORDER0) == 0;
+}
+
 // Density of the current positions -> force meshes (paint must be done).
 // At leapfrog position it (>= 0) only the active prefix of each run is
 // transformed.
 int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
+  const int32_t* act = it >= 0 ? p->d_nsteps : nullptr;
   for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
     const int n = run_active(r, it);
@@ -248,19 +257,36 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
                      p->dk + S.s_off, st));
   }
   prof_mark(p, 1, st);
-  launch_fourier_force(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
-                       zero_rho ? p->rho : nullptr, tabs_of(p),
-                       p->r_split * p->r_split,
-                       (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0,
-                       it >= 0 ? p->d_nsteps : nullptr, it, st);
+  if (stencil_path(p)) {
+    launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
+                             zero_rho ? p->rho : nullptr, tabs_of(p),
+                             p->r_split * p->r_split,
+                             (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0, act, it,
+                             st);
+  } else {
+    launch_fourier_force(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
+                         zero_rho ? p->rho : nullptr, tabs_of(p),
+                         p->r_split * p->r_split,
+                         (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0, act, it,
+                         st);
+  }
   prof_mark(p, 1, st);
   FPM_TRY(launch_ok());
   for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
     const int n = run_active(r, it);
     if (n == 0) continue;
-    FPM_TRY(exec_c2r(pick(r, n, r.c2r3, r.c2r3_n), p->fk + 3 * S.s_off,
-                     p->fmesh + 3 * S.m_off, st));
+    if (stencil_path(p))
+      FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->fk + S.s_off,
+                       p->phi + S.m_off, st));
+    else
+      FPM_TRY(exec_c2r(pick(r, n, r.c2r3, r.c2r3_n), p->fk + 3 * S.s_off,
+                       p->fmesh + 3 * S.m_off, st));
+  }
+  if (stencil_path(p)) {
+    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, p->phi, p->fmesh, act,
+                        it, st);
+    FPM_TRY(launch_ok());
   }
   return FPM_OK;
 }
@@ -294,7 +320,7 @@ int update_schedule(fpm_plan* p, int max_steps, const int32_t* nsteps,
         rc = make_plan(&b, S.mx, S.my, S.mz, CUFFT_C2R, 3 * n, &ws);
       if (adj && rc == FPM_OK)
         rc = make_plan(&c, S.mx, S.my, S.mz, CUFFT_R2C, 3 * n, &ws);
-      if (adj && rc == FPM_OK)
+      if (rc == FPM_OK)
         rc = make_plan(&d, S.mx, S.my, S.mz, CUFFT_C2R, n, &ws);
       if (rc == FPM_OK && ws > p->work_bytes) rc = FPM_ERR_UNSUPPORTED;
       for (cufftHandle h : {a, b, c, d})
@@ -310,10 +336,8 @@ int update_schedule(fpm_plan* p, int max_steps, const int32_t* nsteps,
       }
       r.r2c_n[n] = a;
       r.c2r3_n[n] = b;
-      if (adj) {
-        r.r2c3_n[n] = c;
-        r.c2r1_n[n] = d;
-      }
+      r.c2r1_n[n] = d;
+      if (adj) r.r2c3_n[n] = c;
     }
   }
   (void)st;
@@ -447,12 +471,10 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
       rc = make_plan(&r.r2c, S.mx, S.my, S.mz, CUFFT_R2C, r.count, &ws);
     if (rc == FPM_OK)
       rc = make_plan(&r.c2r3, S.mx, S.my, S.mz, CUFFT_C2R, 3 * r.count, &ws);
-    if (adj) {
-      if (rc == FPM_OK)
-        rc = make_plan(&r.r2c3, S.mx, S.my, S.mz, CUFFT_R2C, 3 * r.count, &ws);
-      if (rc == FPM_OK)
-        rc = make_plan(&r.c2r1, S.mx, S.my, S.mz, CUFFT_C2R, r.count, &ws);
-    }
+    if (rc == FPM_OK)
+      rc = make_plan(&r.c2r1, S.mx, S.my, S.mz, CUFFT_C2R, r.count, &ws);
+    if (adj && rc == FPM_OK)
+      rc = make_plan(&r.r2c3, S.mx, S.my, S.mz, CUFFT_R2C, 3 * r.count, &ws);
     if (lpt) {
       if (rc == FPM_OK)
         rc = make_plan(&r.lr2c3, S.nx, S.ny, S.nz, CUFFT_R2C, 3 * r.count, &ws);
@@ -484,6 +506,7 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
   p->dk = dalloc<float2>(p->total_s, tot, ok);
   p->fk = dalloc<float2>(3 * p->total_s, tot, ok);
   p->fmesh = dalloc<float>(3 * p->total_m, tot, ok);
+  p->phi = dalloc<float>(p->total_m, tot, ok);
   if (lpt) {
     p->lreal1 = dalloc<float>(p->total_l, tot, ok);
     p->lspec1 = dalloc<float2>(p->total_ls, tot, ok);
@@ -712,16 +735,34 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
     FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, sizeof(float) * 3 * p->total_m, st));
     launch_adj_vjp(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     FPM_TRY(launch_ok());
-    for (auto& r : p->runs) {
-      const SimDev& S = p->sims[r.first];
-      const int n = run_active(r, it);
-      if (n == 0) continue;
-      FPM_TRY(exec_r2c(pick(r, n, r.r2c3, r.r2c3_n), p->lmesh + 3 * S.m_off,
-                       p->fk + 3 * S.s_off, st));
+    const int32_t* act = p->d_nsteps;
+    if (stencil_path(p)) {
+      // lphi = -sum_d D_d lf_d, then lrho = pre C2R(w R2C(lphi))
+      launch_stencil_div(p->d_sims, p->nsims, p->ch_m, p->lmesh, p->phi, act,
+                         it, st);
+      FPM_TRY(launch_ok());
+      for (auto& r : p->runs) {
+        const SimDev& S = p->sims[r.first];
+        const int n = run_active(r, it);
+        if (n == 0) continue;
+        FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->phi + S.m_off,
+                         p->dk + S.s_off, st));
+      }
+      launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->dk,
+                               nullptr, tabs_of(p), r2, deconv, act, it, st);
+      FPM_TRY(launch_ok());
+    } else {
+      for (auto& r : p->runs) {
+        const SimDev& S = p->sims[r.first];
+        const int n = run_active(r, it);
+        if (n == 0) continue;
+        FPM_TRY(exec_r2c(pick(r, n, r.r2c3, r.r2c3_n), p->lmesh + 3 * S.m_off,
+                         p->fk + 3 * S.s_off, st));
+      }
+      launch_adj_fourier(p->d_sims, p->nsims, p->ch_s, p->fk, p->dk,
+                         tabs_of(p), r2, deconv, st);
+      FPM_TRY(launch_ok());
     }
-    launch_adj_fourier(p->d_sims, p->nsims, p->ch_s, p->fk, p->dk, tabs_of(p),
-                       r2, deconv, st);
-    FPM_TRY(launch_ok());
     for (auto& r : p->runs) {
       const SimDev& S = p->sims[r.first];
       const int n = run_active(r, it);

@@ -342,3 +342,47 @@ def test_nbody_many_matches_single_runs(fpm):
   for o, ref in zip(r.results(), singles):
     assert_allclose(host(o), ref, atol=1e-4)
   r.close()
+
+
+def _oracle_force_variant(state, nc, omega_m, order=1, r_split=0.0,
+                          deconv=False):
+  """flowpm/tfpm.py:317-366 force with the Fourier operator options of
+  flowpm/kernels.py: gradient order, Gaussian split, CIC compensation."""
+  s = torch.tensor(state, dtype=torch.float64)
+  B = s.shape[1]
+  rho = opm.cic_paint(torch.zeros([B] + nc, dtype=torch.float64), s[0])
+  dk = opm.r2c3d(rho, norm=nc[0] * nc[1] * nc[2])
+  kvec = opm.fftk(nc, symmetric=False)
+  w = opm.laplace_kernel(kvec) * opm.longrange_kernel(kvec, r_split)
+  if deconv:
+    w = w * opm.cic_compensation(kvec)
+  f = []
+  for d in range(3):
+    kd = opm.gradient_kernel(kvec, d, order=order)
+    forced = opm.c2r3d(dk * torch.as_tensor(w * kd),
+                       norm=nc[0] * nc[1] * nc[2])
+    f.append(opm.cic_readout(forced, s[0]))
+  return (torch.stack(f, dim=2) * 1.5 * omega_m).numpy()
+
+
+@pytest.mark.parametrize('flags,r_split,order,deconv', [
+    (0, 0.0, 1, False), (0, 1.5, 1, False), (1, 0.0, 1, True),
+    (4, 0.0, 0, False), (5, 1.2, 0, True)])
+def test_force_operator_options(fpm, flags, r_split, order, deconv):
+  """The fused Fourier force with the Green's function, the gradient of
+  either order, the CIC deconvolution and the Gaussian long-range split
+  (the plan options) against the oracle built from flowpm/kernels.py."""
+  from flowpm_b200 import _lib
+  from flowpm_b200._plans import Plan
+  l = golden('lpt')
+  c = fpm.cosmology.Planck15()
+  s0 = l['n16_init_o2']
+  plan = Plan([(16, 16, 16, 1)], r_split=r_split, flags=flags)
+  x = torch.tensor(s0[0], device='cuda')
+  d = fpm.tfpm._to_disp(x, [16] * 3)
+  f = torch.empty_like(d)
+  _lib.call('fpm_force', plan.handle, _lib.ptr(d),
+            _lib.dvec([1.5 * c.Omega_m]), _lib.ptr(f), _lib.stream_ptr())
+  ref = _oracle_force_variant(s0, [16] * 3, c.Omega_m, order, r_split, deconv)
+  assert_allclose(host(f)[0], ref[0], atol=2e-5 * np.abs(ref).max())
+  plan.close()
