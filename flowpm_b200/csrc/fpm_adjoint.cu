@@ -88,12 +88,12 @@ k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float* ckd =
         ck ? a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3
            : nullptr;
-    const int64_t rel = ch - traverse_first(S);
+    const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
     for (int item = 0; item < kItems; ++item) {
       int i, j, k;
       int64_t local;
-      if (!traverse_particle(S, rel, item, i, j, k, local)) continue;
+      if (!walk_particle(S, w, item, i, j, k, local)) continue;
       const int64_t g = S.p_off + local;
       float3 d = ld3(a.disp, g);
       if (a.it < T) {
@@ -162,12 +162,12 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
         ck ? a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3 +
                  a.total_np * 3
            : nullptr;
-    const int64_t rel = ch - traverse_first(S);
+    const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
     for (int item = 0; item < kItems; ++item) {
       int i, j, k;
       int64_t local;
-      if (!traverse_particle(S, rel, item, i, j, k, local)) continue;
+      if (!walk_particle(S, w, item, i, j, k, local)) continue;
       const int64_t g = S.p_off + local;
       const float3 d = ld3(a.disp, g);
       const float3 lp = ld3(a.lam_p, g);

@@ -20,13 +20,13 @@ k_paint_lattice(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                 int32_t* status) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const SimDev S = sims[find_sim(sims, nsims, ch, kTraverse)];
-    const int64_t rel = ch - traverse_first(S);
+    const Walk w = walk_chunk(S, ch - traverse_first(S));
     float* m = rho + S.m_off;
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
       int i, j, k;
       int64_t local;
-      if (!traverse_particle(S, rel, it, i, j, k, local)) continue;
+      if (!walk_particle(S, w, it, i, j, k, local)) continue;
       const float3 d = ld3(disp, S.p_off + local);
       const float3 x = mesh_pos(S, i, j, k, d);
       if (!finite3(x.x, x.y, x.z)) atomicOr(status, FPM_STATUS_NONFINITE_POS);
@@ -53,54 +53,74 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float invb = 1.0f / (float)S.bf;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
     float* m = a.rho + S.m_off;
-    const int64_t rel = ch - traverse_first(S);
+    const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
     for (int it = 0; it < kItems; ++it) {
       int i, j, k;
       int64_t local;
-      if (!traverse_particle(S, rel, it, i, j, k, local)) continue;
+      // every lane stays in the loop body (the readout and the paint
+      // exchange cells between lanes); missing particles of edge blocks
+      // only skip their memory accesses
+      const bool valid = walk_particle(S, w, it, i, j, k, local);
       const int64_t g = S.p_off + local;
-      float3 d = ld3(a.disp, g);
-      float3 p = ld3(a.mom, g);
+      float3 d = make_float3(0.f, 0.f, 0.f), p = d;
+      if (valid) {
+        d = ld3(a.disp, g);
+        p = ld3(a.mom, g);
+      }
       const float3 x = mesh_pos(S, i, j, k, d);
-      const Axis ax = cic_axis(x.x, S.mx), ay = cic_axis(x.y, S.my),
-                 az = cic_axis(x.z, S.mz);
-      float3 f = readout_cic8(a.fmesh + 3 * S.m_off, mcells,
-                              cic8(ax, ay, az, S.my, S.mz));
+      const Cic8 c0 = cic8(cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
+                           cic_axis(x.z, S.mz), S.my, S.mz);
+#if FPM_WARP_SHARE
+      float3 f = readout_cic8_shared(a.fmesh + 3 * S.m_off, mcells, c0, valid);
+#else
+      float3 f = valid ? readout_cic8(a.fmesh + 3 * S.m_off, mcells, c0)
+                       : make_float3(0.f, 0.f, 0.f);
+#endif
       // force = readout * factor / pm_nc_factor (flowpm/tfpm.py:218, :356)
       f.x = __fmul_rn(__fmul_rn(f.x, fac), invb);
       f.y = __fmul_rn(__fmul_rn(f.y, fac), invb);
       f.z = __fmul_rn(__fmul_rn(f.z, fac), invb);
       if (a.it >= 1) p = axpy(p, ke, f);  // closing kick of step it-1
-      if (a.ckpt && a.it % a.ckpt_every == 0) {
+      if (valid && a.ckpt && a.it % a.ckpt_every == 0) {
         float* o = a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3;
         st3(o, g, d);
         st3(o + a.total_np * 3, g, p);
       }
-      if (a.inter && a.it >= 1) {
+      if (valid && a.inter && a.it >= 1) {
         float* o = a.inter + (int64_t)(a.it - 1) * 3 * a.total_np * 3;
         st3(o, g,
-            make_float3(__fadd_rn((float)i, d.x), __fadd_rn((float)j, d.y),
-                        __fadd_rn((float)k, d.z)));
+            make_float3(__fadd_rn(index_float(i), d.x),
+                        __fadd_rn(index_float(j), d.y),
+                        __fadd_rn(index_float(k), d.z)));
         st3(o + a.total_np * 3, g, p);
         st3(o + 2 * a.total_np * 3, g, f);
       }
-      if (last) {
-        st3(a.force_out, g, f);
-        st3(a.mom, g, p);
-        if (!finite3(p.x, p.y, p.z) || !finite3(f.x, f.y, f.z))
-          atomicOr(a.status, FPM_STATUS_NONFINITE_MOM);
+      if (last) {  // uniform over the block: one sim per chunk
+        if (valid) {
+          st3(a.force_out, g, f);
+          st3(a.mom, g, p);
+          if (!finite3(p.x, p.y, p.z) || !finite3(f.x, f.y, f.z))
+            atomicOr(a.status, FPM_STATUS_NONFINITE_MOM);
+        }
         continue;
       }
       p = axpy(p, ks, f);  // opening kick of step it
       d = axpy(d, dr, p);  // drift of step it
-      st3(a.mom, g, p);
-      st3(a.disp, g, d);
       const float3 xn = mesh_pos(S, i, j, k, d);
-      if (!finite3(xn.x, xn.y, xn.z))
-        atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
-      paint8(m, S.mx, S.my, S.mz, cic_axis(xn.x, S.mx), cic_axis(xn.y, S.my),
-             cic_axis(xn.z, S.mz));
+      if (valid) {
+        st3(a.mom, g, p);
+        st3(a.disp, g, d);
+        if (!finite3(xn.x, xn.y, xn.z))
+          atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
+      }
+      const Cic8 c1 = cic8(cic_axis(xn.x, S.mx), cic_axis(xn.y, S.my),
+                           cic_axis(xn.z, S.mz), S.my, S.mz);
+#if FPM_WARP_SHARE
+      paint_cic8_shared(m, c1, 1.f, valid);
+#else
+      if (valid) paint_cic8(m, c1, 1.f);
+#endif
     }
   }
 }
@@ -116,11 +136,11 @@ k_force_readout(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float fac = ffac[s];
     const float invb = 1.0f / (float)S.bf;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
-    const int64_t rel = ch - traverse_first(S);
+    const Walk w = walk_chunk(S, ch - traverse_first(S));
     for (int it = 0; it < kItems; ++it) {
       int i, j, k;
       int64_t local;
-      if (!traverse_particle(S, rel, it, i, j, k, local)) continue;
+      if (!walk_particle(S, w, it, i, j, k, local)) continue;
       const int64_t g = S.p_off + local;
       const float3 x = mesh_pos(S, i, j, k, ld3(disp, g));
       float3 f = readout_cic8(

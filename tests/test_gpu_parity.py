@@ -54,6 +54,11 @@ def test_cic_neighbours_bit_exact(fpm, nc):
   pos[:6] = [[0, 0, 0], [nc[0] - 1e-5, 0.5, 1.0], [-1e-7, 3.0, 2.0],
              [nc[0], nc[1], nc[2]], [-nc[0] * 7.25, 1e4, -3e3],
              [0.999999, 1.0000001, 2.5]]
+  # round-half ties, -0, and both sides of the 2^22 limit of the kernels'
+  # exact small-magnitude floor
+  pos[6:10] = [[3.5, -2.5, -0.0], [4194303.5, -4194303.5, 4194304.0],
+               [-4194304.5, 8388607.0, -8388608.0],
+               [-2 * nc[0] + 0.25, 2 * nc[1] - 0.25, -nc[2] - 0.5]]
   pos = pos.astype(np.float32)
   idx, w = fpm.utils.cic_neighbours(pos, nc)
   t = torch.tensor(pos).reshape(1, -1, 3)
