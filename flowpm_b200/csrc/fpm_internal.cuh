@@ -24,7 +24,7 @@ struct SimDev {
   int lzh;               // lattice half-spectrum z extent
   int tab;               // offset of this sim's force-mesh axis tables
   int ltab;              // offset of this sim's lattice axis tables
-  int pad_;
+  int fused;             // force meshes by the fused Fourier solve
   int64_t np;            // particles
   int64_t p_off;         // first particle
   int64_t m_off;         // first force-mesh cell

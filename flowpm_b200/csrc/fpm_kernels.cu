@@ -167,11 +167,13 @@ __global__ void __launch_bounds__(kThreads)
 k_fourier_force(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                 const float2* __restrict__ dk, float2* __restrict__ fk,
                 float* __restrict__ rho_zero, AxisTabs tabs, double r2,
-                int deconv, const int32_t* __restrict__ nsteps, int pos) {
+                int deconv, const int32_t* __restrict__ nsteps, int pos,
+                int skip_fused) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const int s = find_sim(sims, nsims, ch, kSpec);
     if (nsteps && pos > nsteps[s]) continue;  // finished simulation
     const SimDev S = sims[s];
+    if (skip_fused && S.fused) continue;
     const int64_t nmodes = (int64_t)S.mx * S.my * S.mzh;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
     // 1 / (nbar N^3) with nbar = Np / N^3 = 1 / bf^3.
@@ -232,11 +234,13 @@ k_fourier_potential(const SimDev* __restrict__ sims, int nsims,
                     int64_t nchunks, const float2* dk, float2* out,
                     float* __restrict__ rho_zero,
                     AxisTabs tabs, double r2, int deconv,
-                    const int32_t* __restrict__ nsteps, int pos) {
+                    const int32_t* __restrict__ nsteps, int pos,
+                    int skip_fused) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const int s = find_sim(sims, nsims, ch, kSpec);
     if (nsteps && pos > nsteps[s]) continue;  // finished simulation
     const SimDev S = sims[s];
+    if (skip_fused && S.fused) continue;
     const int64_t nmodes = (int64_t)S.mx * S.my * S.mzh;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
     const float pre = (float)((double)S.bf * S.bf * S.bf / (double)mcells);
@@ -287,11 +291,12 @@ __device__ __forceinline__ float stencil4(float m2, float m1, float p1,
 __global__ void __launch_bounds__(kThreads)
 k_stencil_grad(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                const float* __restrict__ phi, float* __restrict__ fmesh,
-               const int32_t* __restrict__ nsteps, int pos) {
+               const int32_t* __restrict__ nsteps, int pos, int skip_fused) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const int s = find_sim(sims, nsims, ch, kMesh);
     if (nsteps && pos > nsteps[s]) continue;
     const SimDev S = sims[s];
+    if (skip_fused && S.fused) continue;
     const unsigned my = S.my, mz = S.mz, mx = S.mx;
     const unsigned sx = my * mz, mcells = mx * sx;
     const float* f = phi + S.m_off;
@@ -592,30 +597,31 @@ void launch_paint_lattice(const SimDev* sims, int nsims, int64_t nchunks,
 void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
                           const float2* dk, float2* fk, float* rho_zero,
                           AxisTabs tabs, double r_split2, int deconv,
-                          const int32_t* nsteps, int pos, cudaStream_t st) {
+                          const int32_t* nsteps, int pos, int skip_fused,
+                          cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_fourier_force<<<grid_for(nchunks), kThreads, 0, st>>>(
       sims, nsims, nchunks, dk, fk, rho_zero, tabs, r_split2, deconv, nsteps,
-      pos);
+      pos, skip_fused);
 }
 
 void launch_fourier_potential(const SimDev* sims, int nsims, int64_t nchunks,
                               const float2* dk, float2* out, float* rho_zero,
                               AxisTabs tabs, double r_split2, int deconv,
-                              const int32_t* nsteps, int pos,
+                              const int32_t* nsteps, int pos, int skip_fused,
                               cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_fourier_potential<<<grid_for(nchunks), kThreads, 0, st>>>(
       sims, nsims, nchunks, dk, out, rho_zero, tabs, r_split2, deconv, nsteps,
-      pos);
+      pos, skip_fused);
 }
 
 void launch_stencil_grad(const SimDev* sims, int nsims, int64_t nchunks,
                          const float* phi, float* fmesh, const int32_t* nsteps,
-                         int pos, cudaStream_t st) {
+                         int pos, int skip_fused, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_stencil_grad<<<grid_for(nchunks), kThreads, 0, st>>>(
-      sims, nsims, nchunks, phi, fmesh, nsteps, pos);
+      sims, nsims, nchunks, phi, fmesh, nsteps, pos, skip_fused);
 }
 
 void launch_stencil_div(const SimDev* sims, int nsims, int64_t nchunks,

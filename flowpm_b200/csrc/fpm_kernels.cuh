@@ -37,27 +37,48 @@ void launch_paint_lattice(const SimDev* sims, int nsims, int64_t nchunks,
 
 // R2C output -> three force spectra (Green's function * gradient, optional
 // CIC deconvolution and Gaussian long-range window); also zeroes rho.  With
-// nsteps, simulations with nsteps[s] < pos (finished) are skipped.
+// nsteps, simulations with nsteps[s] < pos (finished) are skipped, and with
+// skip_fused those whose force meshes come from the fused solve.
 void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
                           const float2* dk, float2* fk, float* rho_zero,
                           AxisTabs tabs, double r_split2, int deconv,
-                          const int32_t* nsteps, int pos, cudaStream_t st);
+                          const int32_t* nsteps, int pos, int skip_fused,
+                          cudaStream_t st);
 
 // Potential spectrum delta_k * pre * w(k) (one output per sim, layout of
 // dk); also zeroes rho_zero when given.  The adjoint reuses it as is.
 void launch_fourier_potential(const SimDev* sims, int nsims, int64_t nchunks,
                               const float2* dk, float2* out, float* rho_zero,
                               AxisTabs tabs, double r_split2, int deconv,
-                              const int32_t* nsteps, int pos, cudaStream_t st);
+                              const int32_t* nsteps, int pos, int skip_fused,
+                              cudaStream_t st);
 
 // f_d = D_d phi with the 4-point stencil (nchunks = mesh chunks), and its
 // adjoint lphi = -sum_d D_d lf_d.
 void launch_stencil_grad(const SimDev* sims, int nsims, int64_t nchunks,
                          const float* phi, float* fmesh, const int32_t* nsteps,
-                         int pos, cudaStream_t st);
+                         int pos, int skip_fused, cudaStream_t st);
 void launch_stencil_div(const SimDev* sims, int nsims, int64_t nchunks,
                         const float* lf, float* lphi, const int32_t* nsteps,
                         int pos, cudaStream_t st);
+
+// Fused Fourier solve (fpm_fft.cu) for meshes with every axis a power of
+// two in [16, 128]: density -> three force meshes (the transfer function of
+// launch_fourier_force) in three kernels over the sims [first, first + n)
+// of one run (equal shapes); also zeroes rho when zero_rho.  dk and fk are
+// the spectrum scratch (R2C layout, fk three spectra per sim).
+bool fft_fused_supported(int nx, int ny, int nz);
+// Once per shape and device before the first launch (twiddle table, shared
+// memory limits).
+int fft_fused_prepare(int nx, int ny, int nz);
+// With the 4-point gradient (grad3 false) the solve produces the potential
+// and takes the gradient with the real-space stencil (phi: potential mesh
+// scratch); with grad3 (order-0 gradient) it transforms three force spectra
+// (fk scratch).
+void launch_fft_force(const SimDev* sims, int first, int n, int nx, int ny,
+                      int nz, float* rho, int zero_rho, float2* dk,
+                      float2* fk, float* fmesh, float* phi, AxisTabs tabs,
+                      double r2, int deconv, bool grad3, cudaStream_t st);
 
 // Fused readout + kick(end) + kick(start) + drift + paint of one iteration.
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,

@@ -28,6 +28,7 @@ constexpr int kProfKinds = 3;  // 0 step, 1 fourier force, 2 initial paint
 
 struct Run {
   int first, count;        // simulations [first, first + count)
+  bool fused = false;      // force meshes by the fused Fourier solve
   // Simulations of the run still active at leapfrog position it (a prefix
   // when the run is ordered by non-increasing step count), and the batched
   // cuFFT plans of each smaller active count.
@@ -249,30 +250,49 @@ bool stencil_path(const fpm_plan* p) {
 // transformed.
 int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
   const int32_t* act = it >= 0 ? p->d_nsteps : nullptr;
+  const double r2 = p->r_split * p->r_split;
+  const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
+  // runs on the fused solve: three launches each, straight to fmesh
+  bool any_cufft = false;
+  prof_mark(p, 1, st);
   for (auto& r : p->runs) {
+    if (!r.fused) {
+      any_cufft = true;
+      continue;
+    }
+    const SimDev& S = p->sims[r.first];
+    const int n = run_active(r, it);
+    if (n == 0) continue;
+    launch_fft_force(p->d_sims, r.first, n, S.mx, S.my, S.mz, p->rho,
+                     zero_rho ? 1 : 0, p->dk, p->fk, p->fmesh, p->phi,
+                     tabs_of(p), r2, deconv, !stencil_path(p), st);
+  }
+  FPM_TRY(launch_ok());
+  if (!any_cufft) {
+    prof_mark(p, 1, st);
+    return FPM_OK;
+  }
+  for (auto& r : p->runs) {
+    if (r.fused) continue;
     const SimDev& S = p->sims[r.first];
     const int n = run_active(r, it);
     if (n == 0) continue;
     FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->rho + S.m_off,
                      p->dk + S.s_off, st));
   }
-  prof_mark(p, 1, st);
   if (stencil_path(p)) {
     launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
-                             zero_rho ? p->rho : nullptr, tabs_of(p),
-                             p->r_split * p->r_split,
-                             (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0, act, it,
-                             st);
+                             zero_rho ? p->rho : nullptr, tabs_of(p), r2,
+                             deconv, act, it, 1, st);
   } else {
     launch_fourier_force(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
-                         zero_rho ? p->rho : nullptr, tabs_of(p),
-                         p->r_split * p->r_split,
-                         (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0, act, it,
-                         st);
+                         zero_rho ? p->rho : nullptr, tabs_of(p), r2, deconv,
+                         act, it, 1, st);
   }
   prof_mark(p, 1, st);
   FPM_TRY(launch_ok());
   for (auto& r : p->runs) {
+    if (r.fused) continue;
     const SimDev& S = p->sims[r.first];
     const int n = run_active(r, it);
     if (n == 0) continue;
@@ -285,7 +305,7 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
   }
   if (stencil_path(p)) {
     launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, p->phi, p->fmesh, act,
-                        it, st);
+                        it, 1, st);
     FPM_TRY(launch_ok());
   }
   return FPM_OK;
@@ -465,6 +485,19 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
   size_t ws = 0;
   const bool lpt = (flags & FPM_PLAN_LPT) != 0;
   const bool adj = (flags & FPM_PLAN_ADJOINT) != 0;
+  for (auto& r : p->runs) {
+    const SimDev& S0 = p->sims[r.first];
+    // the fused kernels move density and force planes as float4
+    bool aligned = true;
+    for (int s = r.first; s < r.first + r.count; ++s)
+      if (p->sims[s].m_off % 4 != 0) aligned = false;
+    if (!(flags & FPM_PLAN_CUFFT) && aligned &&
+        fft_fused_supported(S0.mx, S0.my, S0.mz) &&
+        fft_fused_prepare(S0.mx, S0.my, S0.mz) == FPM_OK) {
+      r.fused = true;
+      for (int s = r.first; s < r.first + r.count; ++s) p->sims[s].fused = 1;
+    }
+  }
   for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
     if (rc == FPM_OK)
@@ -749,7 +782,8 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
                          p->dk + S.s_off, st));
       }
       launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->dk,
-                               nullptr, tabs_of(p), r2, deconv, act, it, st);
+                               nullptr, tabs_of(p), r2, deconv, act, it, 0,
+                               st);
       FPM_TRY(launch_ok());
     } else {
       for (auto& r : p->runs) {

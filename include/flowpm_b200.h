@@ -56,8 +56,12 @@ enum {
                                     buffers on the particle lattice         */
   FPM_PLAN_GRAD_ORDER0 = 1u << 2, /* gradient i*k (order 0) instead of the
                                     4-point finite difference (order 1)   */
-  FPM_PLAN_ADJOINT = 1u << 3     /* also allocate the adjoint buffers and
+  FPM_PLAN_ADJOINT = 1u << 3,    /* also allocate the adjoint buffers and
                                     cuFFT plans (fpm_nbody_adjoint)         */
+  FPM_PLAN_CUFFT = 1u << 4       /* force meshes through cuFFT for every
+                                    mesh shape; by default meshes of 16 to
+                                    128 cells (powers of two) per axis use
+                                    the library's fused Fourier solve       */
 };
 
 /* nbody flags (fpm_nbody). */
