@@ -449,11 +449,19 @@ __device__ __forceinline__ float stencil4f(float m2, float m1, float p1,
 // conj X[M-k], B = X[k] - conj X[M-k], and the inverse M-point DFT of Zc
 // gives x[2m] + i x[2m+1].  The columns kz = 0 and kz = M, real after the y
 // inverse, share one complex column (X[.][0] + i X[.][M]).
-template <int NY, int M, bool GRAD3>
+// Output modes of k_fft_plane_inv.
+enum PlaneOut {
+  kOutStencil = 0,  // potential -> phi, force y and z by the 4-point stencil
+  kOutGrad3 = 1,    // three force spectra -> the three force meshes
+  kOutReal = 2      // one spectrum -> one real mesh (phi)
+};
+
+template <int NY, int M, int MODE>
 __global__ void __launch_bounds__(kPlaneThreads)
 k_fft_plane_inv(const SimDev* __restrict__ sims, int first, int nx,
                 const float2* __restrict__ spec, float* __restrict__ fmesh,
                 float* __restrict__ phi) {
+  constexpr bool GRAD3 = MODE == kOutGrad3;
   extern __shared__ float2 P[];
   constexpr int T = kPlaneThreads;
   constexpr int NZH = M + 1;
@@ -467,16 +475,21 @@ k_fft_plane_inv(const SimDev* __restrict__ sims, int first, int nx,
   const int64_t plane = (int64_t)x * NY * 2 * M;
   const float2* src = spec + (GRAD3 ? 3 * S.s_off + d * nmodes : S.s_off) +
                       (int64_t)x * NY * NZH;
-#pragma unroll 4
-  for (int e = threadIdx.x; e < NY * NZH; e += T) {
-    const int ky = e / NZH, kz = e - ky * NZH;
-    if (kz == M) continue;
-    float2 v = src[e];
-    if (kz == 0) {
-      const float2 xm = src[e + M];
-      v = make_float2(v.x - xm.y, v.y + xm.x);
+  // M columns per row after packing kz = 0 and kz = M into column 0
+  constexpr int NL = NY * M;
+#pragma unroll
+  for (int i = 0; i < (NL + T - 1) / T; ++i) {
+    const int e = threadIdx.x + i * T;
+    if (NL % T == 0 || e < NL) {
+      const int ky = e / M, kz = e % M;
+      const float2* row = src + ky * NZH;
+      float2 v = row[kz];
+      if (kz == 0) {
+        const float2 xm = row[M];
+        v = make_float2(v.x - xm.y, v.y + xm.x);
+      }
+      P[ky * NZH + kz] = v;
     }
-    P[e] = v;
   }
   __syncthreads();
   cols_dft<NY, true, T, M, NZH>(P);
@@ -503,9 +516,10 @@ k_fft_plane_inv(const SimDev* __restrict__ sims, int first, int nx,
   __syncthreads();
   rows_inv<M, T>(P, NY, NZH);
   constexpr int NV = NY * M / 2;  // float4 per plane
-  if (GRAD3) {
-    float4* dst = reinterpret_cast<float4*>(fmesh + 3 * S.m_off + d * mcells +
-                                            plane);
+  if (MODE != kOutStencil) {
+    float4* dst = reinterpret_cast<float4*>(
+        GRAD3 ? fmesh + 3 * S.m_off + d * mcells + plane
+              : phi + S.m_off + plane);
     for (int e = threadIdx.x; e < NV; e += T) {
       const int r = (2 * e) / M, m = (2 * e) % M;
       const float2 a = P[r * NZH + m], b = P[r * NZH + m + 1];
@@ -518,29 +532,24 @@ k_fft_plane_inv(const SimDev* __restrict__ sims, int first, int nx,
   constexpr int RS = 2 * NZH;  // floats per row
   constexpr int NZ = 2 * M;
   const float* f = reinterpret_cast<const float*>(P);
-  float4* ophi = reinterpret_cast<float4*>(phi + S.m_off + plane);
-  float4* oy = reinterpret_cast<float4*>(fmesh + 3 * S.m_off + mcells + plane);
-  float4* oz = reinterpret_cast<float4*>(fmesh + 3 * S.m_off + 2 * mcells +
-                                         plane);
-  for (int e = threadIdx.x; e < NV; e += T) {
-    const int y = (4 * e) / NZ, z0 = (4 * e) % NZ;
+  float* gphi = phi + S.m_off + plane;
+  float* gy = fmesh + 3 * S.m_off + mcells + plane;
+  float* gz = fmesh + 3 * S.m_off + 2 * mcells + plane;
+  // consecutive lanes on consecutive z: conflict-free shared reads,
+  // coalesced stores
+  for (int e = threadIdx.x; e < NY * NZ; e += T) {
+    const int y = e / NZ, z = e % NZ;
     const float* r0 = f + y * RS;
-    const float* rm2 = f + ((y - 2) & (NY - 1)) * RS;
-    const float* rm1 = f + ((y - 1) & (NY - 1)) * RS;
-    const float* rp1 = f + ((y + 1) & (NY - 1)) * RS;
-    const float* rp2 = f + ((y + 2) & (NY - 1)) * RS;
-    float v[4], fy[4], fz[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int z = z0 + q;
-      v[q] = r0[z];
-      fy[q] = stencil4f(rm2[z], rm1[z], rp1[z], rp2[z]);
-      fz[q] = stencil4f(r0[(z - 2) & (NZ - 1)], r0[(z - 1) & (NZ - 1)],
-                        r0[(z + 1) & (NZ - 1)], r0[(z + 2) & (NZ - 1)]);
-    }
-    ophi[e] = make_float4(v[0], v[1], v[2], v[3]);
-    oy[e] = make_float4(fy[0], fy[1], fy[2], fy[3]);
-    oz[e] = make_float4(fz[0], fz[1], fz[2], fz[3]);
+    const float v = r0[z];
+    const float fy = stencil4f(f[((y - 2) & (NY - 1)) * RS + z],
+                               f[((y - 1) & (NY - 1)) * RS + z],
+                               f[((y + 1) & (NY - 1)) * RS + z],
+                               f[((y + 2) & (NY - 1)) * RS + z]);
+    const float fz = stencil4f(r0[(z - 2) & (NZ - 1)], r0[(z - 1) & (NZ - 1)],
+                               r0[(z + 1) & (NZ - 1)], r0[(z + 2) & (NZ - 1)]);
+    gphi[e] = v;
+    gy[e] = fy;
+    gz[e] = fz;
   }
 }
 
@@ -584,10 +593,13 @@ int set_plane_smem() {
   if (cudaFuncSetAttribute(k_fft_plane_fwd<NY, M>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(k_fft_plane_inv<NY, M, false>,
+      cudaFuncSetAttribute(k_fft_plane_inv<NY, M, kOutStencil>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(k_fft_plane_inv<NY, M, true>,
+      cudaFuncSetAttribute(k_fft_plane_inv<NY, M, kOutGrad3>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(k_fft_plane_inv<NY, M, kOutReal>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            bytes) != cudaSuccess) {
     cudaGetLastError();
@@ -617,7 +629,7 @@ template <int NY, int M>
 void launch_shape(const SimDev* sims, int first, int n, int nx, float* rho,
                   int zero_rho, float2* dk, float2* fk, float* fmesh,
                   float* phi, AxisTabs tabs, double r2, int deconv, bool grad3,
-                  cudaStream_t st) {
+                  bool real_out, cudaStream_t st) {
   const size_t smem = (size_t)NY * (M + 1) * sizeof(float2);
   k_fft_plane_fwd<NY, M><<<n * nx, kPlaneThreads, smem, st>>>(
       sims, first, nx, rho, dk, zero_rho);
@@ -639,11 +651,16 @@ void launch_shape(const SimDev* sims, int first, int n, int nx, float* rho,
 #undef FPM_COL_CASE
   }
   if (grad3) {
-    k_fft_plane_inv<NY, M, true><<<n * nx * 3, kPlaneThreads, smem, st>>>(
+    k_fft_plane_inv<NY, M, kOutGrad3><<<n * nx * 3, kPlaneThreads, smem, st>>>(
         sims, first, nx, fk, fmesh, phi);
     return;
   }
-  k_fft_plane_inv<NY, M, false><<<n * nx, kPlaneThreads, smem, st>>>(
+  if (real_out) {  // potential of `rho` -> phi
+    k_fft_plane_inv<NY, M, kOutReal><<<n * nx, kPlaneThreads, smem, st>>>(
+        sims, first, nx, dk, nullptr, phi);
+    return;
+  }
+  k_fft_plane_inv<NY, M, kOutStencil><<<n * nx, kPlaneThreads, smem, st>>>(
       sims, first, nx, dk, fmesh, phi);
   const int64_t quads = (int64_t)nx * NY * 2 * M / 4;
   int64_t bx = (quads + kFftThreads - 1) / kFftThreads;
@@ -657,12 +674,12 @@ template <int NY>
 void launch_ny(int M, const SimDev* sims, int first, int n, int nx,
                float* rho, int zero_rho, float2* dk, float2* fk, float* fmesh,
                float* phi, AxisTabs tabs, double r2, int deconv, bool grad3,
-               cudaStream_t st) {
+               bool real_out, cudaStream_t st) {
   switch (M) {
 #define FPM_SHAPE_CASE(MM)                                                  \
   case MM:                                                                  \
     launch_shape<NY, MM>(sims, first, n, nx, rho, zero_rho, dk, fk, fmesh,  \
-                         phi, tabs, r2, deconv, grad3, st);                 \
+                         phi, tabs, r2, deconv, grad3, real_out, st);       \
     break;
     FPM_FFT_HALF(FPM_SHAPE_CASE)
 #undef FPM_SHAPE_CASE
@@ -718,7 +735,25 @@ void launch_fft_force(const SimDev* sims, int first, int n, int nx, int ny,
 #define FPM_NY_CASE(NN)                                                      \
   case NN:                                                                   \
     launch_ny<NN>(nz / 2, sims, first, n, nx, rho, zero_rho, dk, fk, fmesh,  \
-                  phi, tabs, r2, deconv, grad3, st);                         \
+                  phi, tabs, r2, deconv, grad3, false, st);                  \
+    break;
+    FPM_FFT_SIZES(FPM_NY_CASE)
+#undef FPM_NY_CASE
+  }
+}
+
+void launch_fft_potential(const SimDev* sims, int first, int n, int nx,
+                          int ny, int nz, const float* in, float2* dk,
+                          float* out, AxisTabs tabs, double r2, int deconv,
+                          cudaStream_t st) {
+  if (n <= 0) return;
+  g_launches.fetch_add(3, std::memory_order_relaxed);
+  float* src = const_cast<float*>(in);  // read only (zero_rho = 0)
+  switch (ny) {
+#define FPM_NY_CASE(NN)                                                   \
+  case NN:                                                                \
+    launch_ny<NN>(nz / 2, sims, first, n, nx, src, 0, dk, nullptr,        \
+                  nullptr, out, tabs, r2, deconv, false, true, st);       \
     break;
     FPM_FFT_SIZES(FPM_NY_CASE)
 #undef FPM_NY_CASE

@@ -79,6 +79,13 @@ void launch_fft_force(const SimDev* sims, int first, int n, int nx, int ny,
                       int nz, float* rho, int zero_rho, float2* dk,
                       float2* fk, float* fmesh, float* phi, AxisTabs tabs,
                       double r2, int deconv, bool grad3, cudaStream_t st);
+// out = C2R(pre * w(k) * R2C(in)) for the sims [first, first + n) of one
+// run (the adjoint's density cotangent from the potential cotangent); in is
+// only read.
+void launch_fft_potential(const SimDev* sims, int first, int n, int nx,
+                          int ny, int nz, const float* in, float2* dk,
+                          float* out, AxisTabs tabs, double r2, int deconv,
+                          cudaStream_t st);
 
 // Fused readout + kick(end) + kick(start) + drift + paint of one iteration.
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,

@@ -774,15 +774,25 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
       launch_stencil_div(p->d_sims, p->nsims, p->ch_m, p->lmesh, p->phi, act,
                          it, st);
       FPM_TRY(launch_ok());
+      bool any_cufft = false;
       for (auto& r : p->runs) {
         const SimDev& S = p->sims[r.first];
         const int n = run_active(r, it);
         if (n == 0) continue;
+        if (r.fused) {  // lrho straight from lphi
+          launch_fft_potential(p->d_sims, r.first, n, S.mx, S.my, S.mz,
+                               p->phi, p->dk, p->lrho, tabs_of(p), r2, deconv,
+                               st);
+          continue;
+        }
+        any_cufft = true;
         FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->phi + S.m_off,
                          p->dk + S.s_off, st));
       }
+      FPM_TRY(launch_ok());
+      if (!any_cufft) continue;
       launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->dk,
-                               nullptr, tabs_of(p), r2, deconv, act, it, 0,
+                               nullptr, tabs_of(p), r2, deconv, act, it, 1,
                                st);
       FPM_TRY(launch_ok());
     } else {
@@ -800,7 +810,7 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
     for (auto& r : p->runs) {
       const SimDev& S = p->sims[r.first];
       const int n = run_active(r, it);
-      if (n == 0) continue;
+      if (n == 0 || (r.fused && stencil_path(p))) continue;
       FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->dk + S.s_off,
                        p->lrho + S.m_off, st));
     }
