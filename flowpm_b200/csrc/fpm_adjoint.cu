@@ -156,7 +156,7 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float uf = fac * invb;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
     const float* f0 = a.fmesh + 3 * S.m_off;
-    float* l0 = a.lmesh + 3 * S.m_off;
+    float* l0 = a.lmesh + (a.lvec4 ? 4 : 3) * S.m_off;
     const bool ck = !last && a.ckpt && (a.it % a.ckpt_every == 0);
     const float* ckp =
         ck ? a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3 +
@@ -200,9 +200,13 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
         r2 = __fadd_rn(r2, __fmul_rn(a2, w));
         grad_acc(ax, ay, az, dx, dy, dz, cx, cy, cz,
                  v.x * a0 + v.y * a1 + v.z * a2, acc);
-        red_add(l0 + o, u0 * w);
-        red_add(l0 + mcells + o, u1 * w);
-        red_add(l0 + 2 * mcells + o, u2 * w);
+        if (a.lvec4) {  // one 16-byte reduction for the three components
+          red_add_v4(l0 + 4 * o, u0 * w, u1 * w, u2 * w);
+        } else {
+          red_add(l0 + o, u0 * w);
+          red_add(l0 + mcells + o, u1 * w);
+          red_add(l0 + 2 * mcells + o, u2 * w);
+        }
       }
       const float3 f = make_float3(__fmul_rn(__fmul_rn(r0, fac), invb),
                                    __fmul_rn(__fmul_rn(r1, fac), invb),

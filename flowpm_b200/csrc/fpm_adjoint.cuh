@@ -14,7 +14,11 @@ struct AdjArgs {
   const float* lam_f;     // (total_np, 3) dL/dF at the final position or null
   const float* fmesh;     // forward force meshes at the current position
   const float* lrho;      // adjoint density mesh of the previous position
-  float* lmesh;           // three adjoint force meshes (scatter target)
+  float* lmesh;           // adjoint force meshes (scatter target): with
+                          // lvec4 one float4 (x, y, z, 0) per cell (sim s
+                          // at lmesh + 4 m_off), else three planes
+                          // (lmesh + 3 m_off + d mcells)
+  int lvec4;
   float* rho;             // density target of the paint
   const float* coefs;     // (nsims, max_steps, 3) {kick_start, drift, kick_end}
   const float* ffac;      // (nsims)

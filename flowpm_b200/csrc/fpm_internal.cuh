@@ -176,6 +176,15 @@ __device__ __forceinline__ void red_add(float* p, float v) {
   asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }
 
+// p[0..2] += (a, b, c) as one 16-byte vector reduction (p 16-byte aligned;
+// p[3] += 0).
+__device__ __forceinline__ void red_add_v4(float* p, float a, float b,
+                                           float c) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p),
+               "f"(a), "f"(b), "f"(c), "f"(0.f)
+               : "memory");
+}
+
 // Tuning knobs of the particle kernels (compile-time).
 #ifndef FPM_STEP_BLOCKED
 #define FPM_STEP_BLOCKED 1  // k_step walks 8x8x16 lattice blocks

@@ -338,7 +338,8 @@ k_stencil_grad(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 }
 
 // Adjoint of k_stencil_grad: lphi = sum_d D_d^T lf_d = -sum_d D_d lf_d
-// (the stencil is antisymmetric).
+// (the stencil is antisymmetric).  lf holds one float4 (lf_x, lf_y, lf_z, 0)
+// per cell (the vector-reduction target of the readout adjoint).
 __global__ void __launch_bounds__(kThreads)
 k_stencil_div(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
               const float* __restrict__ lf, float* __restrict__ lphi,
@@ -349,9 +350,7 @@ k_stencil_div(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const SimDev S = sims[s];
     const unsigned my = S.my, mz = S.mz, mx = S.mx;
     const unsigned sx = my * mz, mcells = mx * sx;
-    const float* l0 = lf + 3 * S.m_off;
-    const float* l1 = l0 + mcells;
-    const float* l2 = l1 + mcells;
+    const float* l4 = lf + 4 * S.m_off;  // (x, y, z, 0) per cell
     float* o = lphi + S.m_off;
     const unsigned base = (unsigned)(ch - S.ch_m) * kChunk + threadIdx.x;
 #pragma unroll
@@ -375,12 +374,15 @@ k_stencil_div(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       const unsigned zm1 = z >= 1 ? z - 1 : z + mz - 1;
       const unsigned zp1 = z + 1 < mz ? z + 1 : z + 1 - mz;
       const unsigned zp2 = z + 2 < mz ? z + 2 : z + 2 - mz;
-      const float a = stencil4(__ldg(l0 + xm2 + rx), __ldg(l0 + xm1 + rx),
-                               __ldg(l0 + xp1 + rx), __ldg(l0 + xp2 + rx));
-      const float b = stencil4(__ldg(l1 + ym2 + ry), __ldg(l1 + ym1 + ry),
-                               __ldg(l1 + yp1 + ry), __ldg(l1 + yp2 + ry));
-      const float cz = stencil4(__ldg(l2 + rz + zm2), __ldg(l2 + rz + zm1),
-                                __ldg(l2 + rz + zp1), __ldg(l2 + rz + zp2));
+      const float a =
+          stencil4(__ldg(l4 + 4 * (xm2 + rx)), __ldg(l4 + 4 * (xm1 + rx)),
+                   __ldg(l4 + 4 * (xp1 + rx)), __ldg(l4 + 4 * (xp2 + rx)));
+      const float b = stencil4(
+          __ldg(l4 + 4 * (ym2 + ry) + 1), __ldg(l4 + 4 * (ym1 + ry) + 1),
+          __ldg(l4 + 4 * (yp1 + ry) + 1), __ldg(l4 + 4 * (yp2 + ry) + 1));
+      const float cz = stencil4(
+          __ldg(l4 + 4 * (rz + zm2) + 2), __ldg(l4 + 4 * (rz + zm1) + 2),
+          __ldg(l4 + 4 * (rz + zp1) + 2), __ldg(l4 + 4 * (rz + zp2) + 2));
       o[c] = -((a + b) + cz);
     }
   }

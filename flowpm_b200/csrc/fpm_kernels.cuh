@@ -54,7 +54,7 @@ void launch_fourier_potential(const SimDev* sims, int nsims, int64_t nchunks,
                               cudaStream_t st);
 
 // f_d = D_d phi with the 4-point stencil (nchunks = mesh chunks), and its
-// adjoint lphi = -sum_d D_d lf_d.
+// adjoint lphi = -sum_d D_d lf_d (lf interleaved: float4 per cell).
 void launch_stencil_grad(const SimDev* sims, int nsims, int64_t nchunks,
                          const float* phi, float* fmesh, const int32_t* nsteps,
                          int pos, int skip_fused, cudaStream_t st);

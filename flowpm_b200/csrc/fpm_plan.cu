@@ -80,7 +80,8 @@ struct fpm_plan {
   float* lreal9 = nullptr;
   float* lreal3 = nullptr;
   // adjoint buffers (FPM_PLAN_ADJOINT)
-  float* lmesh = nullptr;   // 3 adjoint force meshes
+  float* lmesh = nullptr;   // adjoint force meshes (float4 per cell on the
+                            // stencil path, else 3 planes)
   float* lrho = nullptr;    // adjoint density mesh
   float* fpart = nullptr;   // per-particle force of the reverse sweep
   // parameters
@@ -548,7 +549,7 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
     p->lreal3 = dalloc<float>(3 * p->total_l, tot, ok);
   }
   if (adj) {
-    p->lmesh = dalloc<float>(3 * p->total_m, tot, ok);
+    p->lmesh = dalloc<float>((stencil_path(p) ? 4 : 3) * p->total_m, tot, ok);
     p->lrho = dalloc<float>(p->total_m, tot, ok);
     p->fpart = dalloc<float>(3 * p->total_np, tot, ok);
   }
@@ -748,6 +749,7 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   a.fmesh = p->fmesh;
   a.lrho = p->lrho;
   a.lmesh = p->lmesh;
+  a.lvec4 = stencil_path(p) ? 1 : 0;
   a.rho = p->rho;
   a.coefs = p->d_coefs;
   a.ffac = p->d_ffac;
@@ -765,7 +767,9 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
     launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     FPM_TRY(launch_ok());
     FPM_TRY(force_meshes(p, st, false, it));
-    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, sizeof(float) * 3 * p->total_m, st));
+    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0,
+                             sizeof(float) * (a.lvec4 ? 4 : 3) * p->total_m,
+                             st));
     launch_adj_vjp(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     FPM_TRY(launch_ok());
     const int32_t* act = p->d_nsteps;
