@@ -16,6 +16,7 @@ from .utils import cic_paint, cic_readout, r2c3d, c2r3d, white_noise
 from .tfpm import nbody, linear_field, lpt_init
 from .pk import power_spectrum
 from .batch import BatchRunner, nbody_many
+from .stream import NBodyStream, nbody_stream
 from ._plans import clear_plans
 
 __version__ = '0.1.0'

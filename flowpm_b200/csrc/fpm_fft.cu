@@ -280,7 +280,10 @@ __device__ __forceinline__ void cols_dft(float2* P) {
 // together as column 0 = X[.][0] + i X[.][M] and are separated on the way
 // out (Y0 = (C[ky] + conj C[-ky]) / 2, YM = (C[ky] - conj C[-ky]) / 2i), so
 // the y pass covers M columns.
-constexpr int kPlaneThreads = 512;  // threads of the plane kernels
+#ifndef FPM_PLANE_THREADS
+#define FPM_PLANE_THREADS 512
+#endif
+constexpr int kPlaneThreads = FPM_PLANE_THREADS;  // threads of the plane kernels
 
 template <int NY, int M>
 __global__ void __launch_bounds__(kPlaneThreads)
