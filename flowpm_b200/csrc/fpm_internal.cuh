@@ -191,7 +191,11 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 #endif
 // Measured on B200 at 128^3: 3 blocks (80 registers) beats 2 (128
 // registers) and 4 (64 registers, spills); the v4 pair reduction is slower
-// than two scalar reductions (33 vs 49 us for 2^21 particles).
+// than two scalar reductions (33 vs 49 us for 2^21 particles).  Painting
+// after the readout phase of the whole block, directly or through a
+// shared-memory tile of the block's cells, was slower (103 and 144 vs 87 us
+// per step): the paint's reductions overlap the readout's gathers best when
+// each warp issues both, particle by particle.
 #ifndef FPM_STEP_MINBLOCKS
 #define FPM_STEP_MINBLOCKS 3   // resident blocks of 256 threads per SM
 #endif
@@ -334,102 +338,6 @@ __device__ __forceinline__ float3 readout_cic8(const float* __restrict__ f0,
     r2 = __fadd_rn(r2, __fmul_rn(__ldg(f2 + o1), w1));
   }
   return make_float3(r0, r1, r2);
-}
-
-// ---------------------------------------------------------------------------
-// Lane sharing of z-adjacent cells.  The particle kernels hand consecutive
-// lattice particles along z to consecutive lanes, and at pm_nc_factor 1 the
-// upper z cells (row, z1) of lane t are usually the lower cells (row, z0) of
-// lane t + 1.  When they are the same cells, lane t takes its upper readout
-// values from lane t + 1 by a shuffle instead of loading them again, and
-// hands its upper paint weights to lane t + 1, which deposits them together
-// with its own: half the loads and half the L2 reductions in the common
-// case, the plain path otherwise.  The readout sum keeps its order, so the
-// shared readout is bit-identical to readout_cic8.  All 32 lanes must call
-// these helpers (invalid lanes with valid = false).  Measured on B200 at
-// 128^3 and 256^3: no faster than the plain path (the step is limited by
-// the spread of its reductions over L2 sectors once particles cluster, not
-// by their number), so it is off by default.
-// ---------------------------------------------------------------------------
-#ifndef FPM_WARP_SHARE
-#define FPM_WARP_SHARE 0
-#endif
-
-constexpr unsigned kFullMask = 0xffffffffu;
-
-// Flat cell index of neighbour (0, 0, 0) / (0, 0, 1); never equal for an
-// invalid lane (cell indices are < 2^31).
-__device__ __forceinline__ unsigned cic_key0(const Cic8& c, bool valid) {
-  return valid ? c.row[0] + c.z0 : 0xffffffffu;
-}
-__device__ __forceinline__ unsigned cic_key1(const Cic8& c, bool valid) {
-  return valid ? c.row[0] + c.z1 : 0xfffffffeu;
-}
-
-// True when this lane's upper cells are the next lane's lower cells (same
-// (x0, y0) cell, hence the same 4 rows, and z1 == next z0).
-__device__ __forceinline__ bool next_shares(const Cic8& c, bool valid) {
-  const unsigned nxt = __shfl_down_sync(kFullMask, cic_key0(c, valid), 1);
-  return (threadIdx.x & 31) != 31 && cic_key1(c, valid) == nxt;
-}
-
-__device__ __forceinline__ float3 readout_cic8_shared(
-    const float* __restrict__ f0, int64_t mcells, const Cic8& c, bool valid) {
-  const bool share = next_shares(c, valid);
-  const float* f1 = f0 + mcells;
-  const float* f2 = f1 + mcells;
-  float r0 = 0.f, r1 = 0.f, r2 = 0.f;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const unsigned o0 = c.row[q] + c.z0, o1 = c.row[q] + c.z1;
-    const float w0 = __fmul_rn(c.wxy[q], c.wz0);
-    const float w1 = __fmul_rn(c.wxy[q], c.wz1);
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-    if (valid) {
-      a0 = __ldg(f0 + o0);
-      a1 = __ldg(f1 + o0);
-      a2 = __ldg(f2 + o0);
-    }
-    float b0 = __shfl_down_sync(kFullMask, a0, 1);
-    float b1 = __shfl_down_sync(kFullMask, a1, 1);
-    float b2 = __shfl_down_sync(kFullMask, a2, 1);
-    if (valid && !share) {
-      b0 = __ldg(f0 + o1);
-      b1 = __ldg(f1 + o1);
-      b2 = __ldg(f2 + o1);
-    }
-    r0 = __fadd_rn(r0, __fmul_rn(a0, w0));
-    r1 = __fadd_rn(r1, __fmul_rn(a1, w0));
-    r2 = __fadd_rn(r2, __fmul_rn(a2, w0));
-    r0 = __fadd_rn(r0, __fmul_rn(b0, w1));
-    r1 = __fadd_rn(r1, __fmul_rn(b1, w1));
-    r2 = __fadd_rn(r2, __fmul_rn(b2, w1));
-  }
-  return make_float3(r0, r1, r2);
-}
-
-// Deposit s * W at the 8 neighbours, the upper cells through the next lane
-// when it shares them.
-__device__ __forceinline__ void paint_cic8_shared(float* __restrict__ m,
-                                                  const Cic8& c, float s,
-                                                  bool valid) {
-  const bool share = next_shares(c, valid);
-  const bool from_prev =
-      __shfl_up_sync(kFullMask, share, 1) && (threadIdx.x & 31) != 0;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    float w0 = __fmul_rn(c.wxy[q], c.wz0), w1 = __fmul_rn(c.wxy[q], c.wz1);
-    if (s != 1.f) {
-      w0 = __fmul_rn(s, w0);
-      w1 = __fmul_rn(s, w1);
-    }
-    const float in = __shfl_up_sync(kFullMask, w1, 1);
-    if (from_prev) w0 = __fadd_rn(w0, in);
-    if (valid) {
-      red_add(m + c.row[q] + c.z0, w0);
-      if (!share) red_add(m + c.row[q] + c.z1, w1);
-    }
-  }
 }
 
 __device__ __forceinline__ float3 readout3(const float* __restrict__ f0,

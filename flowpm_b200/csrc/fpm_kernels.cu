@@ -58,9 +58,7 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     for (int it = 0; it < kItems; ++it) {
       int i, j, k;
       int64_t local;
-      // every lane stays in the loop body (the readout and the paint
-      // exchange cells between lanes); missing particles of edge blocks
-      // only skip their memory accesses
+      // missing particles of edge blocks skip their memory accesses
       const bool valid = walk_particle(S, w, it, i, j, k, local);
       const int64_t g = S.p_off + local;
       float3 d = make_float3(0.f, 0.f, 0.f), p = d;
@@ -71,12 +69,8 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       const float3 x = mesh_pos(S, i, j, k, d);
       const Cic8 c0 = cic8(cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
                            cic_axis(x.z, S.mz), S.my, S.mz);
-#if FPM_WARP_SHARE
-      float3 f = readout_cic8_shared(a.fmesh + 3 * S.m_off, mcells, c0, valid);
-#else
       float3 f = valid ? readout_cic8(a.fmesh + 3 * S.m_off, mcells, c0)
                        : make_float3(0.f, 0.f, 0.f);
-#endif
       // force = readout * factor / pm_nc_factor (flowpm/tfpm.py:218, :356)
       f.x = __fmul_rn(__fmul_rn(f.x, fac), invb);
       f.y = __fmul_rn(__fmul_rn(f.y, fac), invb);
@@ -116,11 +110,7 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       }
       const Cic8 c1 = cic8(cic_axis(xn.x, S.mx), cic_axis(xn.y, S.my),
                            cic_axis(xn.z, S.mz), S.my, S.mz);
-#if FPM_WARP_SHARE
-      paint_cic8_shared(m, c1, 1.f, valid);
-#else
       if (valid) paint_cic8(m, c1, 1.f);
-#endif
     }
   }
 }
