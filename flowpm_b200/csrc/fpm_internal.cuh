@@ -189,15 +189,16 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 #ifndef FPM_STEP_BLOCKED
 #define FPM_STEP_BLOCKED 1  // k_step walks 8x8x16 lattice blocks
 #endif
-// Measured on B200 at 128^3: 3 blocks (80 registers) beats 2 (128
-// registers) and 4 (64 registers, spills); the v4 pair reduction is slower
-// than two scalar reductions (33 vs 49 us for 2^21 particles).  Painting
+// Measured on B200, k_step per leapfrog step at 128^3 / 256^3: 3 blocks
+// (80 registers) 87.4 / 621 us, 4 blocks (64) 84.6 / 594, 5 blocks (48)
+// 85.4 / 583, 6 blocks (40, spills) 96.1 / 657.  The v4 pair reduction is
+// slower than two scalar reductions (33 vs 49 us for 2^21 particles).  Painting
 // after the readout phase of the whole block, directly or through a
 // shared-memory tile of the block's cells, was slower (103 and 144 vs 87 us
 // per step): the paint's reductions overlap the readout's gathers best when
 // each warp issues both, particle by particle.
 #ifndef FPM_STEP_MINBLOCKS
-#define FPM_STEP_MINBLOCKS 3   // resident blocks of 256 threads per SM
+#define FPM_STEP_MINBLOCKS 4   // resident blocks of 256 threads per SM
 #endif
 #ifndef FPM_PAINT_VEC
 #define FPM_PAINT_VEC 0        // z-adjacent neighbour pairs as one v4 add
