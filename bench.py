@@ -559,13 +559,13 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
   peak, peak_kind = peaks()
   tot_np, nc_tot = 2 * np_, 2 * np_
   # algorithmic bytes per launch: step 64 B / particle (Np = Nc), paint
-  # 12 Np + 4 Nc, Fourier read 8 B x half modes + write 3 x 8 B x half modes
-  # + zero 4 Nc
-  half = 2 * n * n * (n // 2 + 1)
+  # 12 Np + 4 Nc; the Fourier solve (density -> three force meshes, all of
+  # its transforms and kernels) reads and zeroes the density and writes the
+  # three force meshes, 20 Nc
   kbytes = {
       'step': KERNEL_BYTES_PER_PART * tot_np,
       'paint': 12 * tot_np + 4 * nc_tot,
-      'fourier': 8 * half + 24 * half + 4 * nc_tot,
+      'fourier': 20 * nc_tot,
   }
   roof = {}
   for k, (ms, cnt) in kt.items():

@@ -24,7 +24,7 @@ using namespace fpm;
 namespace {
 
 // Kernels timed by fpm_plan_profile.
-constexpr int kProfKinds = 3;  // 0 step, 1 fourier force, 2 initial paint
+constexpr int kProfKinds = 3;  // 0 step, 1 Fourier solve, 2 initial paint
 
 struct Run {
   int first, count;        // simulations [first, first + count)
@@ -253,9 +253,10 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
   const int32_t* act = it >= 0 ? p->d_nsteps : nullptr;
   const double r2 = p->r_split * p->r_split;
   const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
-  // runs on the fused solve: three launches each, straight to fmesh
+  // profile kind 1 brackets the whole solve, density -> force meshes
   bool any_cufft = false;
   prof_mark(p, 1, st);
+  // runs on the fused solve: a few launches each, straight to fmesh
   for (auto& r : p->runs) {
     if (!r.fused) {
       any_cufft = true;
@@ -290,7 +291,6 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
                          zero_rho ? p->rho : nullptr, tabs_of(p), r2, deconv,
                          act, it, 1, st);
   }
-  prof_mark(p, 1, st);
   FPM_TRY(launch_ok());
   for (auto& r : p->runs) {
     if (r.fused) continue;
@@ -309,6 +309,7 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
                         it, 1, st);
     FPM_TRY(launch_ok());
   }
+  prof_mark(p, 1, st);
   return FPM_OK;
 }
 
