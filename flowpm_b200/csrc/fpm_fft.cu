@@ -280,6 +280,9 @@ __device__ __forceinline__ void cols_dft(float2* P) {
 // together as column 0 = X[.][0] + i X[.][M] and are separated on the way
 // out (Y0 = (C[ky] + conj C[-ky]) / 2, YM = (C[ky] - conj C[-ky]) / 2i), so
 // the y pass covers M columns.
+// Measured on B200 at 128^3 (Fourier solve per step): 512 threads 51 us,
+// 1024 threads 52 us; splitting each plane over a cluster of two CTAs
+// (the y pass through distributed shared memory) 63 us.
 #ifndef FPM_PLANE_THREADS
 #define FPM_PLANE_THREADS 512
 #endif
