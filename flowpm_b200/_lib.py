@@ -47,6 +47,8 @@ SIGNATURES = {
                           c_void_p]),
     'fpm_nbody_set_steps': (c_int, [c_void_p, c_int, P_int32, P_double,
                                     P_double, c_void_p]),
+    'fpm_nbody_set_pgd': (c_int, [c_void_p, c_int, P_double, c_void_p]),
+    'fpm_pgd': (c_int, [c_void_p, c_void_p, P_double, c_void_p]),
     'fpm_nbody_run': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p,
                               c_void_p, c_uint, c_void_p, c_int, c_void_p]),
     'fpm_nbody_adjoint': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p,

@@ -358,8 +358,7 @@ k_fft_plane_fwd(const SimDev* __restrict__ sims, int first, int nx,
 template <int NX, bool GRAD3>
 __global__ void __launch_bounds__(kFftThreads)
 k_fft_columns(const SimDev* __restrict__ sims, int first, int nblk,
-              float2* dk, float2* __restrict__ fk, AxisTabs tabs, double r2,
-              int deconv) {
+              float2* dk, float2* __restrict__ fk, AxisTabs tabs, Green G) {
   constexpr int N1 = Split<NX>::N1, N2 = Split<NX>::N2;
   constexpr int C = kFftThreads / N2;
   __shared__ float2 ex[C * NX];
@@ -378,7 +377,7 @@ k_fft_columns(const SimDev* __restrict__ sims, int first, int nblk,
   for (int j1 = 0; j1 < N1; ++j1)
     a[j1] = valid ? src[(int64_t)(N2 * j1 + g) * ncols] : make_float2(0.f, 0.f);
   fwd_line<NX>(a, line, C, g, valid);
-  // potential spectrum, as k_fourier_force: delta * pre * w(k)
+  // potential spectrum delta * pre * w(k), w the transfer function G
   const int ky = valid ? c / nzh : 0;
   const int kz = valid ? c - ky * nzh : 0;
   const float pre = (float)((double)S.bf * S.bf * S.bf /
@@ -393,16 +392,13 @@ k_fft_columns(const SimDev* __restrict__ sims, int first, int nblk,
   const float* gy = gx + S.mx;
   const float* gz = gy + S.my;
   const double kyz = kky[ky] + kkz[kz];
-  const float wyz = deconv ? __fmul_rn(wy[ky], wz[kz]) : 1.f;
+  const float wyv = wy[ky], wzv = wz[kz];
 #pragma unroll
   for (int u = 0; u < N1 / N2; ++u)
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) {
       const int kx = g + N2 * u + N1 * k2;
-      const double kk = kkx[kx] + kyz;
-      float w = kk == 0.0 ? 0.f : (float)(1.0 / kk);
-      if (r2 != 0.0) w = __fmul_rn(w, (float)exp(-kk * r2));
-      if (deconv) w = __fmul_rn(w, __fmul_rn(wx[kx], wyz));
+      const float w = green_w(G, s, kkx[kx] + kyz, wx[kx], wyv, wzv);
       float2 v = a[u * N2 + k2];
       v.x = __fmul_rn(__fmul_rn(v.x, pre), w);
       v.y = __fmul_rn(__fmul_rn(v.y, pre), w);
@@ -634,7 +630,7 @@ int prepare_ny(int M) {
 template <int NY, int M>
 void launch_shape(const SimDev* sims, int first, int n, int nx, float* rho,
                   int zero_rho, float2* dk, float2* fk, float* fmesh,
-                  float* phi, AxisTabs tabs, double r2, int deconv, bool grad3,
+                  float* phi, AxisTabs tabs, const Green& G, bool grad3,
                   bool real_out, cudaStream_t st) {
   const size_t smem = (size_t)NY * (M + 1) * sizeof(float2);
   k_fft_plane_fwd<NY, M><<<n * nx, kPlaneThreads, smem, st>>>(
@@ -647,10 +643,10 @@ void launch_shape(const SimDev* sims, int first, int n, int nx, float* rho,
     const int nblk = (ncols + C - 1) / C;                                  \
     if (grad3)                                                             \
       k_fft_columns<NN, true><<<n * nblk, kFftThreads, 0, st>>>(           \
-          sims, first, nblk, dk, fk, tabs, r2, deconv);                    \
+          sims, first, nblk, dk, fk, tabs, G);                             \
     else                                                                   \
       k_fft_columns<NN, false><<<n * nblk, kFftThreads, 0, st>>>(          \
-          sims, first, nblk, dk, fk, tabs, r2, deconv);                    \
+          sims, first, nblk, dk, fk, tabs, G);                             \
     break;                                                                 \
   }
     FPM_FFT_SIZES(FPM_COL_CASE)
@@ -679,13 +675,13 @@ void launch_shape(const SimDev* sims, int first, int n, int nx, float* rho,
 template <int NY>
 void launch_ny(int M, const SimDev* sims, int first, int n, int nx,
                float* rho, int zero_rho, float2* dk, float2* fk, float* fmesh,
-               float* phi, AxisTabs tabs, double r2, int deconv, bool grad3,
+               float* phi, AxisTabs tabs, const Green& G, bool grad3,
                bool real_out, cudaStream_t st) {
   switch (M) {
 #define FPM_SHAPE_CASE(MM)                                                  \
   case MM:                                                                  \
     launch_shape<NY, MM>(sims, first, n, nx, rho, zero_rho, dk, fk, fmesh,  \
-                         phi, tabs, r2, deconv, grad3, real_out, st);       \
+                         phi, tabs, G, grad3, real_out, st);                \
     break;
     FPM_FFT_HALF(FPM_SHAPE_CASE)
 #undef FPM_SHAPE_CASE
@@ -734,14 +730,14 @@ int fft_fused_prepare(int nx, int ny, int nz) {
 void launch_fft_force(const SimDev* sims, int first, int n, int nx, int ny,
                       int nz, float* rho, int zero_rho, float2* dk,
                       float2* fk, float* fmesh, float* phi, AxisTabs tabs,
-                      double r2, int deconv, bool grad3, cudaStream_t st) {
+                      const Green& G, bool grad3, cudaStream_t st) {
   if (n <= 0) return;
   g_launches.fetch_add(grad3 ? 3 : 4, std::memory_order_relaxed);
   switch (ny) {
 #define FPM_NY_CASE(NN)                                                      \
   case NN:                                                                   \
     launch_ny<NN>(nz / 2, sims, first, n, nx, rho, zero_rho, dk, fk, fmesh,  \
-                  phi, tabs, r2, deconv, grad3, false, st);                  \
+                  phi, tabs, G, grad3, false, st);                           \
     break;
     FPM_FFT_SIZES(FPM_NY_CASE)
 #undef FPM_NY_CASE
@@ -750,7 +746,7 @@ void launch_fft_force(const SimDev* sims, int first, int n, int nx, int ny,
 
 void launch_fft_potential(const SimDev* sims, int first, int n, int nx,
                           int ny, int nz, const float* in, float2* dk,
-                          float* out, AxisTabs tabs, double r2, int deconv,
+                          float* out, AxisTabs tabs, const Green& G,
                           cudaStream_t st) {
   if (n <= 0) return;
   g_launches.fetch_add(3, std::memory_order_relaxed);
@@ -759,7 +755,7 @@ void launch_fft_potential(const SimDev* sims, int first, int n, int nx,
 #define FPM_NY_CASE(NN)                                                   \
   case NN:                                                                \
     launch_ny<NN>(nz / 2, sims, first, n, nx, src, 0, dk, nullptr,        \
-                  nullptr, out, tabs, r2, deconv, false, true, st);       \
+                  nullptr, out, tabs, G, false, true, st);                \
     break;
     FPM_FFT_SIZES(FPM_NY_CASE)
 #undef FPM_NY_CASE

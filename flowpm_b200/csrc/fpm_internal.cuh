@@ -52,6 +52,49 @@ struct AxisTabs {
   const float* win;
 };
 
+// Transfer function of the potential, common to the three force
+// components (evaluated per mode; s = the mode's simulation):
+// * force (pgd null): the Green's function 1/k^2 rounded to float (0 at
+//   k = 0, where the gradient vanishes anyway), times the optional
+//   Gaussian long-range split exp(-k^2 r2) and CIC deconvolution
+//   (flowpm/tfpm.py:199-215, kernels.py:28-48, :81-102, :137-152);
+// * PGD (pgd set): the same 1/k^2 times the PGD kernel
+//   exp(-kl^2 / k^2) exp(-k^4 / ks^4) in float32 (flowpm/tfpm.py:222-270,
+//   kernels.py:105-134), (kl, ks) = pgd[(s * pgd_stride + pos) * 3 + 1, 2].
+struct Green {
+  double r2;
+  int deconv;
+  int pgd_stride;
+  const float* pgd;
+  int pos;
+};
+
+__host__ __device__ inline Green force_green(double r2, int deconv) {
+  Green g;
+  g.r2 = r2;
+  g.deconv = deconv;
+  g.pgd_stride = 0;
+  g.pgd = nullptr;
+  g.pos = 0;
+  return g;
+}
+
+__device__ __forceinline__ float green_w(const Green& G, int s, double kk,
+                                         float wx, float wy, float wz) {
+  if (kk == 0.0) return 0.f;
+  float w = (float)(1.0 / kk);
+  if (G.pgd) {
+    const float* q = G.pgd + ((int64_t)s * G.pgd_stride + G.pos) * 3;
+    const float kkf = (float)kk, kl = q[1], ks = q[2];
+    const float kl2 = kl * kl, ks4 = (ks * ks) * (ks * ks);
+    const float v = expf(-kl2 / kkf) * expf(-(kkf * kkf) / ks4);
+    return __fmul_rn(w, v);
+  }
+  if (G.r2 != 0.0) w = __fmul_rn(w, (float)exp(-kk * G.r2));
+  if (G.deconv) w = __fmul_rn(w, __fmul_rn(__fmul_rn(wx, wy), wz));
+  return w;
+}
+
 enum ChunkKind {
   kPart = 0, kSpec = 1, kMesh = 2, kLat = 3, kLatSpec = 4, kBlock = 5
 };

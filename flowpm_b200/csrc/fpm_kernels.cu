@@ -115,6 +115,52 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
   }
 }
 
+// PGD correction of one step (flowpm/tfpm.py:369-422, applied after the
+// drift at :487-488): readout of the three PGD displacement meshes at
+// (q + d) * bf, d += (alpha * R) / bf (the reference's update = readout *
+// alpha / pm_nc_factor), then the paint of the moved particle into rho
+// (zeroed by the PGD solve) for the force that follows.  pgd holds rows
+// (alpha, kl, ks) of stride pgd_stride per sim; with nsteps, the row of
+// step pos and only the sims with nsteps > pos (the ones that drifted).
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
+k_pgd(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+      float* __restrict__ disp, const float* __restrict__ fmesh,
+      float* __restrict__ rho, const float* __restrict__ pgd, int pgd_stride,
+      int pos, const int32_t* __restrict__ nsteps, int32_t* status) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kTraverse);
+    if (nsteps && nsteps[s] <= pos) continue;
+    const SimDev S = sims[s];
+    const float alpha =
+        pgd[((int64_t)s * pgd_stride + (nsteps ? pos : 0)) * 3];
+    const float b = (float)S.bf;
+    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
+    float* m = rho + S.m_off;
+    const Walk w = walk_chunk(S, ch - traverse_first(S));
+#pragma unroll 1
+    for (int it = 0; it < kItems; ++it) {
+      int i, j, k;
+      int64_t local;
+      if (!walk_particle(S, w, it, i, j, k, local)) continue;
+      const int64_t g = S.p_off + local;
+      float3 d = ld3(disp, g);
+      const float3 x = mesh_pos(S, i, j, k, d);
+      const float3 r = readout_cic8(fmesh + 3 * S.m_off, mcells,
+                                    cic8(cic_axis(x.x, S.mx),
+                                         cic_axis(x.y, S.my),
+                                         cic_axis(x.z, S.mz), S.my, S.mz));
+      d.x = __fadd_rn(d.x, __fdiv_rn(__fmul_rn(r.x, alpha), b));
+      d.y = __fadd_rn(d.y, __fdiv_rn(__fmul_rn(r.y, alpha), b));
+      d.z = __fadd_rn(d.z, __fdiv_rn(__fmul_rn(r.z, alpha), b));
+      st3(disp, g, d);
+      const float3 xn = mesh_pos(S, i, j, k, d);
+      if (!finite3(xn.x, xn.y, xn.z)) atomicOr(status, FPM_STATUS_NONFINITE_POS);
+      paint8(m, S.mx, S.my, S.mz, cic_axis(xn.x, S.mx), cic_axis(xn.y, S.my),
+             cic_axis(xn.z, S.mz));
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_force_readout(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                 const float* __restrict__ disp,
@@ -223,7 +269,7 @@ __global__ void __launch_bounds__(kThreads)
 k_fourier_potential(const SimDev* __restrict__ sims, int nsims,
                     int64_t nchunks, const float2* dk, float2* out,
                     float* __restrict__ rho_zero,
-                    AxisTabs tabs, double r2, int deconv,
+                    AxisTabs tabs, Green G,
                     const int32_t* __restrict__ nsteps, int pos,
                     int skip_fused) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -249,10 +295,8 @@ k_fourier_potential(const SimDev* __restrict__ sims, int nsims,
       if (local < nmodes) {
         int i, j, l;
         mode_ijl(local, S.my, S.mzh, i, j, l);
-        const double kk = kkx[i] + kky[j] + kkz[l];
-        float w = kk == 0.0 ? 0.f : (float)(1.0 / kk);
-        if (r2 != 0.0) w = __fmul_rn(w, (float)exp(-kk * r2));
-        if (deconv) w = __fmul_rn(w, __fmul_rn(__fmul_rn(wx[i], wy[j]), wz[l]));
+        const float w = green_w(G, s, kkx[i] + kky[j] + kkz[l], wx[i], wy[j],
+                                wz[l]);
         float2 dv = din[local];
         dv.x = __fmul_rn(dv.x, pre);
         dv.y = __fmul_rn(dv.y, pre);
@@ -266,7 +310,7 @@ k_fourier_potential(const SimDev* __restrict__ sims, int nsims,
   }
 }
 
-// 4-point central difference along one axis with periodic wrap:
+// 4-point central difference with periodic wrap:
 // (8 (f[+1] - f[-1]) - (f[+2] - f[-2])) / 12.
 __device__ __forceinline__ float stencil4(float m2, float m1, float p1,
                                           float p2) {
@@ -599,13 +643,13 @@ void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
 
 void launch_fourier_potential(const SimDev* sims, int nsims, int64_t nchunks,
                               const float2* dk, float2* out, float* rho_zero,
-                              AxisTabs tabs, double r_split2, int deconv,
+                              AxisTabs tabs, const Green& G,
                               const int32_t* nsteps, int pos, int skip_fused,
                               cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_fourier_potential<<<grid_for(nchunks), kThreads, 0, st>>>(
-      sims, nsims, nchunks, dk, out, rho_zero, tabs, r_split2, deconv, nsteps,
-      pos, skip_fused);
+      sims, nsims, nchunks, dk, out, rho_zero, tabs, G, nsteps, pos,
+      skip_fused);
 }
 
 void launch_stencil_grad(const SimDev* sims, int nsims, int64_t nchunks,
@@ -628,6 +672,16 @@ void launch_step(const SimDev* sims, int nsims, int64_t nchunks,
                  const StepArgs& a, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_step<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
+}
+
+void launch_pgd(const SimDev* sims, int nsims, int64_t nchunks, float* disp,
+                const float* fmesh, float* rho, const float* pgd,
+                int pgd_stride, int pos, const int32_t* nsteps,
+                int32_t* status, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_pgd<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, disp,
+                                                fmesh, rho, pgd, pgd_stride,
+                                                pos, nsteps, status);
 }
 
 void launch_force_readout(const SimDev* sims, int nsims, int64_t nchunks,

@@ -45,11 +45,12 @@ void launch_fourier_force(const SimDev* sims, int nsims, int64_t nchunks,
                           const int32_t* nsteps, int pos, int skip_fused,
                           cudaStream_t st);
 
-// Potential spectrum delta_k * pre * w(k) (one output per sim, layout of
-// dk); also zeroes rho_zero when given.  The adjoint reuses it as is.
+// Potential spectrum delta_k * pre * w(k) with w the transfer function G
+// (one output per sim, layout of dk); also zeroes rho_zero when given.  The
+// adjoint reuses it as is; the PGD correction passes its own G.
 void launch_fourier_potential(const SimDev* sims, int nsims, int64_t nchunks,
                               const float2* dk, float2* out, float* rho_zero,
-                              AxisTabs tabs, double r_split2, int deconv,
+                              AxisTabs tabs, const Green& G,
                               const int32_t* nsteps, int pos, int skip_fused,
                               cudaStream_t st);
 
@@ -78,18 +79,25 @@ int fft_fused_prepare(int nx, int ny, int nz);
 void launch_fft_force(const SimDev* sims, int first, int n, int nx, int ny,
                       int nz, float* rho, int zero_rho, float2* dk,
                       float2* fk, float* fmesh, float* phi, AxisTabs tabs,
-                      double r2, int deconv, bool grad3, cudaStream_t st);
+                      const Green& G, bool grad3, cudaStream_t st);
 // out = C2R(pre * w(k) * R2C(in)) for the sims [first, first + n) of one
 // run (the adjoint's density cotangent from the potential cotangent); in is
 // only read.
 void launch_fft_potential(const SimDev* sims, int first, int n, int nx,
                           int ny, int nz, const float* in, float2* dk,
-                          float* out, AxisTabs tabs, double r2, int deconv,
+                          float* out, AxisTabs tabs, const Green& G,
                           cudaStream_t st);
 
 // Fused readout + kick(end) + kick(start) + drift + paint of one iteration.
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,
                  const StepArgs& a, cudaStream_t st);
+
+// PGD correction of one step: d += alpha * readout(PGD meshes) / bf, then
+// the paint of the moved particles into rho (see k_pgd).
+void launch_pgd(const SimDev* sims, int nsims, int64_t nchunks, float* disp,
+                const float* fmesh, float* rho, const float* pgd,
+                int pgd_stride, int pos, const int32_t* nsteps,
+                int32_t* status, cudaStream_t st);
 
 // Readout of the three force meshes at (q + disp) * bf, times ffac / bf.
 void launch_force_readout(const SimDev* sims, int nsims, int64_t nchunks,

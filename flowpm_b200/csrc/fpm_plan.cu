@@ -91,6 +91,12 @@ struct fpm_plan {
   int32_t* d_nsteps = nullptr;
   float* d_ffac = nullptr;
   float* d_lcoef = nullptr;
+  // PGD correction: (alpha, kl, ks) per sim and step (stride coef_cap), and
+  // per sim for one fpm_pgd call
+  float* d_pgd = nullptr;
+  int pgd_cap = 0;
+  bool pgd_on = false;
+  float* d_pgd1 = nullptr;
   int32_t* d_status = nullptr;
   void* work = nullptr;
   size_t device_bytes = 0;
@@ -107,6 +113,20 @@ struct fpm_plan {
 namespace {
 
 AxisTabs tabs_of(const fpm_plan* p) { return AxisTabs{p->d_kk, p->d_grad, p->d_win}; }
+
+Green plan_green(const fpm_plan* p) {
+  return force_green(p->r_split * p->r_split,
+                     (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0);
+}
+
+// PGD transfer function of step `pos` (table d_pgd) or of one fpm_pgd call.
+Green pgd_green(const fpm_plan* p, int pos, bool single) {
+  Green g = force_green(0.0, 0);
+  g.pgd = single ? p->d_pgd1 : p->d_pgd;
+  g.pgd_stride = single ? 1 : p->pgd_cap;
+  g.pos = single ? 0 : pos;
+  return g;
+}
 
 // Chunks of the mesh-touching particle kernels (see kTraverse).
 int64_t traverse_chunks(const fpm_plan* p) {
@@ -148,7 +168,8 @@ void free_all(fpm_plan* p) {
   void* bufs[] = {p->d_sims, p->d_kk,   p->d_grad,  p->d_win,   p->rho,
                   p->dk,     p->fk,     p->fmesh,   p->lreal1,  p->lspec1,
                   p->lspec9, p->lreal9, p->lreal3,  p->d_coefs, p->d_nsteps,
-                  p->d_ffac, p->d_lcoef, p->d_status, p->work,
+                  p->d_ffac, p->d_lcoef, p->d_status, p->work, p->d_pgd,
+                  p->d_pgd1,
                   p->lmesh,  p->lrho,   p->fpart,   p->phi};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -253,6 +274,7 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
   const int32_t* act = it >= 0 ? p->d_nsteps : nullptr;
   const double r2 = p->r_split * p->r_split;
   const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
+  const Green G = plan_green(p);
   // profile kind 1 brackets the whole solve, density -> force meshes
   bool any_cufft = false;
   prof_mark(p, 1, st);
@@ -267,7 +289,7 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
     if (n == 0) continue;
     launch_fft_force(p->d_sims, r.first, n, S.mx, S.my, S.mz, p->rho,
                      zero_rho ? 1 : 0, p->dk, p->fk, p->fmesh, p->phi,
-                     tabs_of(p), r2, deconv, !stencil_path(p), st);
+                     tabs_of(p), G, !stencil_path(p), st);
   }
   FPM_TRY(launch_ok());
   if (!any_cufft) {
@@ -284,8 +306,8 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
   }
   if (stencil_path(p)) {
     launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
-                             zero_rho ? p->rho : nullptr, tabs_of(p), r2,
-                             deconv, act, it, 1, st);
+                             zero_rho ? p->rho : nullptr, tabs_of(p), G, act,
+                             it, 1, st);
   } else {
     launch_fourier_force(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
                          zero_rho ? p->rho : nullptr, tabs_of(p), r2, deconv,
@@ -311,6 +333,56 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
   }
   prof_mark(p, 1, st);
   return FPM_OK;
+}
+
+// PGD displacement meshes (into fmesh) of the density in rho, which is
+// zeroed: the force solve's path with the PGD transfer function and the
+// 4-point stencil gradient (flowpm/tfpm.py:222-270 uses order 1 whatever
+// the force's gradient).  pos >= 0: the sims still moving at step pos
+// (nsteps > pos) with the parameters of step pos; pos < 0: every sim with
+// the parameters of one fpm_pgd call.
+int pgd_meshes(fpm_plan* p, cudaStream_t st, int pos) {
+  const bool single = pos < 0;
+  const Green G = pgd_green(p, pos, single);
+  const int32_t* act = single ? nullptr : p->d_nsteps;
+  const int apos = single ? -1 : pos + 1;  // sims with nsteps >= pos + 1
+  bool any_cufft = false;
+  for (auto& r : p->runs) {
+    if (!r.fused) {
+      any_cufft = true;
+      continue;
+    }
+    const SimDev& S = p->sims[r.first];
+    const int n = run_active(r, apos);
+    if (n == 0) continue;
+    launch_fft_force(p->d_sims, r.first, n, S.mx, S.my, S.mz, p->rho, 1,
+                     p->dk, p->fk, p->fmesh, p->phi, tabs_of(p), G, false,
+                     st);
+  }
+  FPM_TRY(launch_ok());
+  if (!any_cufft) return FPM_OK;
+  for (auto& r : p->runs) {
+    if (r.fused) continue;
+    const SimDev& S = p->sims[r.first];
+    const int n = run_active(r, apos);
+    if (n == 0) continue;
+    FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->rho + S.m_off,
+                     p->dk + S.s_off, st));
+  }
+  launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk, p->rho,
+                           tabs_of(p), G, act, apos, 1, st);
+  FPM_TRY(launch_ok());
+  for (auto& r : p->runs) {
+    if (r.fused) continue;
+    const SimDev& S = p->sims[r.first];
+    const int n = run_active(r, apos);
+    if (n == 0) continue;
+    FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->fk + S.s_off,
+                     p->phi + S.m_off, st));
+  }
+  launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, p->phi, p->fmesh, act,
+                      apos, 1, st);
+  return launch_ok();
 }
 
 // Per run and position, the active prefix of the run; batched cuFFT plans
@@ -662,6 +734,10 @@ extern "C" int fpm_nbody_set_steps(fpm_plan* p, int max_steps,
     p->coef_cap = max_steps;
     p->coef_gen++;
     p->device_bytes += sizeof(float) * 3 * (size_t)p->nsims * max_steps;
+    if (p->pgd_on) {  // its table has the old stride: set it again
+      p->pgd_on = false;
+      p->sched_gen++;
+    }
   }
   if (max_steps > 0) {
     std::vector<float> c(3 * (size_t)p->nsims * max_steps);
@@ -716,7 +792,88 @@ extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
     launch_step(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     prof_mark(p, 0, st);
     FPM_TRY(launch_ok());
+    if (p->pgd_on && it < p->max_steps) {  // after the drift of step it
+      FPM_TRY(pgd_meshes(p, st, it));
+      launch_pgd(p->d_sims, p->nsims, traverse_chunks(p), disp, p->fmesh,
+                 p->rho, p->d_pgd, p->pgd_cap, it, p->d_nsteps, p->d_status,
+                 st);
+      FPM_TRY(launch_ok());
+    }
   }
+  return FPM_OK;
+}
+
+extern "C" int fpm_nbody_set_pgd(fpm_plan* p, int enable, const double* params,
+                                 void* stream) {
+  if (!p || (enable && !params)) return FPM_ERR_ARG;
+  if (!enable) {
+    if (p->pgd_on) {
+      p->pgd_on = false;
+      p->sched_gen++;
+    }
+    return FPM_OK;
+  }
+  if (!p->steps_set) return FPM_ERR_STATE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int cap = p->coef_cap > 0 ? p->coef_cap : 1;
+  if (!p->d_pgd || p->pgd_cap != cap) {
+    if (p->d_pgd) {
+      FPM_CUDA(cudaStreamSynchronize(st));
+      cudaFree(p->d_pgd);
+      p->device_bytes -= sizeof(float) * 3 * (size_t)p->nsims * p->pgd_cap;
+      p->d_pgd = nullptr;
+    }
+    if (cudaMalloc(&p->d_pgd, sizeof(float) * 3 * (size_t)p->nsims * cap) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      p->pgd_cap = 0;
+      return FPM_ERR_OOM;
+    }
+    p->pgd_cap = cap;
+    p->coef_gen++;  // captured graphs hold the old table
+    p->device_bytes += sizeof(float) * 3 * (size_t)p->nsims * cap;
+  }
+  std::vector<float> h(3 * (size_t)p->nsims * cap, 0.f);
+  for (int s = 0; s < p->nsims; ++s)
+    for (int t = 0; t < p->max_steps; ++t)
+      for (int q = 0; q < 3; ++q)
+        h[((size_t)s * cap + t) * 3 + q] =
+            (float)params[((size_t)s * p->max_steps + t) * 3 + q];
+  FPM_CUDA(cudaMemcpyAsync(p->d_pgd, h.data(), sizeof(float) * h.size(),
+                           cudaMemcpyHostToDevice, st));
+  FPM_CUDA(cudaStreamSynchronize(st));  // h is pageable and dies here
+  if (!p->pgd_on) {
+    p->pgd_on = true;
+    p->sched_gen++;
+  }
+  return FPM_OK;
+}
+
+extern "C" int fpm_pgd(fpm_plan* p, float* disp, const double* params,
+                       void* stream) {
+  if (!p || !disp || !params) return FPM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!p->d_pgd1) {
+    if (cudaMalloc(&p->d_pgd1, sizeof(float) * 3 * (size_t)p->nsims) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return FPM_ERR_OOM;
+    }
+    p->device_bytes += sizeof(float) * 3 * (size_t)p->nsims;
+  }
+  std::vector<float> h(3 * (size_t)p->nsims);
+  for (size_t i = 0; i < h.size(); ++i) h[i] = (float)params[i];
+  FPM_CUDA(cudaMemcpyAsync(p->d_pgd1, h.data(), sizeof(float) * h.size(),
+                           cudaMemcpyHostToDevice, st));
+  FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
+  launch_paint_lattice(p->d_sims, p->nsims, traverse_chunks(p), disp, p->rho,
+                       p->d_status, st);
+  FPM_TRY(launch_ok());
+  FPM_TRY(pgd_meshes(p, st, -1));
+  launch_pgd(p->d_sims, p->nsims, traverse_chunks(p), disp, p->fmesh, p->rho,
+             p->d_pgd1, 1, 0, nullptr, p->d_status, st);
+  FPM_TRY(launch_ok());
+  FPM_CUDA(cudaStreamSynchronize(st));  // h is pageable and dies here
   return FPM_OK;
 }
 
@@ -737,6 +894,7 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
       (ckpt && ckpt_every < 1))
     return FPM_ERR_ARG;
   if (!(p->flags & FPM_PLAN_ADJOINT) || !p->steps_set) return FPM_ERR_STATE;
+  if (p->pgd_on) return FPM_ERR_UNSUPPORTED;  // no adjoint of the PGD step
   cudaStream_t st = (cudaStream_t)stream;
   FPM_CUDA(cudaMemcpyAsync(p->fpart, force, sizeof(float) * 3 * p->total_np,
                            cudaMemcpyDeviceToDevice, st));
@@ -786,8 +944,8 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
         if (n == 0) continue;
         if (r.fused) {  // lrho straight from lphi
           launch_fft_potential(p->d_sims, r.first, n, S.mx, S.my, S.mz,
-                               p->phi, p->dk, p->lrho, tabs_of(p), r2, deconv,
-                               st);
+                               p->phi, p->dk, p->lrho, tabs_of(p),
+                               plan_green(p), st);
           continue;
         }
         any_cufft = true;
@@ -797,7 +955,7 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
       FPM_TRY(launch_ok());
       if (!any_cufft) continue;
       launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->dk,
-                               nullptr, tabs_of(p), r2, deconv, act, it, 1,
+                               nullptr, tabs_of(p), plan_green(p), act, it, 1,
                                st);
       FPM_TRY(launch_ok());
     } else {

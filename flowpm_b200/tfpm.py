@@ -19,6 +19,7 @@ from .kernels import fftk
 from .utils import as_cuda, _seed
 
 __all__ = ['linear_field', 'lpt_init', 'nbody', 'force', 'kick', 'drift',
+           'pgd',
            'linear_amplitude']
 
 
@@ -164,6 +165,36 @@ def force(cosmo, state, nc, pm_nc_factor=1, name='Force', **kwargs):
   return torch.stack((state[0], state[1], f))
 
 
+def _pgd_rows(pgdparams, rows):
+  """(alpha, kl, ks) rows as a float64 array of shape (rows, 3)."""
+  p = np.asarray(pgdparams, dtype=np.float64)
+  if p.shape == (3,) and rows == 1:
+    p = p.reshape(1, 3)
+  if p.shape != (rows, 3):
+    raise ValueError('pgdparams must hold %d rows of (alpha, kl, ks), got '
+                     'shape %s' % (rows, p.shape))
+  return p
+
+
+def pgd(state, pgdparams, nc, pm_nc_factor=1, name='PGD', **kwargs):
+  """State with X moved by the PGD correction (flowpm/tfpm.py:369-422):
+  paint at X * pm_nc_factor, potential with the PGD kernel
+  exp(-kl^2/k^2) exp(-k^4/ks^4) (kernels.py:105-134), 4-point gradient,
+  readout, X += alpha * update / pm_nc_factor.  ``pgdparams`` =
+  (alpha, kl, ks), kl and ks in the force mesh's k units."""
+  nc = _nc3(nc)
+  state = _state(state, nc)
+  B = state.shape[1]
+  par = _pgd_rows(pgdparams, 1)
+  plan = get_plan([tuple(nc) + (int(pm_nc_factor),)] * B)
+  d = _to_disp(state[0], nc)
+  _lib.call('fpm_pgd', plan.handle, _lib.ptr(d),
+            _lib.dvec(np.tile(par, (B, 1)).ravel()), _lib.stream_ptr())
+  out = state.clone()
+  _to_pos(d, nc, out[0])
+  return out
+
+
 def kick(cosmo, state, ai, ac, af, name='Kick', **kwargs):
   """P += fac F with the FP64 kick prefactor (flowpm/tfpm.py:273-292)."""
   state = as_cuda(state).clone()
@@ -195,18 +226,26 @@ def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
   ``checkpoint_every = k`` stores (d, p) every k steps in the forward and
   resets the rebuilt trajectory there, bounding its FP32 drift.
 
+  With ``pgdparams`` (one row (alpha, kl, ks) per step) the PGD
+  correction moves the particles after every drift (flowpm/tfpm.py:487-488,
+  see ``pgd``); that path has no gradient.
+
   With ``check_finite`` the device status word is read at the end and a
   non-finite particle state raises ``FlowPMError``."""
   nc = _nc3(nc)
   stages = [float(s) for s in np.asarray(stages).ravel()]
-  if pgdparams is not None:
-    raise NotImplementedError('PGD correction is not available yet')
   state = _state(state, nc)
   if len(stages) == 0:
     return state
   B = state.shape[1]
   T = len(stages) - 1
+  par = None
+  if pgdparams is not None and T > 0:
+    par = _pgd_rows(pgdparams, T)
   if _autograd.needs_grad(state):
+    if par is not None:
+      raise NotImplementedError(
+          'gradients through the PGD correction are not supported')
     if return_intermediate_states:
       raise NotImplementedError(
           'gradients through intermediate states are not supported')
@@ -223,6 +262,10 @@ def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
   st = _lib.stream_ptr()
   _lib.call('fpm_nbody_set_steps', plan.handle, T, _lib.ivec([T] * B),
             _lib.dvec(coefs.ravel()), _lib.dvec([1.5 * cosmo.Omega_m] * B), st)
+  # the plan is shared: PGD is switched on or off for this call
+  _lib.call('fpm_nbody_set_pgd', plan.handle, 0 if par is None else 1,
+            None if par is None else _lib.dvec(np.tile(par, (B, 1)).ravel()),
+            st)
   d, p, f = plan.work()
   _lib.call('fpm_lattice_shift', _lib.ptr(state[0]), _lib.ptr(d), B, nc[0],
             nc[1], nc[2], -1, st)

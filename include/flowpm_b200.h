@@ -194,6 +194,24 @@ int fpm_nbody_run(fpm_plan* plan, float* disp, float* mom, float* force,
                   float* inter, unsigned flags, float* ckpt, int ckpt_every,
                   void* stream);
 
+/* PGD correction (flowpm/tfpm.py:369-422, applied by nbody after each drift
+ * at :487-488): with enable, every later fpm_nbody_run moves the particles
+ * of step t after its drift by alpha * readout(c2r(delta_k * lap(k) *
+ * exp(-kl^2/k^2) exp(-k^4/ks^4) * i D_d(k))) / pm_nc_factor (4-point
+ * gradient), then paints them for the force.  params: (alpha, kl, ks) per
+ * simulation and step, nsims x max_steps x 3 doubles, kl and ks in the
+ * units of the force mesh's k = 2 pi fftfreq.  Call after
+ * fpm_nbody_set_steps (a set_steps that grows the tables switches PGD off
+ * again).  enable = 0 switches it off.  Plans with PGD on have no adjoint
+ * (FPM_ERR_UNSUPPORTED).  Synchronises the stream once. */
+int fpm_nbody_set_pgd(fpm_plan* plan, int enable, const double* params,
+                      void* stream);
+
+/* One PGD correction of the positions q + disp of every simulation
+ * (flowpm/tfpm.py:369-422 pgd): disp is updated in place.  params: (alpha,
+ * kl, ks) per simulation, nsims x 3 doubles.  Synchronises the stream. */
+int fpm_pgd(fpm_plan* plan, float* disp, const double* params, void* stream);
+
 /* Checkpoints: when ckpt is not NULL, fpm_nbody_run stores the state
  * (disp, mom) at every position j (after the closing kick of step j-1,
  * j = 0 the initial state) with j % ckpt_every == 0 in slot j / ckpt_every

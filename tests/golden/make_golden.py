@@ -228,6 +228,29 @@ def gen_nbody(tf, m):
   save('nbody.npz', **out)
 
 
+def gen_pgd(tf, m):
+  """PGD correction (flowpm/tfpm.py:222-270 apply_pgd, :369-422 pgd, applied
+  after every drift by nbody at :487-488) at 16^3: one (alpha, kl, ks) per
+  step; kl, ks in the mesh's own k units."""
+  tfpm, cosmology = m['tfpm'], m['cosmology']
+  lpt = np.load(os.path.join(HERE, 'lpt.npz'))
+  stages = np.linspace(0.1, 1.0, 10)
+  c = cosmology.Planck15()
+  s0 = lpt['n16_init_o1']
+  params = np.stack([np.linspace(0.2, 0.4, 9), np.full(9, 0.6),
+                     np.full(9, 3.0)], axis=1).astype(np.float32)
+  out = {'stages': stages, 'params': params}
+  out['single'] = np.asarray(tfpm.pgd(s0, tf.constant(params[0]), [16, 16, 16]))
+  out['single_b2'] = np.asarray(
+      tfpm.pgd(s0, tf.constant(params[0]), [16, 16, 16], pm_nc_factor=2))
+  out['final'] = np.asarray(
+      tfpm.nbody(c, s0, stages, 16, pgdparams=tf.constant(params)))
+  out['final_b2'] = np.asarray(
+      tfpm.nbody(c, s0, stages, 16, pm_nc_factor=2,
+                 pgdparams=tf.constant(params)))
+  save('pgd.npz', **out)
+
+
 def gen_pk(tf, m):
   pk = m['pk']
   nb = np.load(os.path.join(HERE, 'nbody.npz'))
@@ -254,7 +277,13 @@ def main():
   gen_lpt(tf, m)
   gen_nbody(tf, m)
   gen_pk(tf, m)
+  gen_pgd(tf, m)
 
 
 if __name__ == '__main__':
-  main()
+  if len(sys.argv) > 1:  # named generators only, e.g. `pgd`
+    tf, m = load_reference()
+    for name in sys.argv[1:]:
+      globals()['gen_' + name](tf, m)
+  else:
+    main()

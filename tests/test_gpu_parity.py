@@ -349,6 +349,39 @@ def test_nbody_many_matches_single_runs(fpm):
   r.close()
 
 
+def test_pgd_golden(fpm, capsys):
+  """PGD correction (flowpm/tfpm.py:369-422; after every drift in nbody,
+  :487-488) against the reference's own output: one call, and a 9-step
+  leapfrog at pm_nc_factor 1 and 2 (also against the FP64 oracle).  The
+  same cached plan then runs without PGD and gives the plain result."""
+  z, l, nb = golden('pgd'), golden('lpt'), golden('nbody')
+  c = fpm.cosmology.Planck15()
+  s0 = l['n16_init_o1']
+  out = host(fpm.tfpm.pgd(s0, z['params'][0], 16))
+  assert_allclose(out, z['single'], atol=2e-5)
+  out = host(fpm.tfpm.pgd(s0, z['params'][0], 16, pm_nc_factor=2))
+  assert_allclose(out, z['single_b2'], atol=2e-5)
+  for bf, key, tol in ((1, 'final', 2e-3), (2, 'final_b2', 5e-3)):
+    out = host(fpm.nbody(c, s0, z['stages'], 16, pm_nc_factor=bf,
+                         pgdparams=z['params']))
+    b64 = obg.Background({}, dtype=np.float64)
+    ref64 = opm.nbody(b64, torch.tensor(s0, dtype=torch.float64),
+                      z['stages'], 16, pm_nc_factor=bf,
+                      pgdparams=z['params']).numpy()
+    with capsys.disabled():
+      print('\npgd bf=%d: vs reference %.2e, vs FP64 %.2e, reference vs '
+            'FP64 %.2e' % (bf, np.abs(out - z[key]).max(),
+                           np.abs(out - ref64).max(),
+                           np.abs(z[key] - ref64).max()))
+    assert_allclose(out, z[key], atol=tol)
+  # PGD off again on the same plan
+  st = host(fpm.nbody(c, s0, z['stages'], 16))
+  assert_allclose(st, nb['n16_b1_final'], atol=1e-4)
+  with pytest.raises(NotImplementedError):
+    x = torch.tensor(s0, device='cuda').requires_grad_(True)
+    fpm.nbody(c, x, z['stages'], 16, pgdparams=z['params'])
+
+
 def test_nbody_stream_matches_nbody(fpm):
   """The host-streaming API (copies overlapped with the computation, double
   buffered, more simulations than buffers) returns, for every host state,

@@ -220,3 +220,22 @@ def test_single_plane_wave_lpt1():
   got = psi[:, 0].reshape(n, n, n)[:, 0, 0]
   assert_allclose(got, expect, atol=1e-7)
   assert np.abs(psi[:, 1:]).max() < 1e-7
+
+
+def test_oracle_pgd_golden():
+  """PGD correction (flowpm/tfpm.py:222-270, :369-422, in nbody at
+  :487-488): the oracle against the reference's own output, one call and
+  a 9-step leapfrog at 16^3, pm_nc_factor 1 and 2."""
+  z, l = golden('pgd'), golden('lpt')
+  s0 = torch.tensor(l['n16_init_o1'])
+  np.testing.assert_allclose(pm.pgd(s0, z['params'][0], 16).numpy(),
+                             z['single'], atol=1e-5)
+  np.testing.assert_allclose(
+      pm.pgd(s0, z['params'][0], 16, pm_nc_factor=2).numpy(),
+      z['single_b2'], atol=1e-5)
+  b = background.Background({}, dtype=np.float32)
+  out = pm.nbody(b, s0, z['stages'], 16, pgdparams=z['params']).numpy()
+  np.testing.assert_allclose(out, z['final'], atol=2e-3)
+  out = pm.nbody(b, s0, z['stages'], 16, pm_nc_factor=2,
+                  pgdparams=z['params']).numpy()
+  np.testing.assert_allclose(out, z['final_b2'], atol=5e-3)
