@@ -12,6 +12,7 @@ from . import kernels
 from . import tfbackground
 from . import tfbackground as background
 from . import tfpower
+from . import raytracing
 from .utils import cic_paint, cic_readout, r2c3d, c2r3d, white_noise
 from .tfpm import nbody, linear_field, lpt_init
 from .pk import power_spectrum

@@ -47,6 +47,59 @@ class CicPaint(torch.autograd.Function):
     return (g if ctx.needs_input_grad[0] else None), lp, lw
 
 
+class CicPaint2D(torch.autograd.Function):
+
+  @staticmethod
+  def forward(ctx, mesh, part, weight, mask):
+    B, nx, ny = mesh.shape
+    out = mesh.detach().clone()
+    w = None if weight is None else weight.detach()
+    _lib.call('fpm_cic_paint_2d', _lib.ptr(out), B, nx, ny,
+              _lib.ptr(part.detach()), part.shape[1], _lib.ptr(w),
+              _lib.ptr(mask), _lib.stream_ptr())
+    ctx.save_for_backward(part, weight, mask)
+    ctx.dims = (B, nx, ny)
+    return out
+
+  @staticmethod
+  def backward(ctx, g):
+    part, weight, mask = ctx.saved_tensors
+    B, nx, ny = ctx.dims
+    g = g.contiguous()
+    lp = torch.empty_like(part) if ctx.needs_input_grad[1] else None
+    lw = (torch.empty_like(weight) if weight is not None and
+          ctx.needs_input_grad[2] else None)
+    if lp is not None or lw is not None:
+      _lib.call('fpm_cic_paint_2d_adjoint', _lib.ptr(g), B, nx, ny,
+                _lib.ptr(part.detach()), part.shape[1],
+                _lib.ptr(None if weight is None else weight.detach()),
+                _lib.ptr(mask), _lib.ptr(lp), _lib.ptr(lw), _lib.stream_ptr())
+    return (g if ctx.needs_input_grad[0] else None), lp, lw, None
+
+
+class DensityPlanes(torch.autograd.Function):
+  """Planes of positions X (batch, npart, 3); ``args`` = the host
+  parameters of fpm_density_planes after X."""
+
+  @staticmethod
+  def forward(ctx, X, args):
+    out = torch.empty(args['shape'], dtype=torch.float32, device=X.device)
+    _lib.call('fpm_density_planes', _lib.ptr(X.detach()), *args['c'],
+              _lib.ptr(out), _lib.stream_ptr())
+    ctx.save_for_backward(X)
+    ctx.args = args
+    return out
+
+  @staticmethod
+  def backward(ctx, g):
+    (X,) = ctx.saved_tensors
+    gX = torch.empty_like(X)
+    _lib.call('fpm_density_planes_adjoint', _lib.ptr(X.detach()),
+              *ctx.args['c'], _lib.ptr(g.contiguous()), _lib.ptr(gX),
+              _lib.stream_ptr())
+    return gX, None
+
+
 class CicReadout(torch.autograd.Function):
 
   @staticmethod

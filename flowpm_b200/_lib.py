@@ -89,6 +89,20 @@ SIGNATURES = {
                                    c_void_p, c_void_p]),
     'fpm_white_noise': (c_int, [c_void_p, c_int64, c_uint64, c_double,
                                 c_void_p]),
+    'fpm_cic_paint_2d': (c_int, [c_void_p, c_int, c_int, c_int, c_void_p,
+                                 c_int64, c_void_p, c_void_p, c_void_p]),
+    'fpm_cic_paint_2d_adjoint': (c_int, [c_void_p, c_int, c_int, c_int,
+                                         c_void_p, c_int64, c_void_p,
+                                         c_void_p, c_void_p, c_void_p,
+                                         c_void_p]),
+    'fpm_density_planes': (c_int, [c_void_p, c_int, c_int64, c_int, c_int,
+                                   c_int, P_double, P_double, c_int,
+                                   P_double, P_double, c_int, c_void_p,
+                                   c_void_p]),
+    'fpm_density_planes_adjoint': (c_int, [c_void_p, c_int, c_int64, c_int,
+                                           c_int, c_int, P_double, P_double,
+                                           c_int, P_double, P_double, c_int,
+                                           c_void_p, c_void_p, c_void_p]),
 }
 
 # Constants of include/flowpm_b200.h.
@@ -96,6 +110,7 @@ FPM_OK = 0
 FPM_ERR_NONFINITE = 6
 FPM_ERR_STATE = 7
 FPM_ERR_LIMIT = 9
+FPM_ERR_RANGE = 10
 FPM_PLAN_CIC_DECONV = 1
 FPM_PLAN_LPT = 2
 FPM_PLAN_GRAD_ORDER0 = 4

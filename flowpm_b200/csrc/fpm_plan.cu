@@ -467,6 +467,7 @@ extern "C" const char* fpm_error_string(int code) {
     case FPM_ERR_UNSUPPORTED: return "unsupported request";
     case FPM_ERR_LIMIT:
       return "request exceeds the fixed scratch of an allocation-free entry";
+    case FPM_ERR_RANGE: return "deposit outside the mesh";
     default: return "unknown error";
   }
 }

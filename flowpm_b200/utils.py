@@ -11,8 +11,8 @@ import torch
 from . import _lib
 from . import _autograd
 
-__all__ = ['cic_paint', 'cic_readout', 'cic_neighbours', 'r2c3d', 'c2r3d',
-           'white_noise', 'compensate_cic']
+__all__ = ['cic_paint', 'cic_paint_2d', 'cic_readout', 'cic_neighbours',
+           'r2c3d', 'c2r3d', 'white_noise', 'compensate_cic']
 
 
 def as_cuda(x, dtype=torch.float32):
@@ -52,6 +52,34 @@ def cic_paint(mesh, part, weight=None, name='CiCPaint'):
   out = mesh.clone()
   _lib.call('fpm_cic_paint', _lib.ptr(out), B, nx, ny, nz, _lib.ptr(part),
             npart, _lib.ptr(w), _lib.stream_ptr())
+  return out
+
+
+def cic_paint_2d(mesh, part, weight=None, mask=None, name='CiCPaint2D'):
+  """Paint particles on a 2-D mesh (flowpm/utils.py:94-160).
+
+  mesh: (batch, nx, ny); part: (batch, npart, 2) in mesh units; weight:
+  (batch, npart) or None; mask: (batch, npart) booleans or None (particles
+  with False are left out).  Indices wrap modulo ny on both axes, as the
+  reference's.  Differentiable in mesh, part and weight."""
+  mesh = as_cuda(mesh)
+  if mesh.dim() != 3 or mesh.dtype != torch.float32:
+    raise ValueError('mesh must be a float32 (batch, nx, ny) tensor')
+  mesh = mesh.contiguous()
+  B, nx, ny = mesh.shape
+  part = as_cuda(part).reshape(B, -1, 2).contiguous()
+  npart = part.shape[1]
+  w = None
+  if weight is not None:
+    w = as_cuda(weight).reshape(B, npart).contiguous()
+  m = None
+  if mask is not None:
+    m = as_cuda(mask, dtype=torch.uint8).reshape(B, npart).contiguous()
+  if _autograd.needs_grad(mesh, part, w):
+    return _autograd.CicPaint2D.apply(mesh, part, w, m)
+  out = mesh.clone()
+  _lib.call('fpm_cic_paint_2d', _lib.ptr(out), B, nx, ny, _lib.ptr(part),
+            npart, _lib.ptr(w), _lib.ptr(m), _lib.stream_ptr())
   return out
 
 

@@ -36,8 +36,11 @@ enum {
   FPM_ERR_NONFINITE = 6,  /* device status: non-finite particle state   */
   FPM_ERR_STATE = 7,      /* call out of order (e.g. missing workspace) */
   FPM_ERR_UNSUPPORTED = 8, /* valid request this build does not handle  */
-  FPM_ERR_LIMIT = 9        /* request larger than the fixed scratch of an
+  FPM_ERR_LIMIT = 9,       /* request larger than the fixed scratch of an
                               allocation-free entry point                  */
+  FPM_ERR_RANGE = 10       /* a deposit fell outside the mesh (2-D paint
+                              with nx < ny, where the reference's indices
+                              wrap by ny); the others were made           */
 };
 
 /* Device status bits accumulated by the kernels of a plan. */
@@ -343,6 +346,44 @@ int fpm_power_spectrum(const float* field, int batch, int nx, int ny, int nz,
  * generator of fpm_linear_field (counter = element index). */
 int fpm_white_noise(float* out, int64_t n, uint64_t seed, double stddev,
                     void* stream);
+
+/* 2-D CIC paint, flowpm/utils.py:94-160 cic_paint_2d: mesh (batch, nx, ny)
+ * += the 4-neighbour CIC weights of part (batch, npart, 2) in mesh units,
+ * times weight (batch, npart; NULL: 1), for the particles whose mask byte
+ * (batch, npart; NULL: all) is non-zero.  Indices wrap modulo ny on both
+ * axes, as the reference's; with nx < ny an x index may reach nx or more,
+ * and such deposits are left out and reported as FPM_ERR_RANGE.
+ * Synchronises the stream. */
+int fpm_cic_paint_2d(float* mesh, int batch, int nx, int ny, const float* part,
+                     int64_t npart, const float* weight, const uint8_t* mask,
+                     void* stream);
+/* Its adjoint for the mesh cotangent grad_mesh: grad_part (batch, npart, 2)
+ * and grad_weight (batch, npart), either may be NULL (not written). */
+int fpm_cic_paint_2d_adjoint(const float* grad_mesh, int batch, int nx,
+                             int ny, const float* part, int64_t npart,
+                             const float* weight, const uint8_t* mask,
+                             float* grad_part, float* grad_weight,
+                             void* stream);
+
+/* Lensing density planes, flowpm/raytracing.py:49-109 density_plane, for
+ * nplanes (<= 64) slabs at once: X (batch, npart, 3) positions in mesh
+ * units; rotation (row-major 3x3, applied as R x) and shift (times
+ * nx, ny, nz), each NULL for none; xy modulo nx, scaled by res / nx;
+ * particles with center - width/2 < z <= center + width/2 painted into
+ * slab p of planes (batch, nplanes, res, res), which is then divided by
+ * (nx / res) (ny / res) width.  Synchronises the stream. */
+int fpm_density_planes(const float* X, int batch, int64_t npart, int nx,
+                       int ny, int nz, const double* rotation,
+                       const double* shift, int nplanes, const double* centers,
+                       const double* widths, int res, float* planes,
+                       void* stream);
+/* Its adjoint: grad_X (batch, npart, 3) for the plane cotangent. */
+int fpm_density_planes_adjoint(const float* X, int batch, int64_t npart,
+                               int nx, int ny, int nz, const double* rotation,
+                               const double* shift, int nplanes,
+                               const double* centers, const double* widths,
+                               int res, const float* grad_planes,
+                               float* grad_X, void* stream);
 
 #ifdef __cplusplus
 }

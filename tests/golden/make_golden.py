@@ -251,6 +251,46 @@ def gen_pgd(tf, m):
   save('pgd.npz', **out)
 
 
+def gen_planes(tf, m):
+  """2-D CIC paint (flowpm/utils.py:94-160 cic_paint_2d) and lensing density
+  planes (flowpm/raytracing.py:49-109 density_plane)."""
+  u = m['utils']
+  sys.modules.setdefault('tensorflow_addons',
+                         types.ModuleType('tensorflow_addons'))
+  rt = importlib.import_module('flowpm.raytracing')
+  rng = np.random.default_rng(77)
+  out = {}
+  pos = (rng.random((2, 600, 2)) * 36 - 6).astype(np.float32)
+  pos[0, :8] = [[0, 0], [23.999999, 0.5], [-0.0, 24.0], [48.5, -24.25],
+                [3.0, 7.0], [11.5, 11.5], [-1e-6, 23.5], [5.25, -0.75]]
+  w = rng.random((2, 600)).astype(np.float32)
+  mask = rng.random((2, 600)) < 0.7
+  out['pos'], out['w'], out['mask'] = pos, w, mask
+  z = tf.zeros((2, 24, 24))
+  out['paint'] = np.asarray(u.cic_paint_2d(z, pos))
+  out['paint_w'] = np.asarray(u.cic_paint_2d(z, pos, weight=w))
+  out['paint_wm'] = np.asarray(u.cic_paint_2d(z, pos, weight=w, mask=mask))
+  # rectangular 24 x 16: the reference wraps both axes by ny
+  posr = np.stack([rng.random(400) * 24, rng.random(400) * 28 - 6],
+                  axis=-1)[None].astype(np.float32)
+  out['pos_rect'] = posr
+  out['paint_rect'] = np.asarray(u.cic_paint_2d(tf.zeros((1, 24, 16)), posr))
+  # density planes of an evolved 32^3 state (the C1 fixture)
+  nb = np.load(os.path.join(HERE, 'nbody.npz'))
+  st = nb['n32_final']
+  out['dp_plane'] = np.asarray(
+      rt.density_plane(st, 32, 16., 8., 48,
+                       shift=np.array([0.3, 0.7, 0.], np.float32)))
+  ang = np.float32(0.5)
+  rot = np.array([[np.cos(ang), -np.sin(ang), 0], [np.sin(ang), np.cos(ang), 0],
+                  [0, 0, 1]], np.float32)
+  out['dp_rot'] = rot
+  out['dp_plane_rot'] = np.asarray(
+      rt.density_plane(st, 32, 26., 4., 40, rotation=rot,
+                       shift=np.array([0.1, 0.2, 0.5], np.float32)))
+  save('planes.npz', **out)
+
+
 def gen_pk(tf, m):
   pk = m['pk']
   nb = np.load(os.path.join(HERE, 'nbody.npz'))
@@ -278,6 +318,7 @@ def main():
   gen_nbody(tf, m)
   gen_pk(tf, m)
   gen_pgd(tf, m)
+  gen_planes(tf, m)
 
 
 if __name__ == '__main__':

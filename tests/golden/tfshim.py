@@ -355,6 +355,11 @@ def where(condition, x=None, y=None, name=None):
                   np.asarray(_t(y, x.dtype))).view(Tensor)
 
 
+def einsum(equation, *inputs, **kwargs):
+  ops = [np.asarray(_t(x)) for x in inputs]
+  return np.einsum(equation, *ops).astype(ops[0].dtype).view(Tensor)
+
+
 def gather(params, indices, axis=0, name=None):
   return np.take(np.asarray(_t(params)), np.asarray(indices),
                  axis=axis).view(Tensor)

@@ -239,3 +239,31 @@ def test_oracle_pgd_golden():
   out = pm.nbody(b, s0, z['stages'], 16, pm_nc_factor=2,
                   pgdparams=z['params']).numpy()
   np.testing.assert_allclose(out, z['final_b2'], atol=5e-3)
+
+
+def test_oracle_planes_golden():
+  """2-D CIC paint (flowpm/utils.py:94-160) and density planes
+  (flowpm/raytracing.py:49-109): the oracle against the reference's own
+  output (weights, mask, the rectangular wrap by ny, shift, rotation)."""
+  from oracle import planes
+  z, nb = golden('planes'), golden('nbody')
+  zz = np.zeros((2, 24, 24), np.float32)
+  pos = torch.tensor(z['pos'])
+  assert_allclose(planes.cic_paint_2d(zz, pos).numpy(), z['paint'],
+                  atol=2e-6)
+  assert_allclose(planes.cic_paint_2d(zz, pos, weight=z['w']).numpy(),
+                  z['paint_w'], atol=2e-6)
+  assert_allclose(
+      planes.cic_paint_2d(zz, pos, weight=z['w'], mask=z['mask']).numpy(),
+      z['paint_wm'], atol=2e-6)
+  assert_allclose(
+      planes.cic_paint_2d(np.zeros((1, 24, 16), np.float32),
+                          torch.tensor(z['pos_rect'])).numpy(),
+      z['paint_rect'], atol=2e-6)
+  st = torch.tensor(nb['n32_final'])
+  out = planes.density_plane(st, 32, 16., 8., 48,
+                             shift=np.array([0.3, 0.7, 0.], np.float32))
+  assert_allclose(out.numpy(), z['dp_plane'], rtol=1e-5, atol=1e-5)
+  out = planes.density_plane(st, 32, 26., 4., 40, rotation=z['dp_rot'],
+                             shift=np.array([0.1, 0.2, 0.5], np.float32))
+  assert_allclose(out.numpy(), z['dp_plane_rot'], rtol=1e-5, atol=1e-5)
