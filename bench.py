@@ -61,6 +61,10 @@ def parse():
   ap.add_argument('--no-extras', action='store_true',
                   help='skip the C4 (forward + adjoint) and C3 (batched) '
                   'measurements')
+  ap.add_argument('--mesh', type=int, default=N_MESH,
+                  help='mesh (= particle lattice) per side of the forward '
+                  'workload, box scaled to keep the C2 spacing; for '
+                  'profiling other sizes (C2 is 128)')
   return ap.parse_args()
 
 
@@ -549,11 +553,13 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
             _lib.ptr(F), None, 0, None, 0, st)
   torch.cuda.synchronize()
   kt = {}
-  for kind, name in [(0, 'step'), (1, 'fourier'), (2, 'paint')]:
+  for kind, name in [(0, 'step'), (1, 'fourier'), (2, 'paint'),
+                     (3, 'green'), (4, 'stencil')]:
     tot, cnt = _lib.c_double(), _lib.c_int64()
     _lib.call('fpm_plan_profile_read', plan.handle, kind,
               _lib.ctypes.byref(tot), _lib.ctypes.byref(cnt))
-    kt[name] = (tot.value / max(cnt.value, 1), cnt.value)
+    if cnt.value:
+      kt[name] = (tot.value / cnt.value, cnt.value)
   _lib.call('fpm_plan_profile', plan.handle, 0)
   kb, pk = fpm.power_spectrum(rho, kmin=0.01, dk=0.01, boxsize=[box] * 3)
   peak, peak_kind = peaks()
@@ -561,11 +567,16 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
   # algorithmic bytes per launch: step 64 B / particle (Np = Nc), paint
   # 12 Np + 4 Nc; the Fourier solve (density -> three force meshes, all of
   # its transforms and kernels) reads and zeroes the density and writes the
-  # three force meshes, 20 Nc
+  # three force meshes, 20 Nc; its Green's-function kernel reads and writes
+  # the half spectrum (8 B per mode each) and zeroes the density, its
+  # stencil reads the potential and writes the three force meshes
+  half = 2 * n * n * (n // 2 + 1)
   kbytes = {
       'step': KERNEL_BYTES_PER_PART * tot_np,
       'paint': 12 * tot_np + 4 * nc_tot,
       'fourier': 20 * nc_tot,
+      'green': 16 * half + 4 * nc_tot,
+      'stencil': 16 * nc_tot,
   }
   roof = {}
   for k, (ms, cnt) in kt.items():
@@ -599,8 +610,15 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
 
 
 def main():
+  global N_MESH, BOX, WORKLOAD
   args = parse()
   rank, world, local = dist_env()
+  if args.mesh != N_MESH:
+    BOX = BOX * args.mesh / N_MESH
+    N_MESH = args.mesh
+    WORKLOAD = ('forward PM, %d^3 particles / %d^3 mesh, box %g Mpc/h, '
+                'Planck15, 2LPT at a0=0.1, 40 KDK steps to a=1 (the C2 '
+                'workload at another size)' % (N_MESH, N_MESH, BOX))
   if args.impl == 'reference':
     run_reference(args, rank, world)
     return

@@ -319,6 +319,69 @@ __device__ __forceinline__ float stencil4(float m2, float m1, float p1,
                    1.0f / 12.0f);
 }
 
+// k_stencil_grad with four z-consecutive cells per thread, for plans whose
+// meshes all have mz % 4 == 0 and m_off % 4 == 0: 11 float4 loads (the 4
+// x neighbours, the 4 y neighbours, and the z window [z0 - 4, z0 + 8) of
+// the row) and 3 float4 stores per quad, one index decomposition per quad.
+// One mesh chunk (kChunk cells) = one quad per thread.
+__device__ __forceinline__ float4 stencil4v(float4 m2, float4 m1, float4 p1,
+                                           float4 p2) {
+  return make_float4(stencil4(m2.x, m1.x, p1.x, p2.x),
+                     stencil4(m2.y, m1.y, p1.y, p2.y),
+                     stencil4(m2.z, m1.z, p1.z, p2.z),
+                     stencil4(m2.w, m1.w, p1.w, p2.w));
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_stencil_grad4(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+                const float* __restrict__ phi, float* __restrict__ fmesh,
+                const int32_t* __restrict__ nsteps, int pos, int skip_fused) {
+  static_assert(kChunk == 4 * kThreads, "one quad per thread and chunk");
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kMesh);
+    if (nsteps && pos > nsteps[s]) continue;
+    const SimDev S = sims[s];
+    if (skip_fused && S.fused) continue;
+    const unsigned my = S.my, mz = S.mz, mx = S.mx;
+    const unsigned sx = my * mz, mcells = mx * sx;
+    const unsigned c = ((unsigned)(ch - S.ch_m) * kThreads + threadIdx.x) * 4;
+    if (c >= mcells) continue;
+    const float* f = phi + S.m_off;
+    const unsigned t = c / mz;
+    const unsigned z = c - t * mz;
+    const unsigned x = t / my;
+    const unsigned y = t - x * my;
+    const unsigned rx = c - x * sx, ry = c - y * mz, rz = c - z;
+    const unsigned xm2 = (x >= 2 ? x - 2 : x + mx - 2) * sx;
+    const unsigned xm1 = (x >= 1 ? x - 1 : x + mx - 1) * sx;
+    const unsigned xp1 = (x + 1 < mx ? x + 1 : x + 1 - mx) * sx;
+    const unsigned xp2 = (x + 2 < mx ? x + 2 : x + 2 - mx) * sx;
+    const unsigned ym2 = (y >= 2 ? y - 2 : y + my - 2) * mz;
+    const unsigned ym1 = (y >= 1 ? y - 1 : y + my - 1) * mz;
+    const unsigned yp1 = (y + 1 < my ? y + 1 : y + 1 - my) * mz;
+    const unsigned yp2 = (y + 2 < my ? y + 2 : y + 2 - my) * mz;
+    const unsigned zl = z >= 4 ? z - 4 : z + mz - 4;
+    const unsigned zr = z + 4 < mz ? z + 4 : z + 4 - mz;
+    auto ld4 = [&](unsigned o) {
+      return __ldg(reinterpret_cast<const float4*>(f + o));
+    };
+    const float4 gx = stencil4v(ld4(xm2 + rx), ld4(xm1 + rx), ld4(xp1 + rx),
+                                ld4(xp2 + rx));
+    const float4 gy = stencil4v(ld4(ym2 + ry), ld4(ym1 + ry), ld4(yp1 + ry),
+                                ld4(yp2 + ry));
+    const float4 L = ld4(rz + zl), C = ld4(c), R = ld4(rz + zr);
+    // row window w[0..11] = L, C, R; cell z + i sits at w[4 + i]
+    const float4 gz = make_float4(stencil4(L.z, L.w, C.y, C.z),
+                                  stencil4(L.w, C.x, C.z, C.w),
+                                  stencil4(C.x, C.y, C.w, R.x),
+                                  stencil4(C.y, C.z, R.x, R.y));
+    float* o0 = fmesh + 3 * S.m_off;
+    reinterpret_cast<float4*>(o0 + c)[0] = gx;
+    reinterpret_cast<float4*>(o0 + mcells + c)[0] = gy;
+    reinterpret_cast<float4*>(o0 + 2 * mcells + c)[0] = gz;
+  }
+}
+
 // Three force meshes f_d = D_d phi of each simulation (sim s: planes at
 // fmesh + 3 m_off + d mcells).  With nsteps, finished simulations skip.
 // 32-bit offsets inside a simulation's mesh.
@@ -654,10 +717,15 @@ void launch_fourier_potential(const SimDev* sims, int nsims, int64_t nchunks,
 
 void launch_stencil_grad(const SimDev* sims, int nsims, int64_t nchunks,
                          const float* phi, float* fmesh, const int32_t* nsteps,
-                         int pos, int skip_fused, cudaStream_t st) {
+                         int pos, int skip_fused, bool quads,
+                         cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_stencil_grad<<<grid_for(nchunks), kThreads, 0, st>>>(
-      sims, nsims, nchunks, phi, fmesh, nsteps, pos, skip_fused);
+  if (quads)
+    k_stencil_grad4<<<grid_for(nchunks), kThreads, 0, st>>>(
+        sims, nsims, nchunks, phi, fmesh, nsteps, pos, skip_fused);
+  else
+    k_stencil_grad<<<grid_for(nchunks), kThreads, 0, st>>>(
+        sims, nsims, nchunks, phi, fmesh, nsteps, pos, skip_fused);
 }
 
 void launch_stencil_div(const SimDev* sims, int nsims, int64_t nchunks,

@@ -54,11 +54,13 @@ void launch_fourier_potential(const SimDev* sims, int nsims, int64_t nchunks,
                               const int32_t* nsteps, int pos, int skip_fused,
                               cudaStream_t st);
 
-// f_d = D_d phi with the 4-point stencil (nchunks = mesh chunks), and its
+// f_d = D_d phi with the 4-point stencil (nchunks = mesh chunks; quads:
+// four cells per thread, every mesh with mz % 4 == 0 and m_off % 4 == 0),
+// and its
 // adjoint lphi = -sum_d D_d lf_d (lf interleaved: float4 per cell).
 void launch_stencil_grad(const SimDev* sims, int nsims, int64_t nchunks,
                          const float* phi, float* fmesh, const int32_t* nsteps,
-                         int pos, int skip_fused, cudaStream_t st);
+                         int pos, int skip_fused, bool quads, cudaStream_t st);
 void launch_stencil_div(const SimDev* sims, int nsims, int64_t nchunks,
                         const float* lf, float* lphi, const int32_t* nsteps,
                         int pos, cudaStream_t st);

@@ -24,7 +24,9 @@ using namespace fpm;
 namespace {
 
 // Kernels timed by fpm_plan_profile.
-constexpr int kProfKinds = 3;  // 0 step, 1 Fourier solve, 2 initial paint
+// 0 step, 1 Fourier solve, 2 initial paint, and on the cuFFT path of the
+// solve 3 the Green's-function kernel, 4 the stencil gradient kernel
+constexpr int kProfKinds = 5;
 
 struct Run {
   int first, count;        // simulations [first, first + count)
@@ -73,6 +75,7 @@ struct fpm_plan {
   float2* fk = nullptr;
   float* fmesh = nullptr;
   float* phi = nullptr;     // potential mesh (stencil force path)
+  bool quads = false;       // every mesh: mz % 4 == 0 and m_off % 4 == 0
   // lattice buffers (FPM_PLAN_LPT)
   float* lreal1 = nullptr;
   float2* lspec1 = nullptr;
@@ -107,7 +110,7 @@ struct fpm_plan {
   // optional per-kernel timing (fpm_plan_profile)
   bool profile = false;
   std::vector<cudaEvent_t> ev[kProfKinds];
-  size_t ev_used[kProfKinds] = {0, 0, 0};
+  size_t ev_used[kProfKinds] = {0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -304,6 +307,7 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
     FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->rho + S.m_off,
                      p->dk + S.s_off, st));
   }
+  prof_mark(p, 3, st);
   if (stencil_path(p)) {
     launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
                              zero_rho ? p->rho : nullptr, tabs_of(p), G, act,
@@ -313,6 +317,7 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
                          zero_rho ? p->rho : nullptr, tabs_of(p), r2, deconv,
                          act, it, 1, st);
   }
+  prof_mark(p, 3, st);
   FPM_TRY(launch_ok());
   for (auto& r : p->runs) {
     if (r.fused) continue;
@@ -327,8 +332,10 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
                        p->fmesh + 3 * S.m_off, st));
   }
   if (stencil_path(p)) {
+    prof_mark(p, 4, st);
     launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, p->phi, p->fmesh, act,
-                        it, 1, st);
+                        it, 1, p->quads, st);
+    prof_mark(p, 4, st);
     FPM_TRY(launch_ok());
   }
   prof_mark(p, 1, st);
@@ -381,7 +388,7 @@ int pgd_meshes(fpm_plan* p, cudaStream_t st, int pos) {
                      p->phi + S.m_off, st));
   }
   launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, p->phi, p->fmesh, act,
-                      apos, 1, st);
+                      apos, 1, p->quads, st);
   return launch_ok();
 }
 
@@ -556,6 +563,9 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
     }
   }
 
+  p->quads = true;
+  for (const SimDev& S : p->sims)
+    if (S.mz % 4 != 0 || S.m_off % 4 != 0) p->quads = false;
   int rc = FPM_OK;
   size_t ws = 0;
   const bool lpt = (flags & FPM_PLAN_LPT) != 0;

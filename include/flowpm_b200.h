@@ -158,7 +158,8 @@ int fpm_plan_status(fpm_plan* plan, int32_t* status, void* stream);
  * pair around every launch of the fused step kernel (kind 0), every
  * Fourier solve -- density to the three force meshes, all of its
  * transforms and kernels (kind 1) -- and the initial paint (kind 2) on the
- * call's stream.  fpm_plan_profile_read waits for the last event, returns the
+ * call's stream; for meshes on the cuFFT path also around the
+ * Green's-function kernel (kind 3) and the stencil gradient (kind 4).  fpm_plan_profile_read waits for the last event, returns the
  * summed device time and the number of timed launches of `kind`, and
  * resets that kind.  Not for use under CUDA graph capture. */
 int fpm_plan_profile(fpm_plan* plan, int enable);
