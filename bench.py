@@ -529,7 +529,7 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
   target = rho + torch.randn(rho.shape, generator=gen, device='cuda')
   status = plan.status(st)
 
-  def fwd_adj():
+  def fwd_seed():  # forward, chi^2 and its cotangents at the final state
     forward()
     density()
     g.copy_(rho)
@@ -538,6 +538,9 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
               np_, None, _lib.ptr(LX), None, st)
     _lib.call('fpm_saxpy', _lib.ptr(LX), _lib.ptr(LX), 1.0, LX.numel(), st)
     LP.zero_()
+
+  def fwd_adj():
+    fwd_seed()
     _lib.call('fpm_graph_launch', ga, st)
 
   fwd_adj()
@@ -553,13 +556,29 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
             _lib.ptr(F), None, 0, None, 0, st)
   torch.cuda.synchronize()
   kt = {}
-  for kind, name in [(0, 'step'), (1, 'fourier'), (2, 'paint'),
-                     (3, 'green'), (4, 'stencil')]:
-    tot, cnt = _lib.c_double(), _lib.c_int64()
-    _lib.call('fpm_plan_profile_read', plan.handle, kind,
-              _lib.ctypes.byref(tot), _lib.ctypes.byref(cnt))
-    if cnt.value:
-      kt[name] = (tot.value / cnt.value, cnt.value)
+
+  def read_kinds(kinds):
+    for kind, name in kinds:
+      tot, cnt = _lib.c_double(), _lib.c_int64()
+      _lib.call('fpm_plan_profile_read', plan.handle, kind,
+                _lib.ctypes.byref(tot), _lib.ctypes.byref(cnt))
+      if cnt.value:
+        kt[name] = (tot.value / cnt.value, cnt.value)
+
+  read_kinds([(0, 'step'), (1, 'fourier'), (2, 'paint'), (3, 'green'),
+              (4, 'stencil')])
+  # and of one reverse sweep (from the checkpointed forward run)
+  _lib.call('fpm_plan_profile', plan.handle, 0)
+  fwd_seed()
+  _lib.call('fpm_plan_profile', plan.handle, 1)
+  torch.cuda._sleep(100_000_000)
+  _lib.call('fpm_nbody_adjoint', plan.handle, _lib.ptr(D), _lib.ptr(P),
+            _lib.ptr(F), _lib.ptr(LX), _lib.ptr(LP), None, _lib.ptr(ck), ckpt,
+            st)
+  torch.cuda.synchronize()
+  read_kinds([(5, 'adj_drift_paint'), (6, 'adj_vjp'), (7, 'adj_div'),
+              (8, 'adj_potential'), (9, 'adj_position'),
+              (1, 'adj_force_solve')])
   _lib.call('fpm_plan_profile', plan.handle, 0)
   kb, pk = fpm.power_spectrum(rho, kmin=0.01, dk=0.01, boxsize=[box] * 3)
   peak, peak_kind = peaks()
@@ -569,7 +588,15 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
   # its transforms and kernels) reads and zeroes the density and writes the
   # three force meshes, 20 Nc; its Green's-function kernel reads and writes
   # the half spectrum (8 B per mode each) and zeroes the density, its
-  # stencil reads the potential and writes the three force meshes
+  # stencil reads the potential and writes the three force meshes.
+  # Reverse sweep, per particle (Np = Nc): the drift + paint kernel reads
+  # d, F and reads and writes lam_x, p, lam_p (12 B each way), writes d,
+  # gathers the adjoint density and paints (4 B per cell each), 116 B; the
+  # VJP reads d, lam_p, the three force meshes (12 B per cell), reads and
+  # writes lam_x and p, writes F and reduces into the adjoint force mesh
+  # (16 B per cell), 112 B; the divergence stencil reads that mesh and
+  # writes the adjoint potential, 20 B per cell; the adjoint potential solve
+  # reads it and writes the adjoint density, 8 B per cell.
   half = 2 * n * n * (n // 2 + 1)
   kbytes = {
       'step': KERNEL_BYTES_PER_PART * tot_np,
@@ -577,9 +604,17 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
       'fourier': 20 * nc_tot,
       'green': 16 * half + 4 * nc_tot,
       'stencil': 16 * nc_tot,
+      'adj_drift_paint': 116 * tot_np,
+      'adj_vjp': 112 * tot_np,
+      'adj_div': 20 * nc_tot,
+      'adj_potential': 8 * nc_tot,
+      'adj_force_solve': 20 * nc_tot,
   }
   roof = {}
   for k, (ms, cnt) in kt.items():
+    if k not in kbytes:
+      roof[k] = {'avg_launch_ms': ms, 'launches': cnt}
+      continue
     gbs = kbytes[k] / (ms * 1e-3) / 1e9
     roof[k] = {'avg_launch_ms': ms, 'launches': cnt,
                'algorithmic_bytes': kbytes[k], 'achieved_gbs': gbs,

@@ -239,7 +239,12 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 // after the readout phase of the whole block, directly or through a
 // shared-memory tile of the block's cells, was slower (103 and 144 vs 87 us
 // per step): the paint's reductions overlap the readout's gathers best when
-// each warp issues both, particle by particle.
+// each warp issues both, particle by particle.  Neither more memory-level
+// parallelism (items unrolled by 2, at 64 or 80 registers; the next
+// particle's state prefetched into L1; reductions without a compiler memory
+// barrier) nor an interleaved force mesh (one float4 (f_x, f_y, f_z, 0) per
+// cell, 8 gathers per readout instead of 24) moved k_step by more than 1-3 %
+// at 128^3 and 256^3: it is not latency-bound and not bound by its gathers.
 #ifndef FPM_STEP_MINBLOCKS
 #define FPM_STEP_MINBLOCKS 4   // resident blocks of 256 threads per SM
 #endif

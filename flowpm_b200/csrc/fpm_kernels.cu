@@ -485,6 +485,115 @@ k_stencil_div(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
   }
 }
 
+// k_stencil_div for large meshes (my % 16 == 0, mz % 64 == 0, mx % XC == 0,
+// m_off % 4 == 0): a block owns a 16 x 64 (y, z) tile and marches over XC
+// x planes.  The x stencil of lf_x comes from a window of five planes in
+// registers; lf_y and lf_z of the current plane, with a halo of two cells
+// in y (lf_y) and z (lf_z), from a ring of three planes in shared memory,
+// so every float4 cell is read about once.  Thread (ty, tq) owns cells
+// (y0 + ty, z0 + tq + 16 i), i < 4: consecutive lanes on consecutive
+// cells for the loads and conflict-free shared reads.  Same arithmetic as
+// k_stencil_div, bit for bit.
+constexpr int kDivTY = 16, kDivTZ = 64;  // tile
+constexpr int kDivRS = 80;               // shared row stride (floats)
+constexpr int kDivRows = kDivTY + 4;
+
+template <int XC>
+__global__ void __launch_bounds__(256, 3)
+k_stencil_div_tiled(const SimDev* __restrict__ sims, int first,
+                    const float* __restrict__ lf, float* __restrict__ lphi,
+                    const int32_t* __restrict__ nsteps, int pos) {
+  __shared__ float sy[3][kDivRows][kDivRS];
+  __shared__ float sz[3][kDivRows][kDivRS];
+  const int s = first + blockIdx.y;
+  if (nsteps && pos > nsteps[s]) return;
+  const SimDev& S = sims[s];
+  const int mx = S.mx, my = S.my, mz = S.mz;
+  const int nzt = mz / kDivTZ, nyt = my / kDivTY;
+  int b = blockIdx.x;
+  const int z0 = (b % nzt) * kDivTZ;
+  b /= nzt;
+  const int y0 = (b % nyt) * kDivTY;
+  const int x0 = (b / nyt) * XC;
+  const int ty = threadIdx.x >> 4, tq = threadIdx.x & 15;
+  const float4* L = reinterpret_cast<const float4*>(lf) + S.m_off;
+  const unsigned sx = (unsigned)my * (unsigned)mz;
+  const unsigned own = (unsigned)(y0 + ty) * mz + z0 + tq;
+  // halo cells of this thread: y halo row hy (lf_y), z halo cell hz (lf_z)
+  const int hr = threadIdx.x >> 6, hc = threadIdx.x & 63;
+  const int hyrow = hr < 2 ? hr : kDivTY + hr;  // tile rows -2,-1,16,17
+  const unsigned hyoff = (unsigned)((y0 - 2 + hyrow + my) % my) * mz + z0 + hc;
+  const bool zh = threadIdx.x < 4 * kDivTY;
+  const int zr = threadIdx.x >> 2, zk = threadIdx.x & 3;
+  const int zcol = zk < 2 ? zk : kDivTZ + zk;   // tile cols -2,-1,64,65
+  const unsigned zhoff =
+      (unsigned)(y0 + (zh ? zr : 0)) * mz + (unsigned)((z0 - 2 + zcol + mz) % mz);
+  auto plane = [&](int x) {
+    return L + (size_t)(unsigned)((x % mx + mx) % mx) * sx;
+  };
+  float xw[5][4];
+  float4 v[4];
+  float hyv = 0.f, hzv = 0.f;
+  auto load = [&](int x, bool halo) {
+    const float4* P = plane(x);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = __ldg(P + own + 16 * i);
+    if (halo) {
+      hyv = __ldg(reinterpret_cast<const float*>(P + hyoff) + 1);
+      if (zh) hzv = __ldg(reinterpret_cast<const float*>(P + zhoff) + 2);
+    }
+  };
+  auto put = [&](int slot) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      sy[slot][ty + 2][tq + 16 * i + 2] = v[i].y;
+      sz[slot][ty + 2][tq + 16 * i + 2] = v[i].z;
+    }
+    sy[slot][hyrow][hc + 2] = hyv;
+    if (zh) sz[slot][zr + 2][zcol] = hzv;
+  };
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {  // planes x0 - 2 .. x0 + 2
+    load(x0 - 2 + k, k >= 2);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) xw[k][i] = v[i].x;
+    if (k >= 2) put(k - 2);
+  }
+  __syncthreads();
+  float* out = lphi + S.m_off + own;
+#pragma unroll 1
+  for (int p = 0; p < XC; ++p) {
+    const int slot = p % 3;
+    const bool next = p + 3 <= XC + 1;  // plane x0 + p + 3 enters the window
+    const bool next_slot = p + 3 < XC;  // and is processed
+    if (next) load(x0 + p + 3, next_slot);
+    const int r = ty + 2;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = tq + 16 * i + 2;
+      const float a = stencil4(xw[0][i], xw[1][i], xw[3][i], xw[4][i]);
+      const float bb = stencil4(sy[slot][r - 2][c], sy[slot][r - 1][c],
+                                sy[slot][r + 1][c], sy[slot][r + 2][c]);
+      const float cz = stencil4(sz[slot][r][c - 2], sz[slot][r][c - 1],
+                                sz[slot][r][c + 1], sz[slot][r][c + 2]);
+      out[(size_t)(unsigned)(x0 + p) * sx + 16 * i] = -((a + bb) + cz);
+    }
+    __syncthreads();  // every thread is done with this slot
+    if (next) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        xw[0][i] = xw[1][i];
+        xw[1][i] = xw[2][i];
+        xw[2][i] = xw[3][i];
+        xw[3][i] = xw[4][i];
+        xw[4][i] = v[i].x;
+      }
+      if (next_slot) put(slot);
+    }
+    // the next plane reads another slot, written two planes ago
+  }
+}
+
 // LPT spectra (flowpm/tfpm.py:66-145 lpt1 / lpt2_source on the lattice).
 __global__ void __launch_bounds__(kThreads)
 k_lpt_fourier(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
@@ -734,6 +843,30 @@ void launch_stencil_div(const SimDev* sims, int nsims, int64_t nchunks,
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_stencil_div<<<grid_for(nchunks), kThreads, 0, st>>>(
       sims, nsims, nchunks, lf, lphi, nsteps, pos);
+}
+
+int stencil_div_chunk(int mx, int my, int mz, int64_t m_off, int count) {
+  if (my % kDivTY != 0 || mz % kDivTZ != 0 || m_off % 4 != 0) return 0;
+  const int64_t tiles = (int64_t)(my / kDivTY) * (mz / kDivTZ) * count;
+  for (int xc : {32, 16})
+    if (mx % xc == 0 && mx >= xc && tiles * (mx / xc) >= 2 * kNumSMs)
+      return xc;
+  return 0;
+}
+
+void launch_stencil_div_tiled(const SimDev* sims, int first, int count,
+                              int mx, int my, int mz, int xc, const float* lf,
+                              float* lphi, const int32_t* nsteps, int pos,
+                              cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const dim3 grid((unsigned)((mx / xc) * (my / kDivTY) * (mz / kDivTZ)),
+                  (unsigned)count);
+  if (xc == 32)
+    k_stencil_div_tiled<32><<<grid, 256, 0, st>>>(sims, first, lf, lphi,
+                                                  nsteps, pos);
+  else
+    k_stencil_div_tiled<16><<<grid, 256, 0, st>>>(sims, first, lf, lphi,
+                                                  nsteps, pos);
 }
 
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,

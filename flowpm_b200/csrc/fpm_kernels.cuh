@@ -64,6 +64,14 @@ void launch_stencil_grad(const SimDev* sims, int nsims, int64_t nchunks,
 void launch_stencil_div(const SimDev* sims, int nsims, int64_t nchunks,
                         const float* lf, float* lphi, const int32_t* nsteps,
                         int pos, cudaStream_t st);
+// Tiled k_stencil_div over the sims [first, first + count) of one mesh
+// shape; stencil_div_chunk gives its x chunk (0: shape not supported, use
+// launch_stencil_div).
+int stencil_div_chunk(int mx, int my, int mz, int64_t m_off, int count);
+void launch_stencil_div_tiled(const SimDev* sims, int first, int count,
+                              int mx, int my, int mz, int xc, const float* lf,
+                              float* lphi, const int32_t* nsteps, int pos,
+                              cudaStream_t st);
 
 // Fused Fourier solve (fpm_fft.cu) for meshes with every axis a power of
 // two in [16, 128]: density -> three force meshes (the transfer function of

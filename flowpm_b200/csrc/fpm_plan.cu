@@ -25,12 +25,15 @@ namespace {
 
 // Kernels timed by fpm_plan_profile.
 // 0 step, 1 Fourier solve, 2 initial paint, and on the cuFFT path of the
-// solve 3 the Green's-function kernel, 4 the stencil gradient kernel
-constexpr int kProfKinds = 5;
+// solve 3 the Green's-function kernel, 4 the stencil gradient kernel;
+// reverse sweep: 5 reverse drift + paint, 6 force VJP, 7 divergence
+// stencil, 8 adjoint potential solve, 9 the whole reverse step
+constexpr int kProfKinds = 10;
 
 struct Run {
   int first, count;        // simulations [first, first + count)
   bool fused = false;      // force meshes by the fused Fourier solve
+  int div_xc = 0;          // x chunk of the tiled divergence stencil
   // Simulations of the run still active at leapfrog position it (a prefix
   // when the run is ordered by non-increasing step count), and the batched
   // cuFFT plans of each smaller active count.
@@ -76,6 +79,7 @@ struct fpm_plan {
   float* fmesh = nullptr;
   float* phi = nullptr;     // potential mesh (stencil force path)
   bool quads = false;       // every mesh: mz % 4 == 0 and m_off % 4 == 0
+  bool div_tiled = false;   // every run takes the tiled divergence stencil
   // lattice buffers (FPM_PLAN_LPT)
   float* lreal1 = nullptr;
   float2* lspec1 = nullptr;
@@ -110,7 +114,7 @@ struct fpm_plan {
   // optional per-kernel timing (fpm_plan_profile)
   bool profile = false;
   std::vector<cudaEvent_t> ev[kProfKinds];
-  size_t ev_used[kProfKinds] = {0, 0, 0, 0, 0};
+  size_t ev_used[kProfKinds] = {};
 };
 
 namespace {
@@ -566,6 +570,14 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
   p->quads = true;
   for (const SimDev& S : p->sims)
     if (S.mz % 4 != 0 || S.m_off % 4 != 0) p->quads = false;
+  p->div_tiled = true;
+  for (auto& r : p->runs) {
+    const SimDev& S0 = p->sims[r.first];
+    r.div_xc = stencil_div_chunk(S0.mx, S0.my, S0.mz, S0.m_off, r.count);
+    for (int s = r.first; s < r.first + r.count; ++s)
+      if (p->sims[s].m_off % 4 != 0) r.div_xc = 0;
+    if (r.div_xc == 0) p->div_tiled = false;
+  }
   int rc = FPM_OK;
   size_t ws = 0;
   const bool lpt = (flags & FPM_PLAN_LPT) != 0;
@@ -896,6 +908,91 @@ extern "C" int fpm_nbody(fpm_plan* p, float* disp, float* mom, float* force,
   return fpm_nbody_run(p, disp, mom, force, inter, flags, nullptr, 0, stream);
 }
 
+// One position of the reverse sweep (flowpm's nbody adjoint, see
+// fpm_nbody_adjoint): reverse drift and paint of x_it, its force meshes,
+// the force VJP into the adjoint force meshes, and their adjoint density
+// lrho for the next (earlier) position.
+static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
+  const double r2 = p->r_split * p->r_split;
+  const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
+  FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
+  prof_mark(p, 5, st);
+  launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
+  prof_mark(p, 5, st);
+  FPM_TRY(launch_ok());
+  FPM_TRY(force_meshes(p, st, false, it));
+  FPM_CUDA(cudaMemsetAsync(p->lmesh, 0,
+                           sizeof(float) * (a.lvec4 ? 4 : 3) * p->total_m,
+                           st));
+  prof_mark(p, 6, st);
+  launch_adj_vjp(p->d_sims, p->nsims, traverse_chunks(p), a, st);
+  prof_mark(p, 6, st);
+  FPM_TRY(launch_ok());
+  const int32_t* act = p->d_nsteps;
+  if (stencil_path(p)) {
+    // lphi = -sum_d D_d lf_d, then lrho = pre C2R(w R2C(lphi))
+    prof_mark(p, 7, st);
+    if (p->div_tiled) {
+      for (auto& r : p->runs) {
+        const int n = run_active(r, it);
+        if (n == 0) continue;
+        const SimDev& S = p->sims[r.first];
+        launch_stencil_div_tiled(p->d_sims, r.first, n, S.mx, S.my, S.mz,
+                                 r.div_xc, p->lmesh, p->phi, act, it, st);
+      }
+    } else {
+      launch_stencil_div(p->d_sims, p->nsims, p->ch_m, p->lmesh, p->phi, act,
+                         it, st);
+    }
+    prof_mark(p, 7, st);
+    FPM_TRY(launch_ok());
+    prof_mark(p, 8, st);
+    bool any_cufft = false;
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      const int n = run_active(r, it);
+      if (n == 0) continue;
+      if (r.fused) {  // lrho straight from lphi
+        launch_fft_potential(p->d_sims, r.first, n, S.mx, S.my, S.mz,
+                             p->phi, p->dk, p->lrho, tabs_of(p),
+                             plan_green(p), st);
+        continue;
+      }
+      any_cufft = true;
+      FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->phi + S.m_off,
+                       p->dk + S.s_off, st));
+    }
+    FPM_TRY(launch_ok());
+    if (any_cufft) {
+      launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->dk,
+                               nullptr, tabs_of(p), plan_green(p), act, it, 1,
+                               st);
+      FPM_TRY(launch_ok());
+    }
+  } else {
+    prof_mark(p, 8, st);
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      const int n = run_active(r, it);
+      if (n == 0) continue;
+      FPM_TRY(exec_r2c(pick(r, n, r.r2c3, r.r2c3_n), p->lmesh + 3 * S.m_off,
+                       p->fk + 3 * S.s_off, st));
+    }
+    launch_adj_fourier(p->d_sims, p->nsims, p->ch_s, p->fk, p->dk,
+                       tabs_of(p), r2, deconv, st);
+    FPM_TRY(launch_ok());
+  }
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    const int n = run_active(r, it);
+    if (n == 0 || (r.fused && stencil_path(p))) continue;
+    FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->dk + S.s_off,
+                     p->lrho + S.m_off, st));
+  }
+  prof_mark(p, 8, st);
+  return FPM_OK;
+}
+
 extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
                                  const float* force, float* lam_x,
                                  float* lam_p, const float* lam_f,
@@ -929,65 +1026,11 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   a.status = p->d_status;
   a.total_np = p->total_np;
   a.max_steps = p->max_steps;
-  const double r2 = p->r_split * p->r_split;
-  const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
   for (int it = p->max_steps; it >= 0; --it) {
     a.it = it;
-    FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
-    launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
-    FPM_TRY(launch_ok());
-    FPM_TRY(force_meshes(p, st, false, it));
-    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0,
-                             sizeof(float) * (a.lvec4 ? 4 : 3) * p->total_m,
-                             st));
-    launch_adj_vjp(p->d_sims, p->nsims, traverse_chunks(p), a, st);
-    FPM_TRY(launch_ok());
-    const int32_t* act = p->d_nsteps;
-    if (stencil_path(p)) {
-      // lphi = -sum_d D_d lf_d, then lrho = pre C2R(w R2C(lphi))
-      launch_stencil_div(p->d_sims, p->nsims, p->ch_m, p->lmesh, p->phi, act,
-                         it, st);
-      FPM_TRY(launch_ok());
-      bool any_cufft = false;
-      for (auto& r : p->runs) {
-        const SimDev& S = p->sims[r.first];
-        const int n = run_active(r, it);
-        if (n == 0) continue;
-        if (r.fused) {  // lrho straight from lphi
-          launch_fft_potential(p->d_sims, r.first, n, S.mx, S.my, S.mz,
-                               p->phi, p->dk, p->lrho, tabs_of(p),
-                               plan_green(p), st);
-          continue;
-        }
-        any_cufft = true;
-        FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->phi + S.m_off,
-                         p->dk + S.s_off, st));
-      }
-      FPM_TRY(launch_ok());
-      if (!any_cufft) continue;
-      launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->dk,
-                               nullptr, tabs_of(p), plan_green(p), act, it, 1,
-                               st);
-      FPM_TRY(launch_ok());
-    } else {
-      for (auto& r : p->runs) {
-        const SimDev& S = p->sims[r.first];
-        const int n = run_active(r, it);
-        if (n == 0) continue;
-        FPM_TRY(exec_r2c(pick(r, n, r.r2c3, r.r2c3_n), p->lmesh + 3 * S.m_off,
-                         p->fk + 3 * S.s_off, st));
-      }
-      launch_adj_fourier(p->d_sims, p->nsims, p->ch_s, p->fk, p->dk,
-                         tabs_of(p), r2, deconv, st);
-      FPM_TRY(launch_ok());
-    }
-    for (auto& r : p->runs) {
-      const SimDev& S = p->sims[r.first];
-      const int n = run_active(r, it);
-      if (n == 0 || (r.fused && stencil_path(p))) continue;
-      FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->dk + S.s_off,
-                       p->lrho + S.m_off, st));
-    }
+    prof_mark(p, 9, st);
+    FPM_TRY(adjoint_step(p, a, it, st));
+    prof_mark(p, 9, st);
   }
   a.it = -1;
   launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);

@@ -159,9 +159,16 @@ int fpm_plan_status(fpm_plan* plan, int32_t* status, void* stream);
  * Fourier solve -- density to the three force meshes, all of its
  * transforms and kernels (kind 1) -- and the initial paint (kind 2) on the
  * call's stream; for meshes on the cuFFT path also around the
- * Green's-function kernel (kind 3) and the stencil gradient (kind 4).  fpm_plan_profile_read waits for the last event, returns the
- * summed device time and the number of timed launches of `kind`, and
- * resets that kind.  Not for use under CUDA graph capture. */
+ * Green's-function kernel (kind 3) and the stencil gradient (kind 4).
+ * fpm_nbody_adjoint records, per position of the reverse sweep, the
+ * reverse drift + paint kernel (kind 5), the force VJP kernel (kind 6),
+ * the divergence stencil (kind 7, stencil path), the adjoint potential
+ * solve -- adjoint force meshes to the adjoint density, all of its
+ * transforms and kernels (kind 8) -- and the whole position (kind 9); its
+ * force solves add to kinds 1, 3 and 4.  fpm_plan_profile_read waits for
+ * the last event, returns the summed device time and the number of timed
+ * launches of `kind`, and resets that kind.  Not for use under CUDA graph
+ * capture. */
 int fpm_plan_profile(fpm_plan* plan, int enable);
 int fpm_plan_profile_read(fpm_plan* plan, int kind, double* total_ms,
                           int64_t* launches);
