@@ -58,6 +58,10 @@ def parse():
   ap.add_argument('--no-cpu-baseline', action='store_true')
   ap.add_argument('--c5', action='store_true',
                   help='also measure the 2 x 512^3 forward + adjoint config')
+  ap.add_argument('--c5-mesh', type=int, default=512,
+                  help='mesh per side of the --c5 measurement, box scaled '
+                  'to keep its spacing; for profiling other sizes (C5 is '
+                  '512)')
   ap.add_argument('--no-extras', action='store_true',
                   help='skip the C4 (forward + adjoint) and C3 (batched) '
                   'measurements')
@@ -473,7 +477,7 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
   of the paint, step (readout + kick + drift + paint) and Fourier kernels."""
   from flowpm_b200 import _lib, tfbackground
   from flowpm_b200._plans import Plan, clear_plans
-  box = 1000.0
+  box = 1000.0 * n / 512
   cosmos = [fpm.cosmology.Planck15(),
             fpm.cosmology.Planck15(Omega_c=0.27, sigma8=0.78)]
   seeds = [5120, 5121]
@@ -626,9 +630,10 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
   plan.close()
   upd = 2.0 * np_ * steps
   return {
-      'workload': 'C5: 2 x 512^3, box 1000 Mpc/h, 30 KDK steps, forward + '
+      'workload': ('C5: ' if n == 512 else '') +
+                  '2 x %d^3, box %g Mpc/h, %d KDK steps, forward + '
                   'reverse-time adjoint, checkpoint every %d, different '
-                  'seeds and cosmologies' % ckpt,
+                  'seeds and cosmologies' % (n, box, steps, ckpt),
       'forward_value': upd / (t_fwd * 1e-3),
       'value': upd / (t_all * 1e-3),
       'unit': 'particle-updates/s (forward + adjoint)',
@@ -866,7 +871,7 @@ def main():
     line['fwd_adjoint'] = measure_fwd_adjoint(fpm, flush, max(args.steps, 3))
     line['batched'] = measure_batched(fpm, flush, max(args.steps, 3))
   if world == 1 and args.c5:
-    line['large'] = measure_large(fpm, flush)
+    line['large'] = measure_large(fpm, flush, n=args.c5_mesh)
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     line['cpu_baseline'] = cpu_baseline()
   _lib.lib.fpm_graph_destroy(graph)

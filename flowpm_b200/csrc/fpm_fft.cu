@@ -33,6 +33,7 @@ constexpr int kFftThreads = 256;
 
 __constant__ float2 c_w128[128];  // exp(-2 pi i m / 128), m = 0..127
 __device__ float2 g_w128[128];    // the same, for lane-dependent indices
+__device__ float2 g_w512[512];    // exp(-2 pi i m / 512), m = 0..511
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -437,6 +438,98 @@ k_fft_columns(const SimDev* __restrict__ sims, int first, int nblk,
   }
 }
 
+// x pass of the Fourier solve of meshes with 256 or 512 cells along x,
+// between batched two-dimensional (y, z) transforms of cuFFT (the
+// spectrum in cuFFT's R2C layout (x, y, z/2 + 1), unnormalised):
+// out = inverse-DFT_x(pre * w(k) * DFT_x(in)) for the kC = 8 consecutive
+// (ky, kz) columns of one simulation held by the block (the potential of
+// k_fourier_potential, the same arithmetic per mode).  The x DFT of
+// length NX = R * 64 runs on the stride-R sub-lines x = R b + a as 64-point
+// DFTs (cols_dft), a twiddle W_NX^(a kb) and R-point DFTs in registers,
+// where the transfer function is applied and the inverse starts; the
+// column block moves through shared memory as 64-byte rows.  With
+// rho_zero, the block also zeroes its share of the sim's density mesh.
+constexpr int kXThreads = 512, kXCols = 8;
+
+template <int NX>
+__global__ void __launch_bounds__(kXThreads)
+k_fft_xcols(const SimDev* __restrict__ sims, int first, int nblk,
+            const float2* in, float2* out, float* __restrict__ rho_zero,
+            AxisTabs tabs, Green G, const int32_t* __restrict__ nsteps,
+            int pos) {
+  constexpr int R = NX / 64, C = kXCols, T = kXThreads;
+  static_assert(64 * C == T, "one (kb, column) pair per thread");
+  __shared__ __align__(16) float2 buf[NX * C];  // x of column c at x C + c
+  const int s = first + blockIdx.x / nblk;
+  if (nsteps && pos > nsteps[s]) return;  // finished simulation
+  const int blk = blockIdx.x % nblk;
+  const SimDev& S = sims[s];
+  const int ncols = S.my * S.mzh;
+  const int c0 = blk * C;
+  const float4* src = reinterpret_cast<const float4*>(in + S.s_off + c0);
+  float4* dst = reinterpret_cast<float4*>(out + S.s_off + c0);
+  const int64_t rstride = ncols / 2;  // float4 per x plane
+  float4* b4 = reinterpret_cast<float4*>(buf);
+#pragma unroll
+  for (int i = 0; i < NX * C / 2 / T; ++i) {
+    const int e = threadIdx.x + i * T;
+    b4[e] = src[(int64_t)(e / (C / 2)) * rstride + e % (C / 2)];
+  }
+  if (rho_zero) {  // this block's share of the density, in float4
+    const int64_t q4 = (int64_t)S.mx * S.my * S.mz / 4;
+    const int64_t per = (q4 + nblk - 1) / nblk;
+    float4* r4 = reinterpret_cast<float4*>(rho_zero + S.m_off);
+    const int64_t e1 = min(q4, (blk + 1) * per);
+    for (int64_t e = blk * per + threadIdx.x; e < e1; e += T)
+      r4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  cols_dft<64, false, T, R * C, R * C>(buf);  // ends with a barrier
+  const int kb = threadIdx.x / C, c = threadIdx.x % C;
+  float2 v[R];
+#pragma unroll
+  for (int a = 0; a < R; ++a) {
+    v[a] = buf[(R * kb + a) * C + c];
+    if (a != 0 && kb != 0)
+      v[a] = cmul(v[a], g_w512[(a * kb * (512 / NX)) & 511]);
+  }
+  dft<R, false>(v);  // v[ka] = X[kb + 64 ka]
+  const int j = c0 + c;
+  const int ky = j / S.mzh, kz = j - ky * S.mzh;
+  const float pre = (float)((double)S.bf * S.bf * S.bf /
+                            ((double)S.mx * S.my * S.mz));
+  const double* kkx = tabs.kk + S.tab;
+  const double* kky = kkx + S.mx;
+  const double* kkz = kky + S.my;
+  const float* wx = tabs.win + S.tab;
+  const float* wy = wx + S.mx;
+  const float* wz = wy + S.my;
+#pragma unroll
+  for (int ka = 0; ka < R; ++ka) {
+    const int kx = kb + 64 * ka;
+    const float w = green_w(G, s, kkx[kx] + kky[ky] + kkz[kz], wx[kx],
+                            wy[ky], wz[kz]);
+    float2 d = v[ka];
+    d.x = __fmul_rn(d.x, pre);
+    d.y = __fmul_rn(d.y, pre);
+    v[ka] = make_float2(__fmul_rn(d.x, w), __fmul_rn(d.y, w));
+  }
+  dft<R, true>(v);  // v[a] = sum_ka X W_R^(-a ka)
+#pragma unroll
+  for (int a = 0; a < R; ++a) {
+    if (a != 0 && kb != 0)
+      v[a] = cmulc(v[a], g_w512[(a * kb * (512 / NX)) & 511]);
+    buf[(R * kb + a) * C + c] = v[a];  // the positions this thread read
+  }
+  __syncthreads();
+  cols_dft<64, true, T, R * C, R * C>(buf);
+#pragma unroll
+  for (int i = 0; i < NX * C / 2 / T; ++i) {
+    const int e = threadIdx.x + i * T;
+    dst[(int64_t)(e / (C / 2)) * rstride + e % (C / 2)] = b4[e];
+  }
+}
+
 // 4-point central difference with periodic wrap, the arithmetic of
 // k_stencil_grad: (8 (f[+1] - f[-1]) - (f[+2] - f[-2])) / 12.
 __device__ __forceinline__ float stencil4f(float m2, float m1, float p1,
@@ -760,6 +853,52 @@ void launch_fft_potential(const SimDev* sims, int first, int n, int nx,
     FPM_FFT_SIZES(FPM_NY_CASE)
 #undef FPM_NY_CASE
   }
+}
+
+bool fft_xpass_supported(int nx, int ny, int nz) {
+  return (nx == 256 || nx == 512) && ny % 8 == 0 && nz % 2 == 0;
+}
+
+int fft_xpass_prepare() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return FPM_ERR_CUDA;
+  }
+  static bool ready[64] = {};
+  std::lock_guard<std::mutex> lock(g_tw_mu);
+  if (ready[dev]) return FPM_OK;
+  float2 w[512];
+  for (int m = 0; m < 512; ++m) {
+    const double t = -2.0 * 3.14159265358979323846 * m / 512.0;
+    w[m] = make_float2((float)std::cos(t), (float)std::sin(t));
+  }
+  float2 w128[128];
+  for (int m = 0; m < 128; ++m) w128[m] = w[4 * m];
+  if (cudaMemcpyToSymbol(g_w512, w, sizeof(w)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_w128, w128, sizeof(w128)) != cudaSuccess ||
+      cudaMemcpyToSymbol(g_w128, w128, sizeof(w128)) != cudaSuccess) {
+    cudaGetLastError();
+    return FPM_ERR_CUDA;
+  }
+  ready[dev] = true;
+  return FPM_OK;
+}
+
+void launch_fft_xpass(const SimDev* sims, int first, int n, int nx, int ny,
+                      int nzh, const float2* in, float2* out, float* rho_zero,
+                      AxisTabs tabs, const Green& G, const int32_t* nsteps,
+                      int pos, cudaStream_t st) {
+  if (n <= 0) return;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const int nblk = ny * nzh / kXCols;
+  const unsigned grid = (unsigned)(n * nblk);
+  if (nx == 512)
+    k_fft_xcols<512><<<grid, kXThreads, 0, st>>>(
+        sims, first, nblk, in, out, rho_zero, tabs, G, nsteps, pos);
+  else
+    k_fft_xcols<256><<<grid, kXThreads, 0, st>>>(
+        sims, first, nblk, in, out, rho_zero, tabs, G, nsteps, pos);
 }
 
 }  // namespace fpm

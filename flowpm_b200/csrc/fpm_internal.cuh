@@ -38,7 +38,7 @@ struct SimDev {
   int64_t ch_ls;         // first lattice-spectrum chunk
   int64_t ch_b;          // first lattice-block chunk
   int nbi, nbj, nbk;     // lattice blocks per axis
-  int pad2_;
+  int xpass;             // cuFFT plane transforms + the x-pass kernel
 };
 
 // Per-axis Fourier tables.  For an axis of n cells and index i,

@@ -276,7 +276,7 @@ k_fourier_potential(const SimDev* __restrict__ sims, int nsims,
     const int s = find_sim(sims, nsims, ch, kSpec);
     if (nsteps && pos > nsteps[s]) continue;  // finished simulation
     const SimDev S = sims[s];
-    if (skip_fused && S.fused) continue;
+    if (skip_fused && (S.fused || S.xpass)) continue;
     const int64_t nmodes = (int64_t)S.mx * S.my * S.mzh;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
     const float pre = (float)((double)S.bf * S.bf * S.bf / (double)mcells);

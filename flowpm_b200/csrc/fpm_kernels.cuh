@@ -97,6 +97,18 @@ void launch_fft_potential(const SimDev* sims, int first, int n, int nx,
                           int ny, int nz, const float* in, float2* dk,
                           float* out, AxisTabs tabs, const Green& G,
                           cudaStream_t st);
+// Meshes of 256 or 512 cells along x on the cuFFT path: the x pass between
+// batched (y, z) plane transforms, potential spectrum out = x-pass(in) of
+// the sims [first, first + n) of one run (in == out allowed; with nsteps,
+// the sims with nsteps < pos skip); with rho_zero it also zeroes their
+// density meshes.  fft_xpass_prepare uploads its twiddles (once per
+// device).
+bool fft_xpass_supported(int nx, int ny, int nz);
+int fft_xpass_prepare();
+void launch_fft_xpass(const SimDev* sims, int first, int n, int nx, int ny,
+                      int nzh, const float2* in, float2* out, float* rho_zero,
+                      AxisTabs tabs, const Green& G, const int32_t* nsteps,
+                      int pos, cudaStream_t st);
 
 // Fused readout + kick(end) + kick(start) + drift + paint of one iteration.
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,

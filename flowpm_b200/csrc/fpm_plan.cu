@@ -33,6 +33,8 @@ constexpr int kProfKinds = 10;
 struct Run {
   int first, count;        // simulations [first, first + count)
   bool fused = false;      // force meshes by the fused Fourier solve
+  bool xpass = false;      // r2c / c2r1 are batched (y, z) plane transforms
+                           // around the x-pass kernel
   int div_xc = 0;          // x chunk of the tiled divergence stencil
   // Simulations of the run still active at leapfrog position it (a prefix
   // when the run is ordered by non-increasing step count), and the batched
@@ -258,6 +260,31 @@ int run_active(const Run& r, int it) {
   return r.active[it];
 }
 
+// Batched two-dimensional (y, z) transforms of `planes` consecutive x
+// planes, in cuFFT's default layout: the spectrum of plane x at
+// x * ny * (nz/2 + 1), the layout of the three-dimensional R2C.
+int make_plane_plan(cufftHandle* h, int ny, int nz, cufftType type,
+                    int planes, size_t* ws) {
+  if (cufftCreate(h) != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  if (cufftSetAutoAllocation(*h, 0) != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  long long n[2] = {ny, nz};
+  size_t w = 0;
+  cufftResult r = cufftMakePlanMany64(*h, 2, n, nullptr, 1, 0, nullptr, 1, 0,
+                                      type, planes, &w);
+  if (r == CUFFT_ALLOC_FAILED) return FPM_ERR_OOM;
+  if (r != CUFFT_SUCCESS) return FPM_ERR_CUFFT;
+  if (w > *ws) *ws = w;
+  return FPM_OK;
+}
+
+// The force-mesh R2C (or C2R) of n sims of run r: three-dimensional, or
+// the plane transforms of the x-pass path.
+int make_mesh_plan(cufftHandle* h, const Run& r, const SimDev& S,
+                   cufftType type, int n, size_t* ws) {
+  if (r.xpass) return make_plane_plan(h, S.my, S.mz, type, S.mx * n, ws);
+  return make_plan(h, S.mx, S.my, S.mz, type, n, ws);
+}
+
 // Plan for `n` of the run's simulations: the full-run plan or the one of
 // the smaller active prefix.
 cufftHandle pick(const Run& r, int n, cufftHandle full,
@@ -272,6 +299,30 @@ cufftHandle pick(const Run& r, int n, cufftHandle full,
 // no finite stencil and keeps three spectra and a batched C2R.
 bool stencil_path(const fpm_plan* p) {
   return (p->flags & FPM_PLAN_GRAD_ORDER0) == 0;
+}
+
+// The potential spectrum out = pre w(k) in of the sims on the cuFFT path
+// (k_fourier_potential), or, for runs on the x-pass path, the x pass that
+// wraps it (both skip the sims with nsteps < pos when act is given); with
+// rho_zero, their density meshes are zeroed.
+void potential_modes(fpm_plan* p, const float2* in, float2* out,
+                     float* rho_zero, const Green& G, const int32_t* act,
+                     int pos, cudaStream_t st) {
+  bool other = false;
+  for (auto& r : p->runs) {
+    if (r.fused) continue;
+    if (!r.xpass) {
+      other = true;
+      continue;
+    }
+    const int n = run_active(r, pos);
+    const SimDev& S = p->sims[r.first];
+    launch_fft_xpass(p->d_sims, r.first, n, S.mx, S.my, S.mzh, in, out,
+                     rho_zero, tabs_of(p), G, act, pos, st);
+  }
+  if (other)
+    launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, in, out, rho_zero,
+                             tabs_of(p), G, act, pos, 1, st);
 }
 
 // Density of the current positions -> force meshes (paint must be done).
@@ -313,9 +364,8 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
   }
   prof_mark(p, 3, st);
   if (stencil_path(p)) {
-    launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
-                             zero_rho ? p->rho : nullptr, tabs_of(p), G, act,
-                             it, 1, st);
+    potential_modes(p, p->dk, p->fk, zero_rho ? p->rho : nullptr, G, act, it,
+                    st);
   } else {
     launch_fourier_force(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk,
                          zero_rho ? p->rho : nullptr, tabs_of(p), r2, deconv,
@@ -380,8 +430,7 @@ int pgd_meshes(fpm_plan* p, cudaStream_t st, int pos) {
     FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->rho + S.m_off,
                      p->dk + S.s_off, st));
   }
-  launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->fk, p->rho,
-                           tabs_of(p), G, act, apos, 1, st);
+  potential_modes(p, p->dk, p->fk, p->rho, G, act, apos, st);
   FPM_TRY(launch_ok());
   for (auto& r : p->runs) {
     if (r.fused) continue;
@@ -420,13 +469,12 @@ int update_schedule(fpm_plan* p, int max_steps, const int32_t* nsteps,
       if (n == 0 || n == r.count || r.r2c_n.count(n)) continue;
       size_t ws = 0;
       cufftHandle a = 0, b = 0, c = 0, d = 0;
-      int rc = make_plan(&a, S.mx, S.my, S.mz, CUFFT_R2C, n, &ws);
+      int rc = make_mesh_plan(&a, r, S, CUFFT_R2C, n, &ws);
       if (rc == FPM_OK)
         rc = make_plan(&b, S.mx, S.my, S.mz, CUFFT_C2R, 3 * n, &ws);
       if (adj && rc == FPM_OK)
         rc = make_plan(&c, S.mx, S.my, S.mz, CUFFT_R2C, 3 * n, &ws);
-      if (rc == FPM_OK)
-        rc = make_plan(&d, S.mx, S.my, S.mz, CUFFT_C2R, n, &ws);
+      if (rc == FPM_OK) rc = make_mesh_plan(&d, r, S, CUFFT_C2R, n, &ws);
       if (rc == FPM_OK && ws > p->work_bytes) rc = FPM_ERR_UNSUPPORTED;
       for (cufftHandle h : {a, b, c, d})
         if (rc == FPM_OK && h && cufftSetWorkArea(h, p->work) != CUFFT_SUCCESS)
@@ -596,13 +644,27 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
     }
   }
   for (auto& r : p->runs) {
+    if (r.fused || (flags & FPM_PLAN_CUFFT) || (flags & FPM_PLAN_GRAD_ORDER0))
+      continue;
+    const SimDev& S0 = p->sims[r.first];
+    bool aligned = true;  // float4 spectrum rows and density zeroing
+    for (int s = r.first; s < r.first + r.count; ++s)
+      if (p->sims[s].s_off % 2 != 0 || p->sims[s].m_off % 4 != 0)
+        aligned = false;
+    if (aligned && fft_xpass_supported(S0.mx, S0.my, S0.mz) &&
+        fft_xpass_prepare() == FPM_OK) {
+      r.xpass = true;
+      for (int s = r.first; s < r.first + r.count; ++s) p->sims[s].xpass = 1;
+    }
+  }
+  for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
     if (rc == FPM_OK)
-      rc = make_plan(&r.r2c, S.mx, S.my, S.mz, CUFFT_R2C, r.count, &ws);
+      rc = make_mesh_plan(&r.r2c, r, S, CUFFT_R2C, r.count, &ws);
     if (rc == FPM_OK)
       rc = make_plan(&r.c2r3, S.mx, S.my, S.mz, CUFFT_C2R, 3 * r.count, &ws);
     if (rc == FPM_OK)
-      rc = make_plan(&r.c2r1, S.mx, S.my, S.mz, CUFFT_C2R, r.count, &ws);
+      rc = make_mesh_plan(&r.c2r1, r, S, CUFFT_C2R, r.count, &ws);
     if (adj && rc == FPM_OK)
       rc = make_plan(&r.r2c3, S.mx, S.my, S.mz, CUFFT_R2C, 3 * r.count, &ws);
     if (lpt) {
@@ -964,9 +1026,7 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
     }
     FPM_TRY(launch_ok());
     if (any_cufft) {
-      launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, p->dk, p->dk,
-                               nullptr, tabs_of(p), plan_green(p), act, it, 1,
-                               st);
+      potential_modes(p, p->dk, p->dk, nullptr, plan_green(p), act, it, st);
       FPM_TRY(launch_ok());
     }
   } else {

@@ -1,9 +1,11 @@
 """The fused Fourier solve (power-of-two meshes of 16 to 128 cells per axis)
-against the cuFFT path of the same library (plan flag FPM_PLAN_CUFFT):
-forces of random particle sets through fpm_force, for single and batched
-plans whose runs mix both paths.  (The oracle comparisons of the force, the
-leapfrog and the density go through the fused solve wherever the mesh
-qualifies, e.g. every 16^3 / 32^3 golden case.)"""
+and the x-pass solve (256 or 512 cells along x: batched cuFFT plane
+transforms around the x-pass kernel) against the three-dimensional cuFFT
+path of the same library (plan flag FPM_PLAN_CUFFT): forces of random
+particle sets through fpm_force, for single and batched plans whose runs
+mix the paths.  (The oracle comparisons of the force, the leapfrog and the
+density go through the fused solve wherever the mesh qualifies, e.g. every
+16^3 / 32^3 golden case.)"""
 import numpy as np
 import pytest
 import torch
@@ -30,6 +32,12 @@ SHAPES = [
     [(128, 128, 128, 1)],
     # runs: fused 32^3 x2, cuFFT 24^3, fused 16x32x64 on a 2x finer mesh
     [(32, 32, 32, 1), (32, 32, 32, 1), (24, 24, 24, 1), (16, 32, 64, 2)],
+    # x pass: 256^3; 512 along x; fused, x pass x2 (one on a 2x finer
+    # mesh) and cuFFT runs in one plan
+    [(256, 256, 256, 1)],
+    [(512, 16, 16, 1)],
+    [(32, 32, 32, 1), (256, 16, 32, 1), (256, 16, 32, 1), (24, 24, 24, 1),
+     (128, 24, 8, 2)],
 ]
 
 
