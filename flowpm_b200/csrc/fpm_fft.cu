@@ -441,15 +441,22 @@ k_fft_columns(const SimDev* __restrict__ sims, int first, int nblk,
 // x pass of the Fourier solve of meshes with 256 or 512 cells along x,
 // between batched two-dimensional (y, z) transforms of cuFFT (the
 // spectrum in cuFFT's R2C layout (x, y, z/2 + 1), unnormalised):
-// out = inverse-DFT_x(pre * w(k) * DFT_x(in)) for the kC = 8 consecutive
+// out = inverse-DFT_x(pre * w(k) * DFT_x(in)) for the kXCols consecutive
 // (ky, kz) columns of one simulation held by the block (the potential of
 // k_fourier_potential, the same arithmetic per mode).  The x DFT of
 // length NX = R * 64 runs on the stride-R sub-lines x = R b + a as 64-point
 // DFTs (cols_dft), a twiddle W_NX^(a kb) and R-point DFTs in registers,
 // where the transfer function is applied and the inverse starts; the
-// column block moves through shared memory as 64-byte rows.  With
+// column block moves through shared memory as rows of kXCols modes.  With
 // rho_zero, the block also zeroes its share of the sim's density mesh.
-constexpr int kXThreads = 512, kXCols = 8;
+// Columns per x-pass block.  Measured on B200 at 2 x 512^3: 8 columns
+// (64-byte rows, 32 KB) 1.19 ms per pass, 16 (128-byte rows, 64 KB) 1.01
+// ms; a persistent variant with cp.async double buffering of 8-column
+// blocks took 1.53 ms.
+#ifndef FPM_XPASS_COLS
+#define FPM_XPASS_COLS 16
+#endif
+constexpr int kXThreads = 512, kXCols = FPM_XPASS_COLS;
 
 template <int NX>
 __global__ void __launch_bounds__(kXThreads)
@@ -458,8 +465,10 @@ k_fft_xcols(const SimDev* __restrict__ sims, int first, int nblk,
             AxisTabs tabs, Green G, const int32_t* __restrict__ nsteps,
             int pos) {
   constexpr int R = NX / 64, C = kXCols, T = kXThreads;
-  static_assert(64 * C == T, "one (kb, column) pair per thread");
-  __shared__ __align__(16) float2 buf[NX * C];  // x of column c at x C + c
+  constexpr int NP = 64 * C / T;                  // (kb, column) pairs
+  constexpr int NS = R * C, NS1 = NS < 64 ? NS : 64;  // sub-lines per pass
+  static_assert(64 * C % T == 0 && NS % NS1 == 0, "block shape");
+  extern __shared__ __align__(16) float2 buf[];   // x of column c at x C + c
   const int s = first + blockIdx.x / nblk;
   if (nsteps && pos > nsteps[s]) return;  // finished simulation
   const int blk = blockIdx.x % nblk;
@@ -484,8 +493,14 @@ k_fft_xcols(const SimDev* __restrict__ sims, int first, int nblk,
       r4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
-  cols_dft<64, false, T, R * C, R * C>(buf);  // ends with a barrier
-  const int kb = threadIdx.x / C, c = threadIdx.x % C;
+#pragma unroll
+  for (int h = 0; h < NS / NS1; ++h)  // each ends with a barrier
+    cols_dft<64, false, T, NS1, NS>(buf + h * NS1);
+  const float pre = (float)((double)S.bf * S.bf * S.bf /
+                            ((double)S.mx * S.my * S.mz));
+#pragma unroll 1
+  for (int pr = 0; pr < NP; ++pr) {
+  const int kb = (threadIdx.x + pr * T) / C, c = threadIdx.x % C;
   float2 v[R];
 #pragma unroll
   for (int a = 0; a < R; ++a) {
@@ -496,19 +511,17 @@ k_fft_xcols(const SimDev* __restrict__ sims, int first, int nblk,
   dft<R, false>(v);  // v[ka] = X[kb + 64 ka]
   const int j = c0 + c;
   const int ky = j / S.mzh, kz = j - ky * S.mzh;
-  const float pre = (float)((double)S.bf * S.bf * S.bf /
-                            ((double)S.mx * S.my * S.mz));
   const double* kkx = tabs.kk + S.tab;
-  const double* kky = kkx + S.mx;
-  const double* kkz = kky + S.my;
+  const double kyv = kkx[S.mx + ky], kzv = kkx[S.mx + S.my + kz];
   const float* wx = tabs.win + S.tab;
-  const float* wy = wx + S.mx;
-  const float* wz = wy + S.my;
+  // the CIC windows only enter with deconvolution
+  const float wyv = G.deconv ? wx[S.mx + ky] : 1.f;
+  const float wzv = G.deconv ? wx[S.mx + S.my + kz] : 1.f;
 #pragma unroll
   for (int ka = 0; ka < R; ++ka) {
     const int kx = kb + 64 * ka;
-    const float w = green_w(G, s, kkx[kx] + kky[ky] + kkz[kz], wx[kx],
-                            wy[ky], wz[kz]);
+    const float w = green_w(G, s, (kkx[kx] + kyv) + kzv,
+                            G.deconv ? wx[kx] : 1.f, wyv, wzv);
     float2 d = v[ka];
     d.x = __fmul_rn(d.x, pre);
     d.y = __fmul_rn(d.y, pre);
@@ -521,8 +534,11 @@ k_fft_xcols(const SimDev* __restrict__ sims, int first, int nblk,
       v[a] = cmulc(v[a], g_w512[(a * kb * (512 / NX)) & 511]);
     buf[(R * kb + a) * C + c] = v[a];  // the positions this thread read
   }
+  }
   __syncthreads();
-  cols_dft<64, true, T, R * C, R * C>(buf);
+#pragma unroll
+  for (int h = 0; h < NS / NS1; ++h)
+    cols_dft<64, true, T, NS1, NS>(buf + h * NS1);
 #pragma unroll
   for (int i = 0; i < NX * C / 2 / T; ++i) {
     const int e = threadIdx.x + i * T;
@@ -855,8 +871,10 @@ void launch_fft_potential(const SimDev* sims, int first, int n, int nx,
   }
 }
 
+size_t xpass_smem(int nx) { return (size_t)nx * kXCols * sizeof(float2); }
+
 bool fft_xpass_supported(int nx, int ny, int nz) {
-  return (nx == 256 || nx == 512) && ny % 8 == 0 && nz % 2 == 0;
+  return (nx == 256 || nx == 512) && ny % kXCols == 0 && nz % 2 == 0;
 }
 
 int fft_xpass_prepare() {
@@ -877,7 +895,13 @@ int fft_xpass_prepare() {
   for (int m = 0; m < 128; ++m) w128[m] = w[4 * m];
   if (cudaMemcpyToSymbol(g_w512, w, sizeof(w)) != cudaSuccess ||
       cudaMemcpyToSymbol(c_w128, w128, sizeof(w128)) != cudaSuccess ||
-      cudaMemcpyToSymbol(g_w128, w128, sizeof(w128)) != cudaSuccess) {
+      cudaMemcpyToSymbol(g_w128, w128, sizeof(w128)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_fft_xcols<512>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)xpass_smem(512)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_fft_xcols<256>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)xpass_smem(256)) != cudaSuccess) {
     cudaGetLastError();
     return FPM_ERR_CUDA;
   }
@@ -894,10 +918,10 @@ void launch_fft_xpass(const SimDev* sims, int first, int n, int nx, int ny,
   const int nblk = ny * nzh / kXCols;
   const unsigned grid = (unsigned)(n * nblk);
   if (nx == 512)
-    k_fft_xcols<512><<<grid, kXThreads, 0, st>>>(
+    k_fft_xcols<512><<<grid, kXThreads, xpass_smem(512), st>>>(
         sims, first, nblk, in, out, rho_zero, tabs, G, nsteps, pos);
   else
-    k_fft_xcols<256><<<grid, kXThreads, 0, st>>>(
+    k_fft_xcols<256><<<grid, kXThreads, xpass_smem(256), st>>>(
         sims, first, nblk, in, out, rho_zero, tabs, G, nsteps, pos);
 }
 
