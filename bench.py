@@ -58,6 +58,10 @@ def parse():
   ap.add_argument('--no-cpu-baseline', action='store_true')
   ap.add_argument('--c5', action='store_true',
                   help='also measure the 2 x 512^3 forward + adjoint config')
+  ap.add_argument('--no-potential-tape', action='store_true',
+                  help='C4 / C5: rebuild the force meshes of the reverse '
+                  'sweep (paint + Fourier solve) instead of keeping the '
+                  "forward's potentials (fpm_nbody_set_tape)")
   ap.add_argument('--c5-mesh', type=int, default=512,
                   help='mesh per side of the --c5 measurement, box scaled '
                   'to keep its spacing; for profiling other sizes (C5 is '
@@ -263,7 +267,7 @@ def _timed(fn, reps, flush):
 
 
 def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5,
-                        fd_dirs=32):
+                        fd_dirs=32, tape=True):
   """Config C4: 128^3, 20 steps, chi^2 of the final CIC density against
   (that density + N(0, 1) noise); gradient with respect to the initial
   linear field.  Timed step = forward leapfrog (graph, checkpoints every
@@ -292,6 +296,12 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5,
   g = torch.empty_like(rho)
   nslot = steps // ckpt + 1
   ck = torch.empty((nslot, 2, np_, 3), device='cuda')
+  # the forward's potential at every position, for the reverse sweep
+  phi_tape = (torch.empty((steps + 1) * np_, device='cuda') if tape
+              else None)
+  if tape:
+    _lib.call('fpm_nbody_set_tape', plan.handle, _lib.ptr(phi_tape),
+              phi_tape.numel())
   gf, ga = _lib.ctypes.c_void_p(), _lib.ctypes.c_void_p()
   _lib.call('fpm_graph_capture_nbody', plan.handle, _lib.ptr(d), _lib.ptr(p),
             _lib.ptr(f), None, 0, _lib.ptr(ck), ckpt, _lib.ctypes.byref(gf))
@@ -363,6 +373,7 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5,
                           'max_rel': float(np.max(errs))}
   _lib.lib.fpm_graph_destroy(gf)
   _lib.lib.fpm_graph_destroy(ga)
+  _lib.call('fpm_nbody_set_tape', plan.handle, None, 0)
   upd = float(np_) * steps
   return {
       'workload': 'C4: 128^3, 20 KDK steps, chi^2(final CIC density, '
@@ -375,6 +386,7 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5,
       'adjoint_over_forward': (ms - ms_fwd) / ms_fwd,
       'grad_vs_fp32_central_differences': fd,
       'fd_directions': fd_dirs,
+      'potential_tape_gb': phi_tape.numel() * 4 / 1e9 if tape else 0.0,
   }
 
 
@@ -468,7 +480,7 @@ def measure_batched(fpm, flush, reps):
   }
 
 
-def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
+def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
   """Config C5: two 512^3 simulations (different seeds and cosmologies),
   box 1000 Mpc/h, 30 steps, forward + reverse-time adjoint with a
   checkpoint every 5 steps, in one plan.  Reports forward and
@@ -508,6 +520,12 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
   ck = torch.empty((steps // ckpt + 1, 2) + tuple(D0.shape), device='cuda')
   rho = torch.empty((2,) + tuple(nc), device='cuda')
   g = torch.empty_like(rho)
+  # the forward's potential at every position, for the reverse sweep
+  phi_tape = (torch.empty((steps + 1) * 2 * np_, device='cuda') if tape
+              else None)
+  if tape:
+    _lib.call('fpm_nbody_set_tape', plan.handle, _lib.ptr(phi_tape),
+              phi_tape.numel())
   gf, ga = _lib.ctypes.c_void_p(), _lib.ctypes.c_void_p()
   _lib.call('fpm_graph_capture_nbody', plan.handle, _lib.ptr(D), _lib.ptr(P),
             _lib.ptr(F), None, 0, _lib.ptr(ck), ckpt, _lib.ctypes.byref(gf))
@@ -595,12 +613,15 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
   # stencil reads the potential and writes the three force meshes.
   # Reverse sweep, per particle (Np = Nc): the drift + paint kernel reads
   # d, F and reads and writes lam_x, p, lam_p (12 B each way), writes d,
-  # gathers the adjoint density and paints (4 B per cell each), 116 B; the
-  # VJP reads d, lam_p, the three force meshes (12 B per cell), reads and
-  # writes lam_x and p, writes F and reduces into the adjoint force mesh
-  # (16 B per cell), 112 B; the divergence stencil reads that mesh and
-  # writes the adjoint potential, 20 B per cell; the adjoint potential solve
-  # reads it and writes the adjoint density, 8 B per cell.
+  # gathers the adjoint density and paints (4 B per cell each), 116 B (112 B
+  # with the potential tape, which drops the paint); the VJP reads d, lam_p,
+  # the three force meshes (12 B per cell), reads and writes lam_x and p,
+  # writes F and reduces into the adjoint force mesh (16 B per cell), 112 B;
+  # the divergence stencil reads the adjoint force mesh and writes the
+  # adjoint potential, 20 B per cell; the adjoint potential solve reads it
+  # and writes the adjoint density, 8 B per cell.  With the potential tape,
+  # the force meshes of a position are the stencil of the stored potential
+  # (20 B per cell, as the forward stencil).
   half = 2 * n * n * (n // 2 + 1)
   kbytes = {
       'step': KERNEL_BYTES_PER_PART * tot_np,
@@ -608,7 +629,8 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
       'fourier': 20 * nc_tot,
       'green': 16 * half + 4 * nc_tot,
       'stencil': 16 * nc_tot,
-      'adj_drift_paint': 116 * tot_np,
+      # with the potential tape the reverse drift does not paint
+      'adj_drift_paint': (112 if tape else 116) * tot_np,
       'adj_vjp': 112 * tot_np,
       'adj_div': 20 * nc_tot,
       'adj_potential': 8 * nc_tot,
@@ -626,7 +648,9 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
   _lib.lib.fpm_graph_destroy(gf)
   _lib.lib.fpm_graph_destroy(ga)
   dev_gb = (plan.device_bytes + 7 * D0.numel() * 4 + ck.numel() * 4 +
-            3 * rho.numel() * 4) / 1e9
+            3 * rho.numel() * 4 +
+            (phi_tape.numel() * 4 if tape else 0)) / 1e9
+  _lib.call('fpm_nbody_set_tape', plan.handle, None, 0)
   plan.close()
   upd = 2.0 * np_ * steps
   return {
@@ -645,6 +669,7 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5):
       'peak_kind': peak_kind,
       'status': status,
       'device_gb': dev_gb,
+      'potential_tape_gb': phi_tape.numel() * 4 / 1e9 if tape else 0.0,
       'pk_final_first_bins': [float(v) for v in pk[0, :8].cpu()],
   }
 
@@ -868,10 +893,12 @@ def main():
       'clocks': clk.summary(),
   }
   if world == 1 and not args.no_extras:
-    line['fwd_adjoint'] = measure_fwd_adjoint(fpm, flush, max(args.steps, 3))
+    line['fwd_adjoint'] = measure_fwd_adjoint(
+        fpm, flush, max(args.steps, 3), tape=not args.no_potential_tape)
     line['batched'] = measure_batched(fpm, flush, max(args.steps, 3))
   if world == 1 and args.c5:
-    line['large'] = measure_large(fpm, flush, n=args.c5_mesh)
+    line['large'] = measure_large(fpm, flush, n=args.c5_mesh,
+                                  tape=not args.no_potential_tape)
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     line['cpu_baseline'] = cpu_baseline()
   _lib.lib.fpm_graph_destroy(graph)

@@ -172,7 +172,8 @@ class NBody(torch.autograd.Function):
   """nbody with the reverse-time adjoint as its backward."""
 
   @staticmethod
-  def forward(ctx, state, cosmo, stages, nc, pm_nc_factor, checkpoint_every):
+  def forward(ctx, state, cosmo, stages, nc, pm_nc_factor, checkpoint_every,
+              store_potential=None):
     B = state.shape[1]
     T = len(stages) - 1
     dims = [tuple(nc) + (int(pm_nc_factor),)] * B
@@ -191,14 +192,23 @@ class NBody(torch.autograd.Function):
     if k > 0:
       ckpt = torch.empty((T // k + 1, 2) + tuple(p.shape), dtype=torch.float32,
                          device=p.device)
-    _lib.call('fpm_nbody_run', plan.handle, _lib.ptr(d), _lib.ptr(p),
-              _lib.ptr(f), None, 0, _lib.ptr(ckpt), k, st)
+    tape = _potential_tape(dims, T, store_potential, p.device)
+    if tape is not None:
+      _lib.call('fpm_nbody_set_tape', plan.handle, _lib.ptr(tape),
+                tape.numel())
+    try:
+      _lib.call('fpm_nbody_run', plan.handle, _lib.ptr(d), _lib.ptr(p),
+                _lib.ptr(f), None, 0, _lib.ptr(ckpt), k, st)
+    finally:
+      if tape is not None:  # the plan is shared: detach the buffer
+        _lib.call('fpm_nbody_set_tape', plan.handle, None, 0)
     out = torch.empty_like(x)
     _lattice_shift(d, nc, 1, out=out[0])
     out[1].copy_(p)
     out[2].copy_(f)
     ctx.save_for_backward(d, p, f)
     ctx.ckpt = ckpt
+    ctx.tape = tape
     ctx.args = (dims, T, coefs, ffac, k, list(nc))
     return out
 
@@ -216,11 +226,37 @@ class NBody(torch.autograd.Function):
     lp = g[1].clone()
     lf = g[2].contiguous()
     dd, pp = d.clone(), p.clone()
-    _lib.call('fpm_nbody_adjoint', plan.handle, _lib.ptr(dd), _lib.ptr(pp),
-              _lib.ptr(f), _lib.ptr(lx), _lib.ptr(lp), _lib.ptr(lf),
-              _lib.ptr(ctx.ckpt), k, st)
+    tape = ctx.tape
+    if tape is not None:
+      _lib.call('fpm_nbody_set_tape', plan.handle, _lib.ptr(tape),
+                tape.numel())
+    try:
+      _lib.call('fpm_nbody_adjoint', plan.handle, _lib.ptr(dd), _lib.ptr(pp),
+                _lib.ptr(f), _lib.ptr(lx), _lib.ptr(lp), _lib.ptr(lf),
+                _lib.ptr(ctx.ckpt), k, st)
+    finally:
+      if tape is not None:
+        _lib.call('fpm_nbody_set_tape', plan.handle, None, 0)
+    ctx.tape = None
     grad = torch.stack((lx, lp, torch.zeros_like(lx)))
-    return grad, None, None, None, None, None
+    return grad, None, None, None, None, None, None
+
+
+def _potential_tape(dims, T, store, device):
+  """The potential tape of a differentiable nbody call: (T + 1) x the
+  plan's force-mesh cells, or None.  store: True, False, or None for
+  automatic (when it takes under a quarter of the free device memory)."""
+  if store is False:
+    return None
+  cells = sum((b * nx) * (b * ny) * (b * nz) for nx, ny, nz, b in dims)
+  n = (T + 1) * cells
+  if store is None:
+    if cells % 4:  # the tape's positions must stay 16-byte aligned
+      return None
+    free, _ = torch.cuda.mem_get_info(device)
+    if 4 * n > free // 4:
+      return None
+  return torch.empty(n, dtype=torch.float32, device=device)
 
 
 def needs_grad(*tensors):

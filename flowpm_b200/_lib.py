@@ -54,6 +54,7 @@ SIGNATURES = {
     'fpm_nbody_adjoint': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p,
                                   c_void_p, c_void_p, c_void_p, c_void_p,
                                   c_int, c_void_p]),
+    'fpm_nbody_set_tape': (c_int, [c_void_p, c_void_p, c_int64]),
     'fpm_graph_capture_nbody': (c_int, [c_void_p, c_void_p, c_void_p,
                                         c_void_p, c_void_p, c_uint, c_void_p,
                                         c_int, ctypes.POINTER(c_void_p)]),
@@ -107,6 +108,8 @@ SIGNATURES = {
 
 # Constants of include/flowpm_b200.h.
 FPM_OK = 0
+FPM_ERR_ARG = 1
+FPM_ERR_UNSUPPORTED = 8
 FPM_ERR_NONFINITE = 6
 FPM_ERR_STATE = 7
 FPM_ERR_LIMIT = 9

@@ -20,6 +20,8 @@ struct AdjArgs {
                           // (lmesh + 3 m_off + d mcells)
   int lvec4;
   float* rho;             // density target of the paint
+  int paint;              // 0: the reverse drift skips the paint of x_it
+                          // (force meshes from a stored potential)
   const float* coefs;     // (nsims, max_steps, 3) {kick_start, drift, kick_end}
   const float* ffac;      // (nsims)
   const int32_t* nsteps;  // (nsims)

@@ -80,6 +80,9 @@ struct fpm_plan {
   float2* fk = nullptr;
   float* fmesh = nullptr;
   float* phi = nullptr;     // potential mesh (stencil force path)
+  float* tape = nullptr;    // caller's potential tape: position it at
+                            // tape + it * total_m (fpm_nbody_set_tape)
+  int64_t tape_floats = 0;
   bool quads = false;       // every mesh: mz % 4 == 0 and m_off % 4 == 0
   bool div_tiled = false;   // every run takes the tiled divergence stencil
   // lattice buffers (FPM_PLAN_LPT)
@@ -328,7 +331,9 @@ void potential_modes(fpm_plan* p, const float2* in, float2* out,
 // Density of the current positions -> force meshes (paint must be done).
 // At leapfrog position it (>= 0) only the active prefix of each run is
 // transformed.
-int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
+int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1,
+                 float* phi = nullptr) {
+  if (!phi) phi = p->phi;  // potential mesh of the stencil path
   const int32_t* act = it >= 0 ? p->d_nsteps : nullptr;
   const double r2 = p->r_split * p->r_split;
   const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
@@ -346,7 +351,7 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
     const int n = run_active(r, it);
     if (n == 0) continue;
     launch_fft_force(p->d_sims, r.first, n, S.mx, S.my, S.mz, p->rho,
-                     zero_rho ? 1 : 0, p->dk, p->fk, p->fmesh, p->phi,
+                     zero_rho ? 1 : 0, p->dk, p->fk, p->fmesh, phi,
                      tabs_of(p), G, !stencil_path(p), st);
   }
   FPM_TRY(launch_ok());
@@ -380,14 +385,14 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1) {
     if (n == 0) continue;
     if (stencil_path(p))
       FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->fk + S.s_off,
-                       p->phi + S.m_off, st));
+                       phi + S.m_off, st));
     else
       FPM_TRY(exec_c2r(pick(r, n, r.c2r3, r.c2r3_n), p->fk + 3 * S.s_off,
                        p->fmesh + 3 * S.m_off, st));
   }
   if (stencil_path(p)) {
     prof_mark(p, 4, st);
-    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, p->phi, p->fmesh, act,
+    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, phi, p->fmesh, act,
                         it, 1, p->quads, st);
     prof_mark(p, 4, st);
     FPM_TRY(launch_ok());
@@ -870,8 +875,12 @@ extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
                        p->d_status, st);
   prof_mark(p, 2, st);
   FPM_TRY(launch_ok());
+  if (p->tape && p->tape_floats < (int64_t)(p->max_steps + 1) * p->total_m)
+    return FPM_ERR_ARG;
   for (int it = 0; it <= p->max_steps; ++it) {
-    FPM_TRY(force_meshes(p, st, it < p->max_steps, it));
+    FPM_TRY(force_meshes(p, st, it < p->max_steps, it,
+                         p->tape ? p->tape + (size_t)it * p->total_m
+                                 : nullptr));
     a.it = it;
     prof_mark(p, 0, st);
     launch_step(p->d_sims, p->nsims, traverse_chunks(p), a, st);
@@ -977,12 +986,24 @@ extern "C" int fpm_nbody(fpm_plan* p, float* disp, float* mom, float* force,
 static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
   const double r2 = p->r_split * p->r_split;
   const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
-  FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
+  const bool tape = p->tape != nullptr;
+  if (!tape)
+    FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
+  a.paint = tape ? 0 : 1;
   prof_mark(p, 5, st);
   launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
   prof_mark(p, 5, st);
   FPM_TRY(launch_ok());
-  FPM_TRY(force_meshes(p, st, false, it));
+  if (tape) {  // the force meshes of the stored potential of position it
+    prof_mark(p, 1, st);
+    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m,
+                        p->tape + (size_t)it * p->total_m, p->fmesh,
+                        p->d_nsteps, it, 0, p->quads, st);
+    prof_mark(p, 1, st);
+    FPM_TRY(launch_ok());
+  } else {
+    FPM_TRY(force_meshes(p, st, false, it));
+  }
   FPM_CUDA(cudaMemsetAsync(p->lmesh, 0,
                            sizeof(float) * (a.lvec4 ? 4 : 3) * p->total_m,
                            st));
@@ -1063,6 +1084,8 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
     return FPM_ERR_ARG;
   if (!(p->flags & FPM_PLAN_ADJOINT) || !p->steps_set) return FPM_ERR_STATE;
   if (p->pgd_on) return FPM_ERR_UNSUPPORTED;  // no adjoint of the PGD step
+  if (p->tape && p->tape_floats < (int64_t)(p->max_steps + 1) * p->total_m)
+    return FPM_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   FPM_CUDA(cudaMemcpyAsync(p->fpart, force, sizeof(float) * 3 * p->total_np,
                            cudaMemcpyDeviceToDevice, st));
@@ -1077,6 +1100,7 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   a.lrho = p->lrho;
   a.lmesh = p->lmesh;
   a.lvec4 = stencil_path(p) ? 1 : 0;
+  a.paint = 1;
   a.rho = p->rho;
   a.coefs = p->d_coefs;
   a.ffac = p->d_ffac;
@@ -1095,6 +1119,16 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   a.it = -1;
   launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
   return launch_ok();
+}
+
+extern "C" int fpm_nbody_set_tape(fpm_plan* p, float* tape, int64_t floats) {
+  if (!p || (tape && floats < 0)) return FPM_ERR_ARG;
+  if (tape && (!stencil_path(p) || p->total_m % 4 != 0))
+    return FPM_ERR_UNSUPPORTED;
+  if (tape != p->tape) p->sched_gen++;  // captured graphs hold the pointer
+  p->tape = tape;
+  p->tape_floats = tape ? floats : 0;
+  return FPM_OK;
 }
 
 extern "C" int fpm_lpt_init(fpm_plan* p, const float* linear,

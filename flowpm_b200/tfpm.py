@@ -215,7 +215,7 @@ def drift(cosmo, state, ai, ac, af, name='Drift', **kwargs):
 
 def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
           return_intermediate_states=False, pgdparams=None, name='NBody',
-          check_finite=True, checkpoint_every=None):
+          check_finite=True, checkpoint_every=None, store_potential=None):
   """Integrate ``state`` across ``stages`` with the FastPM KDK leapfrog
   (flowpm/tfpm.py:425-503): one force at stages[0], then per step
   kick / drift / force / kick.  Returns the final state (3, B, Np, 3) or,
@@ -225,6 +225,11 @@ def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
   (fpm_nbody_adjoint), which rebuilds the trajectory from the final state;
   ``checkpoint_every = k`` stores (d, p) every k steps in the forward and
   resets the rebuilt trajectory there, bounding its FP32 drift.
+  ``store_potential`` keeps the potential of every force solve of the
+  forward ((steps + 1) x B x (pm_nc_factor nc)^3 floats, fpm_nbody_set_tape),
+  so the backward takes its force meshes from it instead of painting and
+  solving again; None (default) stores it when that takes less than a
+  quarter of the free device memory.
 
   With ``pgdparams`` (one row (alpha, kl, ks) per step) the PGD
   correction moves the particles after every drift (flowpm/tfpm.py:487-488,
@@ -250,7 +255,7 @@ def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
       raise NotImplementedError(
           'gradients through intermediate states are not supported')
     out = _autograd.NBody.apply(state, cosmo, stages, nc, pm_nc_factor,
-                                checkpoint_every)
+                                checkpoint_every, store_potential)
     if check_finite:
       plan = get_plan([tuple(nc) + (int(pm_nc_factor),)] * B,
                       flags=_lib.FPM_PLAN_ADJOINT)

@@ -244,6 +244,21 @@ int fpm_nbody_adjoint(fpm_plan* plan, float* disp, float* mom,
                       const float* lam_f, const float* ckpt, int ckpt_every,
                       void* stream);
 
+/* Potential tape (4-point gradient plans; FPM_ERR_UNSUPPORTED for order-0
+ * plans): while tape is set, fpm_nbody_run stores the potential of the
+ * force solve at every position it (0 .. max_steps) at
+ * tape + it * total_mesh_cells, and fpm_nbody_adjoint takes the force
+ * meshes of each position from the stencil of that potential instead of
+ * painting the rebuilt positions and solving again; the forward values
+ * replace the rebuilt ones, which removes the reconstruction drift from
+ * the forces.  total_mesh_cells is the sum over the simulations of
+ * (pm_nc_factor)^3 nx ny nz; floats must be at least (max_steps + 1) times
+ * it (checked by both calls: FPM_ERR_ARG).  The adjoint must follow a
+ * forward run with the same tape and steps.  NULL detaches; setting or
+ * detaching a tape invalidates captured graphs (FPM_ERR_STATE).  This has
+ * no counterpart in the reference, whose tape stores every TF op. */
+int fpm_nbody_set_tape(fpm_plan* plan, float* tape, int64_t floats);
+
 /* 2LPT initial conditions, flowpm/tfpm.py:148-180 lpt_init: from the real
  * linear field (the plan's lattice meshes concatenated) compute the 1LPT
  * and 2LPT displacements at the lattice points and

@@ -82,13 +82,14 @@ def test_lpt_adjoint(fpm, order):
   assert rel_l2(host(g), go.numpy()) < 1e-4
 
 
-def _chi2_ours(fpm, lin, target, stages, nc, pm_nc_factor=1, ckpt=None):
+def _chi2_ours(fpm, lin, target, stages, nc, pm_nc_factor=1, ckpt=None,
+               store=None):
   c = fpm.cosmology.Planck15()
   x = torch.tensor(lin, dtype=torch.float32, device='cuda',
                    requires_grad=True)
   s0 = fpm.lpt_init(c, x, stages[0], order=2)
   st = fpm.nbody(c, s0, stages, nc, pm_nc_factor=pm_nc_factor,
-                 checkpoint_every=ckpt)
+                 checkpoint_every=ckpt, store_potential=store)
   rho = fpm.cic_paint(torch.zeros((1,) + tuple(nc), device='cuda'), st[0])
   loss = ((rho - torch.tensor(target, dtype=torch.float32,
                               device='cuda'))**2).sum()
@@ -110,9 +111,13 @@ def _chi2_oracle(lin, target, stages, nc, pm_nc_factor=1, grad=True):
   return float(loss), g.numpy()
 
 
+@pytest.mark.parametrize('store', [False, True], ids=['rebuilt', 'potential'])
 @pytest.mark.parametrize('pm_nc_factor,ckpt', [(1, None), (2, None), (1, 2)])
-def test_nbody_adjoint_vs_tape(fpm, capsys, pm_nc_factor, ckpt):
-  """d chi^2 / d linear field through lpt_init -> nbody -> cic_paint."""
+def test_nbody_adjoint_vs_tape(fpm, capsys, pm_nc_factor, ckpt, store):
+  """d chi^2 / d linear field through lpt_init -> nbody -> cic_paint, with
+  the force meshes of the reverse sweep rebuilt (paint + Fourier solve at
+  the reconstructed positions) or taken from the stored potential of the
+  forward (fpm_nbody_set_tape)."""
   rng = np.random.default_rng(21)
   nc = [16, 16, 16]
   lin = rng.standard_normal([1] + nc) * 0.6
@@ -120,11 +125,12 @@ def test_nbody_adjoint_vs_tape(fpm, capsys, pm_nc_factor, ckpt):
   rho0 = _rho_oracle(lin, stages, nc, pm_nc_factor)
   target = rho0 + rng.standard_normal(rho0.shape)
   lo, go = _chi2_oracle(lin, target, stages, nc, pm_nc_factor)
-  l, g = _chi2_ours(fpm, lin, target, stages, nc, pm_nc_factor, ckpt)
+  l, g = _chi2_ours(fpm, lin, target, stages, nc, pm_nc_factor, ckpt, store)
   err = rel_l2(g, go)
   with capsys.disabled():
-    print('\n  adjoint vs FP64 tape gradient (B=%d, ckpt=%s): rel-L2 %.2e, '
-          'loss %.6g vs %.6g' % (pm_nc_factor, ckpt, err, l, lo))
+    print('\n  adjoint vs FP64 tape gradient (B=%d, ckpt=%s, stored '
+          'potential %s): rel-L2 %.2e, loss %.6g vs %.6g' %
+          (pm_nc_factor, ckpt, store, err, l, lo))
   assert err < 1e-3
 
 
@@ -194,3 +200,38 @@ def test_batched_adjoint_matches_single(fpm, capsys):
     print('\n  batched vs single adjoint at 128^3: rel l2 %s' %
           ', '.join('%.2e' % e for e in errs))
   assert max(errs) < 1e-5
+
+
+def test_potential_tape_arguments(fpm):
+  """fpm_nbody_set_tape: order-0 plans have no potential; a tape shorter
+  than (steps + 1) positions is refused by the forward and the adjoint."""
+  from flowpm_b200 import _lib
+  from flowpm_b200._plans import Plan
+  p0 = Plan([(16, 16, 16, 1)],
+            flags=_lib.FPM_PLAN_ADJOINT | _lib.FPM_PLAN_GRAD_ORDER0)
+  buf = torch.empty(16**3 * 3, device='cuda')  # 3 of the 4 positions
+  try:
+    assert _lib.lib.fpm_nbody_set_tape(p0.handle, _lib.ptr(buf),
+                                     buf.numel()) == _lib.FPM_ERR_UNSUPPORTED
+  finally:
+    p0.close()
+  plan = Plan([(16, 16, 16, 1)], flags=_lib.FPM_PLAN_ADJOINT)
+  try:
+    st = _lib.stream_ptr()
+    T = 3
+    coefs = np.full((1, T, 3), 0.01)
+    _lib.call('fpm_nbody_set_steps', plan.handle, T, _lib.ivec([T]),
+              _lib.dvec(coefs.ravel()), _lib.dvec([0.45]), st)
+    d = torch.zeros((16**3, 3), device='cuda')
+    p, f = torch.zeros_like(d), torch.zeros_like(d)
+    assert _lib.lib.fpm_nbody_set_tape(plan.handle, _lib.ptr(buf),
+                                       buf.numel()) == _lib.FPM_OK
+    assert _lib.lib.fpm_nbody_run(plan.handle, _lib.ptr(d), _lib.ptr(p),
+                                  _lib.ptr(f), None, 0, None, 0,
+                                  st) == _lib.FPM_ERR_ARG
+    assert _lib.lib.fpm_nbody_adjoint(
+        plan.handle, _lib.ptr(d), _lib.ptr(p), _lib.ptr(f), _lib.ptr(d),
+        _lib.ptr(p), None, None, 0, st) == _lib.FPM_ERR_ARG
+    assert _lib.lib.fpm_nbody_set_tape(plan.handle, None, 0) == _lib.FPM_OK
+  finally:
+    plan.close()
