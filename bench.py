@@ -598,7 +598,8 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
             _lib.ptr(F), _lib.ptr(LX), _lib.ptr(LP), None, _lib.ptr(ck), ckpt,
             st)
   torch.cuda.synchronize()
-  read_kinds([(5, 'adj_drift_paint'), (6, 'adj_vjp'), (7, 'adj_div'),
+  read_kinds([(5, 'adj_drift_paint'),
+              (6, 'adj_drift_vjp' if tape else 'adj_vjp'), (7, 'adj_div'),
               (8, 'adj_potential'), (9, 'adj_position'),
               (1, 'adj_force_solve')])
   _lib.call('fpm_plan_profile', plan.handle, 0)
@@ -632,6 +633,10 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
       # with the potential tape the reverse drift does not paint
       'adj_drift_paint': (112 if tape else 116) * tot_np,
       'adj_vjp': 112 * tot_np,
+      # one pass: read d, F, p, lam_x, lam_p and write them (12 B each way),
+      # gather the adjoint density (4 B per cell) and the three force meshes
+      # (12 B per cell), reduce into the adjoint force mesh (16 B per cell)
+      'adj_drift_vjp': 152 * tot_np,
       'adj_div': 20 * nc_tot,
       'adj_potential': 8 * nc_tot,
       'adj_force_solve': 20 * nc_tot,

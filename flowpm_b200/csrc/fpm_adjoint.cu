@@ -230,6 +230,130 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
   }
 }
 
+// k_adj_drift_paint (without its paint) and k_adj_vjp of the same position
+// it in one pass over the particles, for reverse sweeps whose force meshes
+// of x_it are ready before the reverse drift (the stencil of a stored
+// potential): the state is read and written once instead of twice.  The
+// arithmetic per particle is that of the two kernels in sequence.
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
+k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+               AdjArgs a) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kTraverse);
+    const SimDev S = sims[s];
+    const int T = a.nsteps[s];
+    if (a.it > T) continue;
+    const float* cf = a.coefs + (int64_t)s * a.max_steps * 3;
+    const float b = (float)S.bf;
+    const bool rec = a.it < T;  // a.it >= 0 here
+    const float ke = rec ? cf[a.it * 3 + 2] : 0.f;
+    const float dr = rec ? cf[a.it * 3 + 1] : 0.f;
+    const float ks = rec ? cf[a.it * 3 + 0] : 0.f;
+    const float kep = a.it >= 1 ? cf[(a.it - 1) * 3 + 2] : 0.f;
+    const float cv = ks + kep;
+    const bool last = !rec;
+    const float fac = a.ffac[s];
+    const float invb = 1.0f / b;
+    const float uf = fac * invb;
+    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
+    const float* lr = a.lrho + S.m_off;
+    const float* f0 = a.fmesh + 3 * S.m_off;
+    float* l0 = a.lmesh + (a.lvec4 ? 4 : 3) * S.m_off;
+    const bool ck = rec && a.ckpt && (a.it % a.ckpt_every == 0);
+    const float* ckd =
+        ck ? a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3
+           : nullptr;
+    const float* ckp = ck ? ckd + a.total_np * 3 : nullptr;
+    const Walk w = walk_chunk(S, ch - traverse_first(S));
+#pragma unroll 1
+    for (int item = 0; item < kItems; ++item) {
+      int i, j, k;
+      int64_t local;
+      if (!walk_particle(S, w, item, i, j, k, local)) continue;
+      const int64_t g = S.p_off + local;
+      float3 d = ld3(a.disp, g);
+      float3 lx = ld3(a.lam_x, g);
+      float3 lp = ld3(a.lam_p, g);
+      float3 ph = make_float3(0.f, 0.f, 0.f);
+      if (rec) {  // reverse drift from x_{it+1} (k_adj_drift_paint)
+        const float3 gg = gather_grad(lr, S.mx, S.my, S.mz,
+                                      mesh_pos(S, i, j, k, d));
+        lx.x += b * gg.x;
+        lx.y += b * gg.y;
+        lx.z += b * gg.z;
+        const float3 fo = ld3(a.fpart, g);
+        const float3 p = ld3(a.mom, g);
+        ph = make_float3(__fsub_rn(p.x, __fmul_rn(ke, fo.x)),
+                         __fsub_rn(p.y, __fmul_rn(ke, fo.y)),
+                         __fsub_rn(p.z, __fmul_rn(ke, fo.z)));
+        d = make_float3(__fsub_rn(d.x, __fmul_rn(dr, ph.x)),
+                        __fsub_rn(d.y, __fmul_rn(dr, ph.y)),
+                        __fsub_rn(d.z, __fmul_rn(dr, ph.z)));
+        if (ckd) d = ld3(ckd, g);
+        lp.x += dr * lx.x;
+        lp.y += dr * lx.y;
+        lp.z += dr * lx.z;
+        st3(a.disp, g, d);
+        st3(a.lam_p, g, lp);
+      }
+      // force VJP at x_it (k_adj_vjp)
+      float3 v = make_float3(cv * lp.x, cv * lp.y, cv * lp.z);
+      if (last && a.lam_f) {
+        const float3 lf = ld3(a.lam_f, g);
+        v.x += lf.x;
+        v.y += lf.y;
+        v.z += lf.z;
+      }
+      const float3 y = mesh_pos(S, i, j, k, d);
+      if (!finite3(y.x, y.y, y.z)) atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
+      const Axis ax = cic_axis(y.x, S.mx), ay = cic_axis(y.y, S.my),
+                 az = cic_axis(y.z, S.mz);
+      const DAxis dx = cic_daxis(y.x), dy = cic_daxis(y.y),
+                  dz = cic_daxis(y.z);
+      float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+      float3 acc = make_float3(0.f, 0.f, 0.f);
+      const float u0 = uf * v.x, u1 = uf * v.y, u2 = uf * v.z;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
+        const float wc = cic_w(ax, ay, az, cx, cy, cz);
+        const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
+                  iz = cz ? az.i1 : az.i0;
+        const int64_t o = ((int64_t)ix * S.my + iy) * S.mz + iz;
+        const float a0 = __ldg(f0 + o), a1 = __ldg(f0 + mcells + o),
+                    a2 = __ldg(f0 + 2 * mcells + o);
+        r0 = __fadd_rn(r0, __fmul_rn(a0, wc));
+        r1 = __fadd_rn(r1, __fmul_rn(a1, wc));
+        r2 = __fadd_rn(r2, __fmul_rn(a2, wc));
+        grad_acc(ax, ay, az, dx, dy, dz, cx, cy, cz,
+                 v.x * a0 + v.y * a1 + v.z * a2, acc);
+        if (a.lvec4) {
+          red_add_v4(l0 + 4 * o, u0 * wc, u1 * wc, u2 * wc);
+        } else {
+          red_add(l0 + o, u0 * wc);
+          red_add(l0 + mcells + o, u1 * wc);
+          red_add(l0 + 2 * mcells + o, u2 * wc);
+        }
+      }
+      const float3 f = make_float3(__fmul_rn(__fmul_rn(r0, fac), invb),
+                                   __fmul_rn(__fmul_rn(r1, fac), invb),
+                                   __fmul_rn(__fmul_rn(r2, fac), invb));
+      lx.x += fac * acc.x;
+      lx.y += fac * acc.y;
+      lx.z += fac * acc.z;
+      st3(a.lam_x, g, lx);
+      st3(a.fpart, g, f);
+      if (rec) {
+        float3 p = make_float3(__fsub_rn(ph.x, __fmul_rn(ks, f.x)),
+                               __fsub_rn(ph.y, __fmul_rn(ks, f.y)),
+                               __fsub_rn(ph.z, __fmul_rn(ks, f.z)));
+        if (ckp) p = ld3(ckp, g);
+        st3(a.mom, g, p);
+      }
+    }
+  }
+}
+
 // lam_rho_k = pre * w(k) * sum_d conj(i g_d) lam_f_d,k  (the transpose of
 // the force transfer function; pre and w as in the forward kernel).
 __global__ void __launch_bounds__(kThreads)
@@ -461,6 +585,13 @@ void launch_adj_vjp(const SimDev* sims, int nsims, int64_t nchunks,
                     const AdjArgs& a, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_adj_vjp<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
+}
+
+void launch_adj_position(const SimDev* sims, int nsims, int64_t nchunks,
+                         const AdjArgs& a, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_adj_position<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims,
+                                                         nchunks, a);
 }
 
 void launch_adj_fourier(const SimDev* sims, int nsims, int64_t nchunks,

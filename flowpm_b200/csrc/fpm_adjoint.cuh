@@ -37,6 +37,10 @@ void launch_adj_drift_paint(const SimDev* sims, int nsims, int64_t nchunks,
                             const AdjArgs& a, cudaStream_t st);
 void launch_adj_vjp(const SimDev* sims, int nsims, int64_t nchunks,
                     const AdjArgs& a, cudaStream_t st);
+// k_adj_drift_paint without the paint followed by k_adj_vjp at the same
+// position (a.it >= 0), in one pass; the force meshes of x_it must be ready.
+void launch_adj_position(const SimDev* sims, int nsims, int64_t nchunks,
+                         const AdjArgs& a, cudaStream_t st);
 void launch_adj_fourier(const SimDev* sims, int nsims, int64_t nchunks,
                         const float2* lk, float2* out, AxisTabs tabs,
                         double r_split2, int deconv, cudaStream_t st);

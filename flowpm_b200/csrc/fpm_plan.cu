@@ -987,30 +987,35 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
   const double r2 = p->r_split * p->r_split;
   const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
   const bool tape = p->tape != nullptr;
-  if (!tape)
-    FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
-  a.paint = tape ? 0 : 1;
-  prof_mark(p, 5, st);
-  launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
-  prof_mark(p, 5, st);
-  FPM_TRY(launch_ok());
-  if (tape) {  // the force meshes of the stored potential of position it
+  const size_t lbytes = sizeof(float) * (a.lvec4 ? 4 : 3) * p->total_m;
+  if (tape) {
+    // the force meshes of x_it from the stored potential, then the reverse
+    // drift and the force VJP of position it in one particle pass
     prof_mark(p, 1, st);
     launch_stencil_grad(p->d_sims, p->nsims, p->ch_m,
                         p->tape + (size_t)it * p->total_m, p->fmesh,
                         p->d_nsteps, it, 0, p->quads, st);
     prof_mark(p, 1, st);
     FPM_TRY(launch_ok());
+    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
+    prof_mark(p, 6, st);
+    launch_adj_position(p->d_sims, p->nsims, traverse_chunks(p), a, st);
+    prof_mark(p, 6, st);
+    FPM_TRY(launch_ok());
   } else {
+    FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
+    a.paint = 1;
+    prof_mark(p, 5, st);
+    launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
+    prof_mark(p, 5, st);
+    FPM_TRY(launch_ok());
     FPM_TRY(force_meshes(p, st, false, it));
+    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
+    prof_mark(p, 6, st);
+    launch_adj_vjp(p->d_sims, p->nsims, traverse_chunks(p), a, st);
+    prof_mark(p, 6, st);
+    FPM_TRY(launch_ok());
   }
-  FPM_CUDA(cudaMemsetAsync(p->lmesh, 0,
-                           sizeof(float) * (a.lvec4 ? 4 : 3) * p->total_m,
-                           st));
-  prof_mark(p, 6, st);
-  launch_adj_vjp(p->d_sims, p->nsims, traverse_chunks(p), a, st);
-  prof_mark(p, 6, st);
-  FPM_TRY(launch_ok());
   const int32_t* act = p->d_nsteps;
   if (stencil_path(p)) {
     // lphi = -sum_d D_d lf_d, then lrho = pre C2R(w R2C(lphi))

@@ -161,11 +161,14 @@ int fpm_plan_status(fpm_plan* plan, int32_t* status, void* stream);
  * call's stream; for meshes on the cuFFT path also around the
  * Green's-function kernel (kind 3) and the stencil gradient (kind 4).
  * fpm_nbody_adjoint records, per position of the reverse sweep, the
- * reverse drift + paint kernel (kind 5), the force VJP kernel (kind 6),
+ * reverse drift + paint kernel (kind 5), the force VJP kernel (kind 6; with
+ * a potential tape, the one kernel that does the reverse drift and the
+ * VJP, and no kind 5),
  * the divergence stencil (kind 7, stencil path), the adjoint potential
  * solve -- adjoint force meshes to the adjoint density, all of its
  * transforms and kernels (kind 8) -- and the whole position (kind 9); its
- * force solves add to kinds 1, 3 and 4.  fpm_plan_profile_read waits for
+ * force solves add to kinds 1, 3 and 4 (with a potential tape, kind 1 is
+ * the stencil of the stored potential).  fpm_plan_profile_read waits for
  * the last event, returns the summed device time and the number of timed
  * launches of `kind`, and resets that kind.  Not for use under CUDA graph
  * capture. */
