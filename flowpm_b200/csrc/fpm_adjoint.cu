@@ -48,13 +48,16 @@ __device__ __forceinline__ float3 gather_grad(const float* __restrict__ m,
              az = cic_axis(y.z, mz);
   const DAxis dx = cic_daxis(y.x), dy = cic_daxis(y.y), dz = cic_daxis(y.z);
   float3 acc = make_float3(0.f, 0.f, 0.f);
+  // 32-bit offsets inside one simulation's mesh (< 2^31 cells)
+  const unsigned rx0 = (unsigned)ax.i0 * (unsigned)my;
+  const unsigned rx1 = (unsigned)ax.i1 * (unsigned)my;
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
-    const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
-              iz = cz ? az.i1 : az.i0;
-    grad_acc(ax, ay, az, dx, dy, dz, cx, cy, cz,
-             __ldg(m + ((int64_t)ix * my + iy) * mz + iz), acc);
+    const unsigned o =
+        ((cx ? rx1 : rx0) + (unsigned)(cy ? ay.i1 : ay.i0)) * (unsigned)mz +
+        (unsigned)(cz ? az.i1 : az.i0);
+    grad_acc(ax, ay, az, dx, dy, dz, cx, cy, cz, __ldg(m + o), acc);
   }
   return acc;
 }
@@ -313,13 +316,16 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       float r0 = 0.f, r1 = 0.f, r2 = 0.f;
       float3 acc = make_float3(0.f, 0.f, 0.f);
       const float u0 = uf * v.x, u1 = uf * v.y, u2 = uf * v.z;
+      // 32-bit offsets inside the simulation's mesh (< 2^31 cells)
+      const unsigned my = S.my, mz = S.mz;
+      const unsigned rx0 = (unsigned)ax.i0 * my, rx1 = (unsigned)ax.i1 * my;
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
         const float wc = cic_w(ax, ay, az, cx, cy, cz);
-        const int ix = cx ? ax.i1 : ax.i0, iy = cy ? ay.i1 : ay.i0,
-                  iz = cz ? az.i1 : az.i0;
-        const int64_t o = ((int64_t)ix * S.my + iy) * S.mz + iz;
+        const unsigned o =
+            ((cx ? rx1 : rx0) + (unsigned)(cy ? ay.i1 : ay.i0)) * mz +
+            (unsigned)(cz ? az.i1 : az.i0);
         const float a0 = __ldg(f0 + o), a1 = __ldg(f0 + mcells + o),
                     a2 = __ldg(f0 + 2 * mcells + o);
         r0 = __fadd_rn(r0, __fmul_rn(a0, wc));
