@@ -173,7 +173,7 @@ class NBody(torch.autograd.Function):
 
   @staticmethod
   def forward(ctx, state, cosmo, stages, nc, pm_nc_factor, checkpoint_every,
-              store_potential=None):
+              store_potential=None, pgd_rows=None):
     B = state.shape[1]
     T = len(stages) - 1
     dims = [tuple(nc) + (int(pm_nc_factor),)] * B
@@ -183,6 +183,8 @@ class NBody(torch.autograd.Function):
     st = _lib.stream_ptr()
     _lib.call('fpm_nbody_set_steps', plan.handle, T, _lib.ivec([T] * B),
               _lib.dvec(coefs.ravel()), _lib.dvec(ffac), st)
+    pgd = None if pgd_rows is None else np.tile(pgd_rows, (B, 1)).ravel()
+    _set_pgd(plan, pgd, st)
     x = state.detach()
     d = _lattice_shift(x[0].contiguous(), nc, -1)
     p = x[1].clone().contiguous()
@@ -192,7 +194,11 @@ class NBody(torch.autograd.Function):
     if k > 0:
       ckpt = torch.empty((T // k + 1, 2) + tuple(p.shape), dtype=torch.float32,
                          device=p.device)
-    tape = _potential_tape(dims, T, store_potential, p.device)
+    if pgd is not None and store_potential is False:
+      raise ValueError('gradients through the PGD correction need '
+                       'store_potential')
+    tape = _potential_tape(dims, T, True if pgd is not None else
+                           store_potential, p.device, pgd is not None)
     if tape is not None:
       _lib.call('fpm_nbody_set_tape', plan.handle, _lib.ptr(tape),
                 tape.numel())
@@ -209,18 +215,19 @@ class NBody(torch.autograd.Function):
     ctx.save_for_backward(d, p, f)
     ctx.ckpt = ckpt
     ctx.tape = tape
-    ctx.args = (dims, T, coefs, ffac, k, list(nc))
+    ctx.args = (dims, T, coefs, ffac, k, list(nc), pgd)
     return out
 
   @staticmethod
   def backward(ctx, g):
     d, p, f = ctx.saved_tensors
-    dims, T, coefs, ffac, k, nc = ctx.args
+    dims, T, coefs, ffac, k, nc, pgd = ctx.args
     B = len(dims)
     plan = get_plan(dims, flags=_lib.FPM_PLAN_ADJOINT)
     st = _lib.stream_ptr()
     _lib.call('fpm_nbody_set_steps', plan.handle, T, _lib.ivec([T] * B),
               _lib.dvec(coefs.ravel()), _lib.dvec(ffac), st)
+    _set_pgd(plan, pgd, st)
     g = g.contiguous()
     lx = g[0].clone()
     lp = g[1].clone()
@@ -239,17 +246,29 @@ class NBody(torch.autograd.Function):
         _lib.call('fpm_nbody_set_tape', plan.handle, None, 0)
     ctx.tape = None
     grad = torch.stack((lx, lp, torch.zeros_like(lx)))
-    return grad, None, None, None, None, None, None
+    return grad, None, None, None, None, None, None, None
 
 
-def _potential_tape(dims, T, store, device):
+def _set_pgd(plan, rows, st):
+  """Switch PGD on (rows: nsims x steps x 3 doubles) or off on the shared
+  plan for this call."""
+  _lib.call('fpm_nbody_set_pgd', plan.handle, 0 if rows is None else 1,
+            None if rows is None else _lib.dvec(rows), st)
+
+
+def _potential_tape(dims, T, store, device, pgd=False):
   """The potential tape of a differentiable nbody call: (T + 1) x the
-  plan's force-mesh cells, or None.  store: True, False, or None for
-  automatic (when it takes under a quarter of the free device memory)."""
+  plan's force-mesh cells (with PGD, also T PGD potentials and T particle
+  displacements; the layout of fpm_nbody_set_tape), or None.  store: True,
+  False, or None for automatic (when it takes under a quarter of the free
+  device memory)."""
   if store is False:
     return None
   cells = sum((b * nx) * (b * ny) * (b * nz) for nx, ny, nz, b in dims)
+  parts = sum(nx * ny * nz for nx, ny, nz, b in dims)
   n = (T + 1) * cells
+  if pgd:
+    n += T * (cells + 3 * parts)
   if store is None:
     if cells % 4:  # the tape's positions must stay 16-byte aligned
       return None

@@ -360,6 +360,82 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
   }
 }
 
+// The PGD move of step it in reverse (flowpm/tfpm.py:369-422 apply_pgd,
+// applied after the drift at :487-488): x_{it+1} = x' + (alpha / B) R(x'),
+// R the readout of the PGD displacement meshes g = D phi_pgd(rho(x')).
+// With lam = dL/dx_{it+1} (after the force's paint adjoint at x_{it+1}):
+//   lam_x' = lam + alpha sum_c grad W(x' - c) (lam . g[c])   (readout weights)
+//            + the paint adjoint of the mesh part, which starts here as the
+//   scatter lf[c] += (alpha / B) lam W(x' - c)  (then divergence, PGD
+//   filter, gather at x' by the next kernel).  x' comes from the tape.
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
+k_adj_pgd(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+          AdjArgs a) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kTraverse);
+    const SimDev S = sims[s];
+    const int T = a.nsteps[s];
+    if (a.it >= T) continue;  // no PGD move after position T
+    const float alpha = a.pgd[((int64_t)s * a.pgd_stride + a.it) * 3];
+    const float b = (float)S.bf;
+    const float invb = 1.0f / b;
+    const float uf = alpha * invb;
+    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
+    const float* lr = a.lrho + S.m_off;
+    const float* f0 = a.fmesh + 3 * S.m_off;
+    float* l0 = a.lmesh + (a.lvec4 ? 4 : 3) * S.m_off;
+    const unsigned my = S.my, mz = S.mz;
+    const Walk w = walk_chunk(S, ch - traverse_first(S));
+#pragma unroll 1
+    for (int item = 0; item < kItems; ++item) {
+      int i, j, k;
+      int64_t local;
+      if (!walk_particle(S, w, item, i, j, k, local)) continue;
+      const int64_t g = S.p_off + local;
+      const float3 d = ld3(a.disp, g);
+      const float3 gg = gather_grad(lr, S.mx, S.my, S.mz,
+                                    mesh_pos(S, i, j, k, d));
+      float3 lx = ld3(a.lam_x, g);
+      lx.x += b * gg.x;
+      lx.y += b * gg.y;
+      lx.z += b * gg.z;
+      const float3 dp = ld3(a.pgd_disp, g);
+      const float3 y = mesh_pos(S, i, j, k, dp);
+      const Axis ax = cic_axis(y.x, S.mx), ay = cic_axis(y.y, S.my),
+                 az = cic_axis(y.z, S.mz);
+      const DAxis dx = cic_daxis(y.x), dy = cic_daxis(y.y),
+                  dz = cic_daxis(y.z);
+      float3 acc = make_float3(0.f, 0.f, 0.f);
+      const float u0 = uf * lx.x, u1 = uf * lx.y, u2 = uf * lx.z;
+      const unsigned rx0 = (unsigned)ax.i0 * my, rx1 = (unsigned)ax.i1 * my;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
+        const float wc = cic_w(ax, ay, az, cx, cy, cz);
+        const unsigned o =
+            ((cx ? rx1 : rx0) + (unsigned)(cy ? ay.i1 : ay.i0)) * mz +
+            (unsigned)(cz ? az.i1 : az.i0);
+        const float a0 = __ldg(f0 + o), a1 = __ldg(f0 + mcells + o),
+                    a2 = __ldg(f0 + 2 * mcells + o);
+        grad_acc(ax, ay, az, dx, dy, dz, cx, cy, cz,
+                 lx.x * a0 + lx.y * a1 + lx.z * a2, acc);
+        if (a.lvec4) {
+          red_add_v4(l0 + 4 * o, u0 * wc, u1 * wc, u2 * wc);
+        } else {
+          red_add(l0 + o, u0 * wc);
+          red_add(l0 + mcells + o, u1 * wc);
+          red_add(l0 + 2 * mcells + o, u2 * wc);
+        }
+      }
+      lx.x += alpha * acc.x;
+      lx.y += alpha * acc.y;
+      lx.z += alpha * acc.z;
+      st3(a.lam_x, g, lx);
+      st3(a.disp, g, dp);
+    }
+  }
+}
+
 // lam_rho_k = pre * w(k) * sum_d conj(i g_d) lam_f_d,k  (the transpose of
 // the force transfer function; pre and w as in the forward kernel).
 __global__ void __launch_bounds__(kThreads)
@@ -591,6 +667,12 @@ void launch_adj_vjp(const SimDev* sims, int nsims, int64_t nchunks,
                     const AdjArgs& a, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_adj_vjp<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
+}
+
+void launch_adj_pgd(const SimDev* sims, int nsims, int64_t nchunks,
+                    const AdjArgs& a, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_adj_pgd<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
 }
 
 void launch_adj_position(const SimDev* sims, int nsims, int64_t nchunks,

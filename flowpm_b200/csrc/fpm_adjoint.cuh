@@ -22,6 +22,9 @@ struct AdjArgs {
   float* rho;             // density target of the paint
   int paint;              // 0: the reverse drift skips the paint of x_it
                           // (force meshes from a stored potential)
+  const float* pgd;       // PGD rows (alpha, kl, ks), stride pgd_stride per
+  int pgd_stride;         //   sim (k_adj_pgd)
+  const float* pgd_disp;  // (total_np, 3) displacement before the PGD move
   const float* coefs;     // (nsims, max_steps, 3) {kick_start, drift, kick_end}
   const float* ffac;      // (nsims)
   const int32_t* nsteps;  // (nsims)
@@ -41,6 +44,13 @@ void launch_adj_vjp(const SimDev* sims, int nsims, int64_t nchunks,
 // position (a.it >= 0), in one pass; the force meshes of x_it must be ready.
 void launch_adj_position(const SimDev* sims, int nsims, int64_t nchunks,
                          const AdjArgs& a, cudaStream_t st);
+// The PGD move of step a.it (x' -> x_{it+1}) in reverse, sims with
+// nsteps > a.it: lam_x += B sum_c lam_rho[c] grad W at x_{it+1} (the force
+// paint adjoint), then at x' = q + pgd_disp with the PGD displacement
+// meshes in fmesh: lam_x += alpha sum_c grad W (lam_x . g[c]) and
+// lmesh[c] += (alpha / B) lam_x W; disp = pgd_disp.
+void launch_adj_pgd(const SimDev* sims, int nsims, int64_t nchunks,
+                    const AdjArgs& a, cudaStream_t st);
 void launch_adj_fourier(const SimDev* sims, int nsims, int64_t nchunks,
                         const float2* lk, float2* out, AxisTabs tabs,
                         double r_split2, int deconv, cudaStream_t st);

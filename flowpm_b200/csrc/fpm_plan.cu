@@ -407,7 +407,8 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1,
 // the force's gradient).  pos >= 0: the sims still moving at step pos
 // (nsteps > pos) with the parameters of step pos; pos < 0: every sim with
 // the parameters of one fpm_pgd call.
-int pgd_meshes(fpm_plan* p, cudaStream_t st, int pos) {
+int pgd_meshes(fpm_plan* p, cudaStream_t st, int pos, float* phi = nullptr) {
+  if (!phi) phi = p->phi;
   const bool single = pos < 0;
   const Green G = pgd_green(p, pos, single);
   const int32_t* act = single ? nullptr : p->d_nsteps;
@@ -422,8 +423,7 @@ int pgd_meshes(fpm_plan* p, cudaStream_t st, int pos) {
     const int n = run_active(r, apos);
     if (n == 0) continue;
     launch_fft_force(p->d_sims, r.first, n, S.mx, S.my, S.mz, p->rho, 1,
-                     p->dk, p->fk, p->fmesh, p->phi, tabs_of(p), G, false,
-                     st);
+                     p->dk, p->fk, p->fmesh, phi, tabs_of(p), G, false, st);
   }
   FPM_TRY(launch_ok());
   if (!any_cufft) return FPM_OK;
@@ -443,11 +443,32 @@ int pgd_meshes(fpm_plan* p, cudaStream_t st, int pos) {
     const int n = run_active(r, apos);
     if (n == 0) continue;
     FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->fk + S.s_off,
-                     p->phi + S.m_off, st));
+                     phi + S.m_off, st));
   }
-  launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, p->phi, p->fmesh, act,
+  launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, phi, p->fmesh, act,
                       apos, 1, p->quads, st);
   return launch_ok();
+}
+
+// Potential tape layout: the force potential of position it (0..T) at
+// it * Nc; with PGD, the PGD potential of step it (0..T-1) at
+// (T + 1 + it) * Nc and the displacement before the PGD move of step it at
+// (2T + 1) * Nc + 3 it Np (Nc, Np: the plan's mesh cells and particles).
+int64_t tape_needed(const fpm_plan* p) {
+  int64_t n = (int64_t)(p->max_steps + 1) * p->total_m;
+  if (p->pgd_on)
+    n += (int64_t)p->max_steps * (p->total_m + 3 * p->total_np);
+  return n;
+}
+float* tape_phi(const fpm_plan* p, int it) {
+  return p->tape + (size_t)it * p->total_m;
+}
+float* tape_pgd_phi(const fpm_plan* p, int it) {
+  return p->tape + (size_t)(p->max_steps + 1 + it) * p->total_m;
+}
+float* tape_pgd_disp(const fpm_plan* p, int it) {
+  return p->tape + (size_t)(2 * p->max_steps + 1) * p->total_m +
+         (size_t)it * 3 * p->total_np;
 }
 
 // Per run and position, the active prefix of the run; batched cuFFT plans
@@ -875,19 +896,22 @@ extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
                        p->d_status, st);
   prof_mark(p, 2, st);
   FPM_TRY(launch_ok());
-  if (p->tape && p->tape_floats < (int64_t)(p->max_steps + 1) * p->total_m)
-    return FPM_ERR_ARG;
+  if (p->tape && p->tape_floats < tape_needed(p)) return FPM_ERR_ARG;
   for (int it = 0; it <= p->max_steps; ++it) {
     FPM_TRY(force_meshes(p, st, it < p->max_steps, it,
-                         p->tape ? p->tape + (size_t)it * p->total_m
-                                 : nullptr));
+                         p->tape ? tape_phi(p, it) : nullptr));
     a.it = it;
     prof_mark(p, 0, st);
     launch_step(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     prof_mark(p, 0, st);
     FPM_TRY(launch_ok());
     if (p->pgd_on && it < p->max_steps) {  // after the drift of step it
-      FPM_TRY(pgd_meshes(p, st, it));
+      FPM_TRY(pgd_meshes(p, st, it,
+                         p->tape ? tape_pgd_phi(p, it) : nullptr));
+      if (p->tape)  // the displacement before the move, for the adjoint
+        FPM_CUDA(cudaMemcpyAsync(tape_pgd_disp(p, it), disp,
+                                 sizeof(float) * 3 * p->total_np,
+                                 cudaMemcpyDeviceToDevice, st));
       launch_pgd(p->d_sims, p->nsims, traverse_chunks(p), disp, p->fmesh,
                  p->rho, p->d_pgd, p->pgd_cap, it, p->d_nsteps, p->d_status,
                  st);
@@ -979,6 +1003,59 @@ extern "C" int fpm_nbody(fpm_plan* p, float* disp, float* mom, float* force,
   return fpm_nbody_run(p, disp, mom, force, inter, flags, nullptr, 0, stream);
 }
 
+// Stencil path: the adjoint density lrho of the adjoint force meshes in
+// lmesh, for the sims with nsteps >= pos: lphi = -sum_d D_d lf_d, then
+// lrho = pre C2R(w R2C(lphi)) with the transfer function G (real, so its
+// own transpose).
+static int adjoint_density(fpm_plan* p, int pos, const Green& G,
+                           cudaStream_t st) {
+  const int32_t* act = p->d_nsteps;
+  prof_mark(p, 7, st);
+  if (p->div_tiled) {
+    for (auto& r : p->runs) {
+      const int n = run_active(r, pos);
+      if (n == 0) continue;
+      const SimDev& S = p->sims[r.first];
+      launch_stencil_div_tiled(p->d_sims, r.first, n, S.mx, S.my, S.mz,
+                               r.div_xc, p->lmesh, p->phi, act, pos, st);
+    }
+  } else {
+    launch_stencil_div(p->d_sims, p->nsims, p->ch_m, p->lmesh, p->phi, act,
+                       pos, st);
+  }
+  prof_mark(p, 7, st);
+  FPM_TRY(launch_ok());
+  prof_mark(p, 8, st);
+  bool any_cufft = false;
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    const int n = run_active(r, pos);
+    if (n == 0) continue;
+    if (r.fused) {  // lrho straight from lphi
+      launch_fft_potential(p->d_sims, r.first, n, S.mx, S.my, S.mz, p->phi,
+                           p->dk, p->lrho, tabs_of(p), G, st);
+      continue;
+    }
+    any_cufft = true;
+    FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->phi + S.m_off,
+                     p->dk + S.s_off, st));
+  }
+  FPM_TRY(launch_ok());
+  if (any_cufft) {
+    potential_modes(p, p->dk, p->dk, nullptr, G, act, pos, st);
+    FPM_TRY(launch_ok());
+    for (auto& r : p->runs) {
+      const SimDev& S = p->sims[r.first];
+      const int n = run_active(r, pos);
+      if (n == 0 || r.fused) continue;
+      FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->dk + S.s_off,
+                       p->lrho + S.m_off, st));
+    }
+  }
+  prof_mark(p, 8, st);
+  return FPM_OK;
+}
+
 // One position of the reverse sweep (flowpm's nbody adjoint, see
 // fpm_nbody_adjoint): reverse drift and paint of x_it, its force meshes,
 // the force VJP into the adjoint force meshes, and their adjoint density
@@ -988,13 +1065,29 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
   const int deconv = (p->flags & FPM_PLAN_CIC_DECONV) ? 1 : 0;
   const bool tape = p->tape != nullptr;
   const size_t lbytes = sizeof(float) * (a.lvec4 ? 4 : 3) * p->total_m;
+  if (tape && p->pgd_on && it < p->max_steps) {
+    // the PGD move of step it (x' -> x_{it+1}) in reverse, for the sims
+    // with nsteps > it: its displacement meshes at x' from the stored PGD
+    // potential, the paint adjoint of the force at x_{it+1} and the PGD
+    // VJP at the stored x' (k_adj_pgd), then the adjoint density of the
+    // PGD meshes, which the reverse drift below gathers at x'
+    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, tape_pgd_phi(p, it),
+                        p->fmesh, p->d_nsteps, it + 1, 0, p->quads, st);
+    FPM_TRY(launch_ok());
+    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
+    a.pgd = p->d_pgd;
+    a.pgd_stride = p->pgd_cap;
+    a.pgd_disp = tape_pgd_disp(p, it);
+    launch_adj_pgd(p->d_sims, p->nsims, traverse_chunks(p), a, st);
+    FPM_TRY(launch_ok());
+    FPM_TRY(adjoint_density(p, it + 1, pgd_green(p, it, false), st));
+  }
   if (tape) {
     // the force meshes of x_it from the stored potential, then the reverse
     // drift and the force VJP of position it in one particle pass
     prof_mark(p, 1, st);
-    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m,
-                        p->tape + (size_t)it * p->total_m, p->fmesh,
-                        p->d_nsteps, it, 0, p->quads, st);
+    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, tape_phi(p, it),
+                        p->fmesh, p->d_nsteps, it, 0, p->quads, st);
     prof_mark(p, 1, st);
     FPM_TRY(launch_ok());
     FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
@@ -1016,62 +1109,22 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
     prof_mark(p, 6, st);
     FPM_TRY(launch_ok());
   }
-  const int32_t* act = p->d_nsteps;
-  if (stencil_path(p)) {
-    // lphi = -sum_d D_d lf_d, then lrho = pre C2R(w R2C(lphi))
-    prof_mark(p, 7, st);
-    if (p->div_tiled) {
-      for (auto& r : p->runs) {
-        const int n = run_active(r, it);
-        if (n == 0) continue;
-        const SimDev& S = p->sims[r.first];
-        launch_stencil_div_tiled(p->d_sims, r.first, n, S.mx, S.my, S.mz,
-                                 r.div_xc, p->lmesh, p->phi, act, it, st);
-      }
-    } else {
-      launch_stencil_div(p->d_sims, p->nsims, p->ch_m, p->lmesh, p->phi, act,
-                         it, st);
-    }
-    prof_mark(p, 7, st);
-    FPM_TRY(launch_ok());
-    prof_mark(p, 8, st);
-    bool any_cufft = false;
-    for (auto& r : p->runs) {
-      const SimDev& S = p->sims[r.first];
-      const int n = run_active(r, it);
-      if (n == 0) continue;
-      if (r.fused) {  // lrho straight from lphi
-        launch_fft_potential(p->d_sims, r.first, n, S.mx, S.my, S.mz,
-                             p->phi, p->dk, p->lrho, tabs_of(p),
-                             plan_green(p), st);
-        continue;
-      }
-      any_cufft = true;
-      FPM_TRY(exec_r2c(pick(r, n, r.r2c, r.r2c_n), p->phi + S.m_off,
-                       p->dk + S.s_off, st));
-    }
-    FPM_TRY(launch_ok());
-    if (any_cufft) {
-      potential_modes(p, p->dk, p->dk, nullptr, plan_green(p), act, it, st);
-      FPM_TRY(launch_ok());
-    }
-  } else {
-    prof_mark(p, 8, st);
-    for (auto& r : p->runs) {
-      const SimDev& S = p->sims[r.first];
-      const int n = run_active(r, it);
-      if (n == 0) continue;
-      FPM_TRY(exec_r2c(pick(r, n, r.r2c3, r.r2c3_n), p->lmesh + 3 * S.m_off,
-                       p->fk + 3 * S.s_off, st));
-    }
-    launch_adj_fourier(p->d_sims, p->nsims, p->ch_s, p->fk, p->dk,
-                       tabs_of(p), r2, deconv, st);
-    FPM_TRY(launch_ok());
-  }
+  if (stencil_path(p)) return adjoint_density(p, it, plan_green(p), st);
+  prof_mark(p, 8, st);
   for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
     const int n = run_active(r, it);
-    if (n == 0 || (r.fused && stencil_path(p))) continue;
+    if (n == 0) continue;
+    FPM_TRY(exec_r2c(pick(r, n, r.r2c3, r.r2c3_n), p->lmesh + 3 * S.m_off,
+                     p->fk + 3 * S.s_off, st));
+  }
+  launch_adj_fourier(p->d_sims, p->nsims, p->ch_s, p->fk, p->dk, tabs_of(p),
+                     r2, deconv, st);
+  FPM_TRY(launch_ok());
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    const int n = run_active(r, it);
+    if (n == 0) continue;
     FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->dk + S.s_off,
                      p->lrho + S.m_off, st));
   }
@@ -1088,9 +1141,9 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
       (ckpt && ckpt_every < 1))
     return FPM_ERR_ARG;
   if (!(p->flags & FPM_PLAN_ADJOINT) || !p->steps_set) return FPM_ERR_STATE;
-  if (p->pgd_on) return FPM_ERR_UNSUPPORTED;  // no adjoint of the PGD step
-  if (p->tape && p->tape_floats < (int64_t)(p->max_steps + 1) * p->total_m)
-    return FPM_ERR_ARG;
+  // the PGD move cannot be undone in place: its adjoint needs the tape
+  if (p->pgd_on && !p->tape) return FPM_ERR_UNSUPPORTED;
+  if (p->tape && p->tape_floats < tape_needed(p)) return FPM_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   FPM_CUDA(cudaMemcpyAsync(p->fpart, force, sizeof(float) * 3 * p->total_np,
                            cudaMemcpyDeviceToDevice, st));
@@ -1106,6 +1159,9 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   a.lmesh = p->lmesh;
   a.lvec4 = stencil_path(p) ? 1 : 0;
   a.paint = 1;
+  a.pgd = nullptr;
+  a.pgd_stride = 0;
+  a.pgd_disp = nullptr;
   a.rho = p->rho;
   a.coefs = p->d_coefs;
   a.ffac = p->d_ffac;

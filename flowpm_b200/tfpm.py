@@ -233,7 +233,9 @@ def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
 
   With ``pgdparams`` (one row (alpha, kl, ks) per step) the PGD
   correction moves the particles after every drift (flowpm/tfpm.py:487-488,
-  see ``pgd``); that path has no gradient.
+  see ``pgd``); its gradient needs the stored potentials (the tape also
+  keeps each step's PGD potential and pre-move displacement), so
+  ``store_potential=False`` is refused there.
 
   With ``check_finite`` the device status word is read at the end and a
   non-finite particle state raises ``FlowPMError``."""
@@ -248,14 +250,11 @@ def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
   if pgdparams is not None and T > 0:
     par = _pgd_rows(pgdparams, T)
   if _autograd.needs_grad(state):
-    if par is not None:
-      raise NotImplementedError(
-          'gradients through the PGD correction are not supported')
     if return_intermediate_states:
       raise NotImplementedError(
           'gradients through intermediate states are not supported')
     out = _autograd.NBody.apply(state, cosmo, stages, nc, pm_nc_factor,
-                                checkpoint_every, store_potential)
+                                checkpoint_every, store_potential, par)
     if check_finite:
       plan = get_plan([tuple(nc) + (int(pm_nc_factor),)] * B,
                       flags=_lib.FPM_PLAN_ADJOINT)

@@ -231,7 +231,9 @@ int fpm_pgd(fpm_plan* plan, float* disp, const double* params, void* stream);
  * j = 0 the initial state) with j % ckpt_every == 0 in slot j / ckpt_every
  * of ckpt, each slot 2 x total_particles x 3 floats (disp then mom). */
 
-/* Reverse-time adjoint of fpm_nbody_run (the FastPM adjoint method):
+/* Reverse-time adjoint of fpm_nbody_run (the FastPM adjoint method; with
+ * PGD on it needs a potential tape, fpm_nbody_set_tape, else
+ * FPM_ERR_UNSUPPORTED):
  * given the final state (disp, mom, force = the outputs of the forward run)
  * and the cotangents lam_x = dL/dX, lam_p = dL/dp, lam_f = dL/dF (may be
  * NULL) at the final positions, integrate the leapfrog backwards --
@@ -254,10 +256,17 @@ int fpm_nbody_adjoint(fpm_plan* plan, float* disp, float* mom,
  * meshes of each position from the stencil of that potential instead of
  * painting the rebuilt positions and solving again; the forward values
  * replace the rebuilt ones, which removes the reconstruction drift from
- * the forces.  total_mesh_cells is the sum over the simulations of
- * (pm_nc_factor)^3 nx ny nz; floats must be at least (max_steps + 1) times
- * it (checked by both calls: FPM_ERR_ARG).  The adjoint must follow a
- * forward run with the same tape and steps.  NULL detaches; setting or
+ * the forces.  total_mesh_cells (Nc) is the sum over the simulations of
+ * (pm_nc_factor)^3 nx ny nz; floats must be at least (max_steps + 1) Nc
+ * (checked by both calls: FPM_ERR_ARG).  With PGD on (fpm_nbody_set_pgd)
+ * the tape also holds, per step it < max_steps, the PGD potential at
+ * (max_steps + 1 + it) Nc and the displacement before the PGD move at
+ * (2 max_steps + 1) Nc + 3 it Np (Np = total particles): (2 max_steps + 1)
+ * Nc + 3 max_steps Np floats in all.  This is what makes the PGD step
+ * differentiable: the reverse sweep cannot undo the move, so it takes x'
+ * from the tape and propagates the cotangents through the PGD readout,
+ * its transfer function and its paint (flowpm/tfpm.py:369-422).  The
+ * adjoint must follow a forward run with the same tape and steps.  NULL detaches; setting or
  * detaching a tape invalidates captured graphs (FPM_ERR_STATE).  This has
  * no counterpart in the reference, whose tape stores every TF op. */
 int fpm_nbody_set_tape(fpm_plan* plan, float* tape, int64_t floats);

@@ -377,9 +377,12 @@ def test_pgd_golden(fpm, capsys):
   # PGD off again on the same plan
   st = host(fpm.nbody(c, s0, z['stages'], 16))
   assert_allclose(st, nb['n16_b1_final'], atol=1e-4)
-  with pytest.raises(NotImplementedError):
+  # gradients through PGD need the stored potentials
+  # (tests/test_gpu_adjoint.py checks them against the FP64 oracle)
+  with pytest.raises(ValueError):
     x = torch.tensor(s0, device='cuda').requires_grad_(True)
-    fpm.nbody(c, x, z['stages'], 16, pgdparams=z['params'])
+    fpm.nbody(c, x, z['stages'], 16, pgdparams=z['params'],
+              store_potential=False)
 
 
 def test_nbody_stream_matches_nbody(fpm):
