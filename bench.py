@@ -9,6 +9,12 @@ steps / device time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
+Beside the headline line's main figures, a single-GPU run also reports
+C4 (128^3 forward + adjoint), C3 (a batch of uneven simulations against
+one plan per simulation) and C5 (two 512^3 simulations, 30 steps, forward
++ reverse-time adjoint, with a per-kernel roofline table); --no-extras
+skips them, --no-c5 skips C5.
+
 Under torchrun every rank advances its own replica (different seed), the
 timed region is bracketed by barriers and the max device time over ranks is
 used.  ``--impl reference`` times the CPU restatement of the reference's
@@ -57,7 +63,10 @@ def parse():
                   choices=['flowpm_b200', 'reference'])
   ap.add_argument('--no-cpu-baseline', action='store_true')
   ap.add_argument('--c5', action='store_true',
-                  help='also measure the 2 x 512^3 forward + adjoint config')
+                  help='measure the 2 x 512^3 forward + adjoint config even '
+                  'with --no-extras (it runs by default otherwise)')
+  ap.add_argument('--no-c5', action='store_true',
+                  help='skip the 2 x 512^3 forward + adjoint config')
   ap.add_argument('--no-potential-tape', action='store_true',
                   help='C4 / C5: rebuild the force meshes of the reverse '
                   'sweep (paint + Fourier solve) instead of keeping the '
@@ -901,9 +910,13 @@ def main():
     line['fwd_adjoint'] = measure_fwd_adjoint(
         fpm, flush, max(args.steps, 3), tape=not args.no_potential_tape)
     line['batched'] = measure_batched(fpm, flush, max(args.steps, 3))
-  if world == 1 and args.c5:
-    line['large'] = measure_large(fpm, flush, n=args.c5_mesh,
-                                  tape=not args.no_potential_tape)
+  if world == 1 and (args.c5 or not (args.no_extras or args.no_c5)):
+    try:
+      line['large'] = measure_large(fpm, flush, n=args.c5_mesh,
+                                    tape=not args.no_potential_tape)
+    except (_lib.FlowPMError, RuntimeError) as e:  # e.g. out of memory
+      line['large'] = {'error': str(e)[:300]}
+      torch.cuda.empty_cache()
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     line['cpu_baseline'] = cpu_baseline()
   _lib.lib.fpm_graph_destroy(graph)
