@@ -216,8 +216,9 @@ int fpm_nbody_run(fpm_plan* plan, float* disp, float* mom, float* force,
  * simulation and step, nsims x max_steps x 3 doubles, kl and ks in the
  * units of the force mesh's k = 2 pi fftfreq.  Call after
  * fpm_nbody_set_steps (a set_steps that grows the tables switches PGD off
- * again).  enable = 0 switches it off.  Plans with PGD on have no adjoint
- * (FPM_ERR_UNSUPPORTED).  Synchronises the stream once. */
+ * again).  enable = 0 switches it off.  With PGD on, fpm_nbody_adjoint
+ * needs a potential tape (fpm_nbody_set_tape; else FPM_ERR_UNSUPPORTED).
+ * Synchronises the stream once. */
 int fpm_nbody_set_pgd(fpm_plan* plan, int enable, const double* params,
                       void* stream);
 
