@@ -294,6 +294,7 @@ __global__ void __launch_bounds__(kPlaneThreads)
 k_fft_plane_fwd(const SimDev* __restrict__ sims, int first, int nx,
                 float* __restrict__ rho, float2* __restrict__ dk,
                 int zero_rho) {
+  pdl_wait();  // the density painted before
   extern __shared__ float2 P[];  // NY rows of M + 1
   constexpr int T = kPlaneThreads;
   constexpr int NZH = M + 1;
@@ -360,6 +361,7 @@ template <int NX, bool GRAD3>
 __global__ void __launch_bounds__(kFftThreads)
 k_fft_columns(const SimDev* __restrict__ sims, int first, int nblk,
               float2* dk, float2* __restrict__ fk, AxisTabs tabs, Green G) {
+  pdl_wait();
   constexpr int N1 = Split<NX>::N1, N2 = Split<NX>::N2;
   constexpr int C = kFftThreads / N2;
   __shared__ float2 ex[C * NX];
@@ -572,6 +574,7 @@ __global__ void __launch_bounds__(kPlaneThreads)
 k_fft_plane_inv(const SimDev* __restrict__ sims, int first, int nx,
                 const float2* __restrict__ spec, float* __restrict__ fmesh,
                 float* __restrict__ phi) {
+  pdl_wait();
   constexpr bool GRAD3 = MODE == kOutGrad3;
   extern __shared__ float2 P[];
   constexpr int T = kPlaneThreads;
@@ -670,6 +673,7 @@ template <int NY, int NZ>
 __global__ void __launch_bounds__(kFftThreads)
 k_fft_stencil_x(const SimDev* __restrict__ sims, int first, int nx,
                 const float* __restrict__ phi, float* __restrict__ fmesh) {
+  pdl_wait();
   constexpr int PL = NY * NZ / 4;  // float4 per plane
   const int64_t total = (int64_t)nx * PL;
   const int s = first + blockIdx.y;
@@ -742,8 +746,8 @@ void launch_shape(const SimDev* sims, int first, int n, int nx, float* rho,
                   float* phi, AxisTabs tabs, const Green& G, bool grad3,
                   bool real_out, cudaStream_t st) {
   const size_t smem = (size_t)NY * (M + 1) * sizeof(float2);
-  k_fft_plane_fwd<NY, M><<<n * nx, kPlaneThreads, smem, st>>>(
-      sims, first, nx, rho, dk, zero_rho);
+  launch_pdl(k_fft_plane_fwd<NY, M>, dim3(n * nx), dim3(kPlaneThreads), smem,
+             st, sims, first, nx, rho, dk, zero_rho);
   const int ncols = NY * (M + 1);
   switch (nx) {
 #define FPM_COL_CASE(NN)                                                   \
@@ -751,11 +755,12 @@ void launch_shape(const SimDev* sims, int first, int n, int nx, float* rho,
     constexpr int C = kFftThreads / Split<NN>::N2;                         \
     const int nblk = (ncols + C - 1) / C;                                  \
     if (grad3)                                                             \
-      k_fft_columns<NN, true><<<n * nblk, kFftThreads, 0, st>>>(           \
-          sims, first, nblk, dk, fk, tabs, G);                             \
+      launch_pdl(k_fft_columns<NN, true>, dim3(n * nblk), dim3(kFftThreads), \
+                 0, st, sims, first, nblk, dk, fk, tabs, G);               \
     else                                                                   \
-      k_fft_columns<NN, false><<<n * nblk, kFftThreads, 0, st>>>(          \
-          sims, first, nblk, dk, fk, tabs, G);                             \
+      launch_pdl(k_fft_columns<NN, false>, dim3(n * nblk),                 \
+                 dim3(kFftThreads), 0, st, sims, first, nblk, dk, fk, tabs, \
+                 G);                                                       \
     break;                                                                 \
   }
     FPM_FFT_SIZES(FPM_COL_CASE)
@@ -771,14 +776,16 @@ void launch_shape(const SimDev* sims, int first, int n, int nx, float* rho,
         sims, first, nx, dk, nullptr, phi);
     return;
   }
-  k_fft_plane_inv<NY, M, kOutStencil><<<n * nx, kPlaneThreads, smem, st>>>(
-      sims, first, nx, dk, fmesh, phi);
+  launch_pdl(k_fft_plane_inv<NY, M, kOutStencil>, dim3(n * nx),
+             dim3(kPlaneThreads), smem, st, sims, first, nx,
+             (const float2*)dk, fmesh, phi);
   const int64_t quads = (int64_t)nx * NY * 2 * M / 4;
   int64_t bx = (quads + kFftThreads - 1) / kFftThreads;
   const int64_t cap = (int64_t)kNumSMs * 8 / (n < 1 ? 1 : n) + 1;
   if (bx > cap) bx = cap;
-  k_fft_stencil_x<NY, 2 * M><<<dim3((unsigned)bx, (unsigned)n), kFftThreads,
-                               0, st>>>(sims, first, nx, phi, fmesh);
+  launch_pdl(k_fft_stencil_x<NY, 2 * M>, dim3((unsigned)bx, (unsigned)n),
+             dim3(kFftThreads), 0, st, sims, first, nx, (const float*)phi,
+             fmesh);
 }
 
 template <int NY>

@@ -39,6 +39,7 @@ k_paint_lattice(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 __global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
        StepArgs a) {
+  pdl_wait();  // the force meshes of the solve before
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const int s = find_sim(sims, nsims, ch, kTraverse);
     const SimDev S = sims[s];
@@ -872,7 +873,8 @@ void launch_stencil_div_tiled(const SimDev* sims, int first, int count,
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,
                  const StepArgs& a, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_step<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
+  launch_pdl(k_step, dim3(grid_for(nchunks)), dim3(kThreads), 0, st, sims,
+             nsims, nchunks, a);
 }
 
 void launch_pgd(const SimDev* sims, int nsims, int64_t nchunks, float* disp,
