@@ -911,12 +911,15 @@ def main():
         fpm, flush, max(args.steps, 3), tape=not args.no_potential_tape)
     line['batched'] = measure_batched(fpm, flush, max(args.steps, 3))
   if world == 1 and (args.c5 or not (args.no_extras or args.no_c5)):
+    torch.cuda.nvtx.range_push('c5')  # lets a profiler select this part
     try:
       line['large'] = measure_large(fpm, flush, n=args.c5_mesh,
                                     tape=not args.no_potential_tape)
     except (_lib.FlowPMError, RuntimeError) as e:  # e.g. out of memory
       line['large'] = {'error': str(e)[:300]}
       torch.cuda.empty_cache()
+    finally:
+      torch.cuda.nvtx.range_pop()
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     line['cpu_baseline'] = cpu_baseline()
   _lib.lib.fpm_graph_destroy(graph)
