@@ -642,10 +642,11 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
       # with the potential tape the reverse drift does not paint
       'adj_drift_paint': (112 if tape else 116) * tot_np,
       'adj_vjp': 112 * tot_np,
-      # one pass: read d, F, p, lam_x, lam_p and write them (12 B each way),
-      # gather the adjoint density (4 B per cell) and the three force meshes
-      # (12 B per cell), reduce into the adjoint force mesh (16 B per cell)
-      'adj_drift_vjp': 152 * tot_np,
+      # one pass: read and write d, p, lam_x, lam_p (12 B each way; p
+      # carries the next step's p_half, so no force buffer), gather the
+      # adjoint density (4 B per cell) and the three force meshes (12 B
+      # per cell), reduce into the adjoint force mesh (16 B per cell)
+      'adj_drift_vjp': 128 * tot_np,
       'adj_div': 20 * nc_tot,
       'adj_potential': 8 * nc_tot,
       'adj_force_solve': 20 * nc_tot,

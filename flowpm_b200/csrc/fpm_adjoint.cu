@@ -237,7 +237,11 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 // it in one pass over the particles, for reverse sweeps whose force meshes
 // of x_it are ready before the reverse drift (the stencil of a stored
 // potential): the state is read and written once instead of twice.  The
-// arithmetic per particle is that of the two kernels in sequence.
+// arithmetic per particle is that of the two kernels in sequence, except
+// that the momentum buffer carries p_half of the next (earlier) step,
+// p_it - ke_{it-1} F_it, formed here with the same two roundings, instead
+// of p_it and F_it in two buffers; the last position (it = 0) leaves p_0.
+// The force buffer is not used.
 __global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                AdjArgs a) {
@@ -249,7 +253,6 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float* cf = a.coefs + (int64_t)s * a.max_steps * 3;
     const float b = (float)S.bf;
     const bool rec = a.it < T;  // a.it >= 0 here
-    const float ke = rec ? cf[a.it * 3 + 2] : 0.f;
     const float dr = rec ? cf[a.it * 3 + 1] : 0.f;
     const float ks = rec ? cf[a.it * 3 + 0] : 0.f;
     const float kep = a.it >= 1 ? cf[(a.it - 1) * 3 + 2] : 0.f;
@@ -277,18 +280,14 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       float3 d = ld3(a.disp, g);
       float3 lx = ld3(a.lam_x, g);
       float3 lp = ld3(a.lam_p, g);
-      float3 ph = make_float3(0.f, 0.f, 0.f);
+      // rec: p_half of step it (left by the position after); else p_T
+      const float3 ph = ld3(a.mom, g);
       if (rec) {  // reverse drift from x_{it+1} (k_adj_drift_paint)
         const float3 gg = gather_grad(lr, S.mx, S.my, S.mz,
                                       mesh_pos(S, i, j, k, d));
         lx.x += b * gg.x;
         lx.y += b * gg.y;
         lx.z += b * gg.z;
-        const float3 fo = ld3(a.fpart, g);
-        const float3 p = ld3(a.mom, g);
-        ph = make_float3(__fsub_rn(p.x, __fmul_rn(ke, fo.x)),
-                         __fsub_rn(p.y, __fmul_rn(ke, fo.y)),
-                         __fsub_rn(p.z, __fmul_rn(ke, fo.z)));
         d = make_float3(__fsub_rn(d.x, __fmul_rn(dr, ph.x)),
                         __fsub_rn(d.y, __fmul_rn(dr, ph.y)),
                         __fsub_rn(d.z, __fmul_rn(dr, ph.z)));
@@ -348,14 +347,20 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       lx.y += fac * acc.y;
       lx.z += fac * acc.z;
       st3(a.lam_x, g, lx);
-      st3(a.fpart, g, f);
+      // p_it (rec: p_half - ks F_it, or the checkpoint; else p_T), then
+      // p_half of step it-1 for the next position
+      float3 p = ph;
       if (rec) {
-        float3 p = make_float3(__fsub_rn(ph.x, __fmul_rn(ks, f.x)),
-                               __fsub_rn(ph.y, __fmul_rn(ks, f.y)),
-                               __fsub_rn(ph.z, __fmul_rn(ks, f.z)));
+        p = make_float3(__fsub_rn(ph.x, __fmul_rn(ks, f.x)),
+                        __fsub_rn(ph.y, __fmul_rn(ks, f.y)),
+                        __fsub_rn(ph.z, __fmul_rn(ks, f.z)));
         if (ckp) p = ld3(ckp, g);
-        st3(a.mom, g, p);
       }
+      if (a.it >= 1)
+        p = make_float3(__fsub_rn(p.x, __fmul_rn(kep, f.x)),
+                        __fsub_rn(p.y, __fmul_rn(kep, f.y)),
+                        __fsub_rn(p.z, __fmul_rn(kep, f.z)));
+      if (rec || a.it >= 1) st3(a.mom, g, p);
     }
   }
 }

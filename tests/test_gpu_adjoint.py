@@ -271,7 +271,8 @@ def test_potential_tape_arguments(fpm):
 
 def _run_adjoint(sims, d0, p0, lx0, lp0, tape):
   """Forward + reverse sweep through the C ABI for simulations
-  [(T, stages)] of 16^3 in one plan: returns dL/dX_0, dL/dp_0."""
+  [(T, stages)] of 16^3 in one plan: returns dL/dX_0, dL/dp_0 and the
+  rebuilt initial displacement and momentum."""
   from flowpm_b200 import _lib, tfbackground
   from flowpm_b200._plans import Plan
   n = 16**3
@@ -299,7 +300,7 @@ def _run_adjoint(sims, d0, p0, lx0, lp0, tape):
     _lib.call('fpm_nbody_adjoint', plan.handle, _lib.ptr(d), _lib.ptr(p),
               _lib.ptr(f), _lib.ptr(lx), _lib.ptr(lp), None, None, 0, st)
     torch.cuda.synchronize()
-    return host(lx), host(lp)
+    return host(lx), host(lp), host(d), host(p)
   finally:
     plan.close()
 
@@ -309,7 +310,8 @@ def test_potential_tape_uneven_batch(fpm):
   tape (the shorter one leaves its later positions unwritten and the
   reverse sweep must skip them), against one plan per simulation without
   a tape.  Cotangents of the initial state agree to FP32 rounding of the
-  two routes to the force meshes."""
+  two routes to the force meshes, and so does the rebuilt initial state,
+  which is close to the true one."""
   rng = np.random.default_rng(41)
   n = 16**3
   sims = [(5, np.linspace(0.1, 1.0, 6)), (3, np.linspace(0.2, 0.8, 4))]
@@ -321,10 +323,14 @@ def test_potential_tape_uneven_batch(fpm):
                      device='cuda')
   lp0 = torch.tensor(rng.standard_normal((2 * n, 3)), dtype=torch.float32,
                      device='cuda')
-  lx, lp = _run_adjoint(sims, d0, p0, lx0, lp0, tape=True)
+  lx, lp, dd, pp = _run_adjoint(sims, d0, p0, lx0, lp0, tape=True)
   for s in range(2):
     sl = slice(s * n, (s + 1) * n)
-    rx, rp = _run_adjoint([sims[s]], d0[sl], p0[sl], lx0[sl], lp0[sl],
-                          tape=False)
+    rx, rp, rd, rpp = _run_adjoint([sims[s]], d0[sl], p0[sl], lx0[sl],
+                                   lp0[sl], tape=False)
     assert rel_l2(lx[sl], rx) < 1e-4, (s, rel_l2(lx[sl], rx))
     assert rel_l2(lp[sl], rp) < 1e-4, (s, rel_l2(lp[sl], rp))
+    assert np.abs(dd[sl] - rd).max() < 1e-4, (s, np.abs(dd[sl] - rd).max())
+    assert np.abs(pp[sl] - rpp).max() < 1e-4, (s, np.abs(pp[sl] - rpp).max())
+    assert np.abs(dd[sl] - host(d0[sl])).max() < 1e-3
+    assert np.abs(pp[sl] - host(p0[sl])).max() < 1e-3
