@@ -649,7 +649,8 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
       'adj_drift_vjp': 128 * tot_np,
       'adj_div': 20 * nc_tot,
       'adj_potential': 8 * nc_tot,
-      'adj_force_solve': 20 * nc_tot,
+      # with the tape: the stencil of the stored potential, 16 B per cell
+      'adj_force_solve': (16 if tape else 20) * nc_tot,
   }
   roof = {}
   for k, (ms, cnt) in kt.items():

@@ -595,6 +595,106 @@ k_stencil_div_tiled(const SimDev* __restrict__ sims, int first,
   }
 }
 
+// k_stencil_grad over the same 16 x 64 (y, z) tiles as k_stencil_div_tiled,
+// marching over XC x planes: phi at x +- 1, x +- 2 of a block's cells from a
+// window of five planes in registers, phi of the current plane with a halo
+// of two cells in y and z from a ring of three planes in shared memory, so
+// every phi value is read about once.  Same arithmetic as k_stencil_grad,
+// bit for bit; three force planes out (sim s at fmesh + 3 m_off).
+template <int XC>
+__global__ void __launch_bounds__(256, 3)
+k_stencil_grad_tiled(const SimDev* __restrict__ sims, int first,
+                     const float* __restrict__ phi, float* __restrict__ fmesh,
+                     const int32_t* __restrict__ nsteps, int pos) {
+  __shared__ float sp[3][kDivRows][kDivRS];
+  const int s = first + blockIdx.y;
+  if (nsteps && pos > nsteps[s]) return;
+  const SimDev& S = sims[s];
+  const int mx = S.mx, my = S.my, mz = S.mz;
+  const int nzt = mz / kDivTZ, nyt = my / kDivTY;
+  int b = blockIdx.x;
+  const int z0 = (b % nzt) * kDivTZ;
+  b /= nzt;
+  const int y0 = (b % nyt) * kDivTY;
+  const int x0 = (b / nyt) * XC;
+  const int ty = threadIdx.x >> 4, tq = threadIdx.x & 15;
+  const float* F = phi + S.m_off;
+  const unsigned sx = (unsigned)my * (unsigned)mz;
+  const unsigned mcells = (unsigned)mx * sx;
+  const unsigned own = (unsigned)(y0 + ty) * mz + z0 + tq;
+  const int hr = threadIdx.x >> 6, hc = threadIdx.x & 63;
+  const int hyrow = hr < 2 ? hr : kDivTY + hr;  // tile rows -2,-1,16,17
+  const unsigned hyoff = (unsigned)((y0 - 2 + hyrow + my) % my) * mz + z0 + hc;
+  const bool zh = threadIdx.x < 4 * kDivTY;
+  const int zr = threadIdx.x >> 2, zk = threadIdx.x & 3;
+  const int zcol = zk < 2 ? zk : kDivTZ + zk;   // tile cols -2,-1,64,65
+  const unsigned zhoff =
+      (unsigned)(y0 + (zh ? zr : 0)) * mz + (unsigned)((z0 - 2 + zcol + mz) % mz);
+  auto plane = [&](int x) {
+    return F + (size_t)(unsigned)((x % mx + mx) % mx) * sx;
+  };
+  float xw[5][4];
+  float v[4];
+  float hyv = 0.f, hzv = 0.f;
+  auto load = [&](int x, bool halo) {
+    const float* P = plane(x);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = __ldg(P + own + 16 * i);
+    if (halo) {
+      hyv = __ldg(P + hyoff);
+      if (zh) hzv = __ldg(P + zhoff);
+    }
+  };
+  auto put = [&](int slot) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) sp[slot][ty + 2][tq + 16 * i + 2] = v[i];
+    sp[slot][hyrow][hc + 2] = hyv;
+    if (zh) sp[slot][zr + 2][zcol] = hzv;
+  };
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {  // planes x0 - 2 .. x0 + 2
+    load(x0 - 2 + k, k >= 2);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) xw[k][i] = v[i];
+    if (k >= 2) put(k - 2);
+  }
+  __syncthreads();
+  float* o = fmesh + 3 * S.m_off + own;
+#pragma unroll 1
+  for (int p = 0; p < XC; ++p) {
+    const int slot = p % 3;
+    const bool next = p + 3 <= XC + 1;  // plane x0 + p + 3 enters the window
+    const bool next_slot = p + 3 < XC;  // and is processed
+    if (next) load(x0 + p + 3, next_slot);
+    const int r = ty + 2;
+    const size_t base = (size_t)(unsigned)(x0 + p) * sx;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = tq + 16 * i + 2;
+      o[base + 16 * i] = stencil4(xw[0][i], xw[1][i], xw[3][i], xw[4][i]);
+      o[mcells + base + 16 * i] =
+          stencil4(sp[slot][r - 2][c], sp[slot][r - 1][c],
+                   sp[slot][r + 1][c], sp[slot][r + 2][c]);
+      o[2 * (size_t)mcells + base + 16 * i] =
+          stencil4(sp[slot][r][c - 2], sp[slot][r][c - 1],
+                   sp[slot][r][c + 1], sp[slot][r][c + 2]);
+    }
+    __syncthreads();  // every thread is done with this slot
+    if (next) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        xw[0][i] = xw[1][i];
+        xw[1][i] = xw[2][i];
+        xw[2][i] = xw[3][i];
+        xw[3][i] = xw[4][i];
+        xw[4][i] = v[i];
+      }
+      if (next_slot) put(slot);
+    }
+    // the next plane reads another slot, written two planes ago
+  }
+}
+
 // LPT spectra (flowpm/tfpm.py:66-145 lpt1 / lpt2_source on the lattice).
 __global__ void __launch_bounds__(kThreads)
 k_lpt_fourier(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
@@ -868,6 +968,22 @@ void launch_stencil_div_tiled(const SimDev* sims, int first, int count,
   else
     k_stencil_div_tiled<16><<<grid, 256, 0, st>>>(sims, first, lf, lphi,
                                                   nsteps, pos);
+}
+
+void launch_stencil_grad_tiled(const SimDev* sims, int first, int count,
+                               int mx, int my, int mz, int xc,
+                               const float* phi, float* fmesh,
+                               const int32_t* nsteps, int pos,
+                               cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const dim3 grid((unsigned)((mx / xc) * (my / kDivTY) * (mz / kDivTZ)),
+                  (unsigned)count);
+  if (xc == 32)
+    k_stencil_grad_tiled<32><<<grid, 256, 0, st>>>(sims, first, phi, fmesh,
+                                                   nsteps, pos);
+  else
+    k_stencil_grad_tiled<16><<<grid, 256, 0, st>>>(sims, first, phi, fmesh,
+                                                   nsteps, pos);
 }
 
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,

@@ -68,6 +68,13 @@ void launch_stencil_div(const SimDev* sims, int nsims, int64_t nchunks,
 // shape; stencil_div_chunk gives its x chunk (0: shape not supported, use
 // launch_stencil_div).
 int stencil_div_chunk(int mx, int my, int mz, int64_t m_off, int count);
+// Tiled k_stencil_grad (the same tiles and x chunk as the tiled
+// divergence) over the sims [first, first + count) of one mesh shape.
+void launch_stencil_grad_tiled(const SimDev* sims, int first, int count,
+                               int mx, int my, int mz, int xc,
+                               const float* phi, float* fmesh,
+                               const int32_t* nsteps, int pos,
+                               cudaStream_t st);
 void launch_stencil_div_tiled(const SimDev* sims, int first, int count,
                               int mx, int my, int mz, int xc, const float* lf,
                               float* lphi, const int32_t* nsteps, int pos,

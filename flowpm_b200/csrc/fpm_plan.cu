@@ -328,6 +328,27 @@ void potential_modes(fpm_plan* p, const float2* in, float2* out,
                              tabs_of(p), G, act, pos, 1, st);
 }
 
+// The three force meshes D_d phi of the sims (with act, those with nsteps
+// >= pos; with skip_fused, not the fused-solve runs, which make their own):
+// the tiled stencil when every run takes the tiled stencils, else the
+// per-chunk one.
+void stencil_grad(fpm_plan* p, const float* phi, const int32_t* act, int pos,
+                  int skip_fused, cudaStream_t st) {
+  if (!p->div_tiled) {
+    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, phi, p->fmesh, act, pos,
+                        skip_fused, p->quads, st);
+    return;
+  }
+  for (auto& r : p->runs) {
+    if (skip_fused && r.fused) continue;
+    const int n = run_active(r, pos);
+    if (n == 0) continue;
+    const SimDev& S = p->sims[r.first];
+    launch_stencil_grad_tiled(p->d_sims, r.first, n, S.mx, S.my, S.mz,
+                              r.div_xc, phi, p->fmesh, act, pos, st);
+  }
+}
+
 // Density of the current positions -> force meshes (paint must be done).
 // At leapfrog position it (>= 0) only the active prefix of each run is
 // transformed.
@@ -392,8 +413,7 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1,
   }
   if (stencil_path(p)) {
     prof_mark(p, 4, st);
-    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, phi, p->fmesh, act,
-                        it, 1, p->quads, st);
+    stencil_grad(p, phi, act, it, 1, st);
     prof_mark(p, 4, st);
     FPM_TRY(launch_ok());
   }
@@ -445,8 +465,7 @@ int pgd_meshes(fpm_plan* p, cudaStream_t st, int pos, float* phi = nullptr) {
     FPM_TRY(exec_c2r(pick(r, n, r.c2r1, r.c2r1_n), p->fk + S.s_off,
                      phi + S.m_off, st));
   }
-  launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, phi, p->fmesh, act,
-                      apos, 1, p->quads, st);
+  stencil_grad(p, phi, act, apos, 1, st);
   return launch_ok();
 }
 
@@ -1071,8 +1090,7 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
     // potential, the paint adjoint of the force at x_{it+1} and the PGD
     // VJP at the stored x' (k_adj_pgd), then the adjoint density of the
     // PGD meshes, which the reverse drift below gathers at x'
-    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, tape_pgd_phi(p, it),
-                        p->fmesh, p->d_nsteps, it + 1, 0, p->quads, st);
+    stencil_grad(p, tape_pgd_phi(p, it), p->d_nsteps, it + 1, 0, st);
     FPM_TRY(launch_ok());
     FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
     a.pgd = p->d_pgd;
@@ -1086,8 +1104,7 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
     // the force meshes of x_it from the stored potential, then the reverse
     // drift and the force VJP of position it in one particle pass
     prof_mark(p, 1, st);
-    launch_stencil_grad(p->d_sims, p->nsims, p->ch_m, tape_phi(p, it),
-                        p->fmesh, p->d_nsteps, it, 0, p->quads, st);
+    stencil_grad(p, tape_phi(p, it), p->d_nsteps, it, 0, st);
     prof_mark(p, 1, st);
     FPM_TRY(launch_ok());
     FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));

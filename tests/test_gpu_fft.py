@@ -38,6 +38,9 @@ SHAPES = [
     [(512, 16, 16, 1)],
     [(32, 32, 32, 1), (256, 16, 32, 1), (256, 16, 32, 1), (24, 24, 24, 1),
      (128, 24, 8, 2)],
+    # three 128^3: the cuFFT plan takes the tiled gradient stencil (enough
+    # tiles), the fused solve its own plane stencils
+    [(128, 128, 128, 1)] * 3,
 ]
 
 
