@@ -648,7 +648,9 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
       # per cell), reduce into the adjoint force mesh (16 B per cell)
       'adj_drift_vjp': 128 * tot_np,
       'adj_div': 20 * nc_tot,
-      'adj_potential': 8 * nc_tot,
+      # on x-pass meshes (256 or 512 along x) its x pass also clears the
+      # adjoint force mesh for the next position, 16 B per cell
+      'adj_potential': (24 if n in (256, 512) else 8) * nc_tot,
       # with the tape: the stencil of the stored potential, 16 B per cell
       'adj_force_solve': (16 if tape else 20) * nc_tot,
   }

@@ -450,7 +450,9 @@ k_fft_columns(const SimDev* __restrict__ sims, int first, int nblk,
 // DFTs (cols_dft), a twiddle W_NX^(a kb) and R-point DFTs in registers,
 // where the transfer function is applied and the inverse starts; the
 // column block moves through shared memory as rows of kXCols modes.  With
-// rho_zero, the block also zeroes its share of the sim's density mesh.
+// rho_zero, the block also zeroes its share of that buffer: zmul floats per
+// cell of the sim (1: the density mesh; 4: the interleaved adjoint force
+// mesh).
 // Columns per x-pass block.  Measured on B200 at 2 x 512^3: 8 columns
 // (64-byte rows, 32 KB) 1.19 ms per pass, 16 (128-byte rows, 64 KB) 1.01
 // ms; a persistent variant with cp.async double buffering of 8-column
@@ -464,8 +466,8 @@ template <int NX>
 __global__ void __launch_bounds__(kXThreads)
 k_fft_xcols(const SimDev* __restrict__ sims, int first, int nblk,
             const float2* in, float2* out, float* __restrict__ rho_zero,
-            AxisTabs tabs, Green G, const int32_t* __restrict__ nsteps,
-            int pos) {
+            int zmul, AxisTabs tabs, Green G,
+            const int32_t* __restrict__ nsteps, int pos) {
   constexpr int R = NX / 64, C = kXCols, T = kXThreads;
   constexpr int NP = 64 * C / T;                  // (kb, column) pairs
   constexpr int NS = R * C, NS1 = NS < 64 ? NS : 64;  // sub-lines per pass
@@ -487,10 +489,10 @@ k_fft_xcols(const SimDev* __restrict__ sims, int first, int nblk,
     const int e = threadIdx.x + i * T;
     b4[e] = src[(int64_t)(e / (C / 2)) * rstride + e % (C / 2)];
   }
-  if (rho_zero) {  // this block's share of the density, in float4
-    const int64_t q4 = (int64_t)S.mx * S.my * S.mz / 4;
+  if (rho_zero) {  // this block's share, in float4
+    const int64_t q4 = (int64_t)zmul * S.mx * S.my * S.mz / 4;
     const int64_t per = (q4 + nblk - 1) / nblk;
-    float4* r4 = reinterpret_cast<float4*>(rho_zero + S.m_off);
+    float4* r4 = reinterpret_cast<float4*>(rho_zero + zmul * S.m_off);
     const int64_t e1 = min(q4, (blk + 1) * per);
     for (int64_t e = blk * per + threadIdx.x; e < e1; e += T)
       r4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -757,7 +759,7 @@ void launch_shape(const SimDev* sims, int first, int n, int nx, float* rho,
     const int nblk = ncols / kXCols;  // NY is a multiple of 16
     launch_pdl(k_fft_xcols<128>, dim3(n * nblk), dim3(kXThreads),
                (size_t)128 * kXCols * sizeof(float2), st, sims, first, nblk,
-               (const float2*)dk, dk, (float*)nullptr, tabs, G,
+               (const float2*)dk, dk, (float*)nullptr, 1, tabs, G,
                (const int32_t*)nullptr, 0);
   } else switch (nx) {
 #define FPM_COL_CASE(NN)                                                   \
@@ -929,18 +931,18 @@ int fft_xpass_prepare() {
 
 void launch_fft_xpass(const SimDev* sims, int first, int n, int nx, int ny,
                       int nzh, const float2* in, float2* out, float* rho_zero,
-                      AxisTabs tabs, const Green& G, const int32_t* nsteps,
-                      int pos, cudaStream_t st) {
+                      int zmul, AxisTabs tabs, const Green& G,
+                      const int32_t* nsteps, int pos, cudaStream_t st) {
   if (n <= 0) return;
   g_launches.fetch_add(1, std::memory_order_relaxed);
   const int nblk = ny * nzh / kXCols;
   const unsigned grid = (unsigned)(n * nblk);
   if (nx == 512)
     k_fft_xcols<512><<<grid, kXThreads, xpass_smem(512), st>>>(
-        sims, first, nblk, in, out, rho_zero, tabs, G, nsteps, pos);
+        sims, first, nblk, in, out, rho_zero, zmul, tabs, G, nsteps, pos);
   else
     k_fft_xcols<256><<<grid, kXThreads, xpass_smem(256), st>>>(
-        sims, first, nblk, in, out, rho_zero, tabs, G, nsteps, pos);
+        sims, first, nblk, in, out, rho_zero, zmul, tabs, G, nsteps, pos);
 }
 
 }  // namespace fpm

@@ -108,14 +108,15 @@ void launch_fft_potential(const SimDev* sims, int first, int n, int nx,
 // batched (y, z) plane transforms, potential spectrum out = x-pass(in) of
 // the sims [first, first + n) of one run (in == out allowed; with nsteps,
 // the sims with nsteps < pos skip); with rho_zero it also zeroes their
-// density meshes.  fft_xpass_prepare uploads its twiddles (once per
+// part of that buffer, zmul floats per cell (1: density mesh, 4: the
+// interleaved adjoint force mesh).  fft_xpass_prepare uploads its twiddles (once per
 // device).
 bool fft_xpass_supported(int nx, int ny, int nz);
 int fft_xpass_prepare();
 void launch_fft_xpass(const SimDev* sims, int first, int n, int nx, int ny,
                       int nzh, const float2* in, float2* out, float* rho_zero,
-                      AxisTabs tabs, const Green& G, const int32_t* nsteps,
-                      int pos, cudaStream_t st);
+                      int zmul, AxisTabs tabs, const Green& G,
+                      const int32_t* nsteps, int pos, cudaStream_t st);
 
 // Fused readout + kick(end) + kick(start) + drift + paint of one iteration.
 void launch_step(const SimDev* sims, int nsims, int64_t nchunks,

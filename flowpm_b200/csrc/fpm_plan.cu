@@ -85,6 +85,9 @@ struct fpm_plan {
   int64_t tape_floats = 0;
   bool quads = false;       // every mesh: mz % 4 == 0 and m_off % 4 == 0
   bool div_tiled = false;   // every run takes the tiled divergence stencil
+  bool all_xpass = false;   // every run on the x-pass path: its x pass in
+                            // the reverse sweep zeroes the adjoint force
+                            // mesh after the divergence has read it
   // lattice buffers (FPM_PLAN_LPT)
   float* lreal1 = nullptr;
   float2* lspec1 = nullptr;
@@ -310,7 +313,7 @@ bool stencil_path(const fpm_plan* p) {
 // rho_zero, their density meshes are zeroed.
 void potential_modes(fpm_plan* p, const float2* in, float2* out,
                      float* rho_zero, const Green& G, const int32_t* act,
-                     int pos, cudaStream_t st) {
+                     int pos, cudaStream_t st, int zmul = 1) {
   bool other = false;
   for (auto& r : p->runs) {
     if (r.fused) continue;
@@ -321,7 +324,7 @@ void potential_modes(fpm_plan* p, const float2* in, float2* out,
     const int n = run_active(r, pos);
     const SimDev& S = p->sims[r.first];
     launch_fft_xpass(p->d_sims, r.first, n, S.mx, S.my, S.mzh, in, out,
-                     rho_zero, tabs_of(p), G, act, pos, st);
+                     rho_zero, zmul, tabs_of(p), G, act, pos, st);
   }
   if (other)
     launch_fourier_potential(p->d_sims, p->nsims, p->ch_s, in, out, rho_zero,
@@ -702,6 +705,9 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
       for (int s = r.first; s < r.first + r.count; ++s) p->sims[s].xpass = 1;
     }
   }
+  p->all_xpass = !p->runs.empty();
+  for (auto& r : p->runs)
+    if (!r.xpass) p->all_xpass = false;
   for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
     if (rc == FPM_OK)
@@ -1061,7 +1067,10 @@ static int adjoint_density(fpm_plan* p, int pos, const Green& G,
   }
   FPM_TRY(launch_ok());
   if (any_cufft) {
-    potential_modes(p, p->dk, p->dk, nullptr, G, act, pos, st);
+    // on the x-pass path the x pass also clears the adjoint force mesh,
+    // which the divergence above has consumed, for the next scatter
+    potential_modes(p, p->dk, p->dk, p->all_xpass ? p->lmesh : nullptr, G,
+                    act, pos, st, 4);
     FPM_TRY(launch_ok());
     for (auto& r : p->runs) {
       const SimDev& S = p->sims[r.first];
@@ -1092,7 +1101,7 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
     // PGD meshes, which the reverse drift below gathers at x'
     stencil_grad(p, tape_pgd_phi(p, it), p->d_nsteps, it + 1, 0, st);
     FPM_TRY(launch_ok());
-    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
+    if (!p->all_xpass) FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
     a.pgd = p->d_pgd;
     a.pgd_stride = p->pgd_cap;
     a.pgd_disp = tape_pgd_disp(p, it);
@@ -1107,7 +1116,7 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
     stencil_grad(p, tape_phi(p, it), p->d_nsteps, it, 0, st);
     prof_mark(p, 1, st);
     FPM_TRY(launch_ok());
-    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
+    if (!p->all_xpass) FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
     prof_mark(p, 6, st);
     launch_adj_position(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     prof_mark(p, 6, st);
@@ -1120,7 +1129,7 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
     prof_mark(p, 5, st);
     FPM_TRY(launch_ok());
     FPM_TRY(force_meshes(p, st, false, it));
-    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
+    if (!p->all_xpass) FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
     prof_mark(p, 6, st);
     launch_adj_vjp(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     prof_mark(p, 6, st);
@@ -1179,6 +1188,9 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   a.pgd = nullptr;
   a.pgd_stride = 0;
   a.pgd_disp = nullptr;
+  if (p->all_xpass)  // later positions find it cleared by the x pass
+    FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, sizeof(float) * 4 * p->total_m,
+                             st));
   a.rho = p->rho;
   a.coefs = p->d_coefs;
   a.ffac = p->d_ffac;

@@ -269,20 +269,20 @@ def test_potential_tape_arguments(fpm):
     plan.close()
 
 
-def _run_adjoint(sims, d0, p0, lx0, lp0, tape):
+def _run_adjoint(sims, d0, p0, lx0, lp0, tape, nc=(16, 16, 16), flags=0):
   """Forward + reverse sweep through the C ABI for simulations
-  [(T, stages)] of 16^3 in one plan: returns dL/dX_0, dL/dp_0 and the
+  [(T, stages)] of mesh nc in one plan: returns dL/dX_0, dL/dp_0 and the
   rebuilt initial displacement and momentum."""
   from flowpm_b200 import _lib, tfbackground
   from flowpm_b200._plans import Plan
-  n = 16**3
+  n = int(np.prod(nc))
   B = len(sims)
   maxT = max(T for T, _ in sims)
   c = __import__('flowpm_b200').cosmology.Planck15()
   co = np.zeros((B, maxT, 3))
   for s, (T, stages) in enumerate(sims):
     co[s, :T] = tfbackground.nbody_coefficients(c, stages)
-  plan = Plan([(16, 16, 16, 1)] * B, flags=_lib.FPM_PLAN_ADJOINT)
+  plan = Plan([tuple(nc) + (1,)] * B, flags=_lib.FPM_PLAN_ADJOINT | flags)
   try:
     st = _lib.stream_ptr()
     _lib.call('fpm_nbody_set_steps', plan.handle, maxT,
@@ -334,3 +334,31 @@ def test_potential_tape_uneven_batch(fpm):
     assert np.abs(pp[sl] - rpp).max() < 1e-4, (s, np.abs(pp[sl] - rpp).max())
     assert np.abs(dd[sl] - host(d0[sl])).max() < 1e-3
     assert np.abs(pp[sl] - host(p0[sl])).max() < 1e-3
+
+
+@pytest.mark.parametrize('tape', [False, True], ids=['rebuilt', 'potential'])
+def test_adjoint_xpass_vs_cufft(fpm, tape):
+  """The reverse sweep on a 256 x 16 x 16 mesh, which takes the x-pass
+  Fourier solve (cuFFT plane transforms around the x-pass kernel, whose x
+  pass in the reverse sweep also clears the adjoint force mesh for the
+  next position), against the same plan on the three-dimensional cuFFT
+  path (FPM_PLAN_CUFFT, a memset per position).  Both are FP32 with the
+  same CIC conventions, so they differ by transform rounding only.  (On
+  meshes this elongated the FP32 gradient sits ~5e-3 from the FP64 oracle's
+  on either path: particles within FP32 rounding of a cell face take the
+  other side of the weight derivative.)"""
+  from flowpm_b200 import _lib
+  rng = np.random.default_rng(43)
+  nc = (256, 16, 16)
+  n = int(np.prod(nc))
+  sims = [(4, np.linspace(0.1, 1.0, 5)), (3, np.linspace(0.2, 0.8, 4))]
+  t = lambda a: torch.tensor(a, dtype=torch.float32, device='cuda')
+  d0 = t(rng.standard_normal((2 * n, 3)) * 0.3)
+  p0 = t(rng.standard_normal((2 * n, 3)) * 0.1)
+  lx0 = t(rng.standard_normal((2 * n, 3)))
+  lp0 = t(rng.standard_normal((2 * n, 3)))
+  a = _run_adjoint(sims, d0, p0, lx0, lp0, tape, nc)
+  b = _run_adjoint(sims, d0, p0, lx0, lp0, tape, nc, _lib.FPM_PLAN_CUFFT)
+  for u, v in zip(a, b):
+    assert np.isfinite(u).all()
+    assert rel_l2(u, v) < 1e-4, rel_l2(u, v)
