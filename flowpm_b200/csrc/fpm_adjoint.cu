@@ -129,7 +129,6 @@ k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       if (a.it < 0) continue;
       const float3 x = mesh_pos(S, i, j, k, d);
       if (!finite3(x.x, x.y, x.z)) atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
-      if (!a.paint) continue;
       paint8(m, S.mx, S.my, S.mz, cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
              cic_axis(x.z, S.mz));
     }

@@ -20,8 +20,6 @@ struct AdjArgs {
                           // (lmesh + 3 m_off + d mcells)
   int lvec4;
   float* rho;             // density target of the paint
-  int paint;              // 0: the reverse drift skips the paint of x_it
-                          // (force meshes from a stored potential)
   const float* pgd;       // PGD rows (alpha, kl, ks), stride pgd_stride per
   int pgd_stride;         //   sim (k_adj_pgd)
   const float* pgd_disp;  // (total_np, 3) displacement before the PGD move

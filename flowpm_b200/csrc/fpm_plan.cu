@@ -1123,7 +1123,6 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
     FPM_TRY(launch_ok());
   } else {
     FPM_CUDA(cudaMemsetAsync(p->rho, 0, sizeof(float) * p->total_m, st));
-    a.paint = 1;
     prof_mark(p, 5, st);
     launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
     prof_mark(p, 5, st);
@@ -1184,7 +1183,6 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   a.lrho = p->lrho;
   a.lmesh = p->lmesh;
   a.lvec4 = stencil_path(p) ? 1 : 0;
-  a.paint = 1;
   a.pgd = nullptr;
   a.pgd_stride = 0;
   a.pgd_disp = nullptr;
