@@ -913,7 +913,9 @@ def main():
   if world == 1 and not args.no_extras:
     line['fwd_adjoint'] = measure_fwd_adjoint(
         fpm, flush, max(args.steps, 3), tape=not args.no_potential_tape)
+    torch.cuda.nvtx.range_push('c3')  # lets a profiler select this part
     line['batched'] = measure_batched(fpm, flush, max(args.steps, 3))
+    torch.cuda.nvtx.range_pop()
   if world == 1 and (args.c5 or not (args.no_extras or args.no_c5)):
     torch.cuda.nvtx.range_push('c5')  # lets a profiler select this part
     try:

@@ -85,6 +85,11 @@ struct fpm_plan {
   int64_t tape_floats = 0;
   bool quads = false;       // every mesh: mz % 4 == 0 and m_off % 4 == 0
   bool div_tiled = false;   // every run takes the tiled divergence stencil
+  // side streams for the fused-solve runs after the first (created with
+  // the plan), and the events that fork them off and join them back
+  std::vector<cudaStream_t> side;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
   bool all_xpass = false;   // every run on the x-pass path: its x pass in
                             // the reverse sweep zeroes the adjoint force
                             // mesh after the divergence has read it
@@ -178,6 +183,9 @@ void destroy_handles(fpm_plan* p) {
 
 void free_all(fpm_plan* p) {
   destroy_handles(p);
+  for (cudaStream_t s : p->side) cudaStreamDestroy(s);
+  for (cudaEvent_t e : p->ev_join) cudaEventDestroy(e);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   for (int k = 0; k < kProfKinds; ++k)
     for (cudaEvent_t e : p->ev[k]) cudaEventDestroy(e);
   void* bufs[] = {p->d_sims, p->d_kk,   p->d_grad,  p->d_win,   p->rho,
@@ -365,7 +373,11 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1,
   // profile kind 1 brackets the whole solve, density -> force meshes
   bool any_cufft = false;
   prof_mark(p, 1, st);
-  // runs on the fused solve: a few launches each, straight to fmesh
+  // runs on the fused solve: a few launches each, straight to fmesh.  With
+  // several, the second and later go to the plan's side streams, so that
+  // the latency-bound kernels of the small runs overlap the large run's
+  // (the runs touch disjoint parts of every buffer)
+  int forked = 0;
   for (auto& r : p->runs) {
     if (!r.fused) {
       any_cufft = true;
@@ -374,9 +386,25 @@ int force_meshes(fpm_plan* p, cudaStream_t st, bool zero_rho, int it = -1,
     const SimDev& S = p->sims[r.first];
     const int n = run_active(r, it);
     if (n == 0) continue;
+    cudaStream_t rs = st;
+    if (forked > 0 || !p->side.empty()) {
+      if (forked == 0) {
+        rs = st;  // the first active run stays on the call's stream
+        FPM_CUDA(cudaEventRecord(p->ev_fork, st));
+      } else {
+        rs = p->side[(forked - 1) % p->side.size()];
+        if (forked - 1 < (int)p->side.size())
+          FPM_CUDA(cudaStreamWaitEvent(rs, p->ev_fork, 0));
+      }
+    }
     launch_fft_force(p->d_sims, r.first, n, S.mx, S.my, S.mz, p->rho,
                      zero_rho ? 1 : 0, p->dk, p->fk, p->fmesh, phi,
-                     tabs_of(p), G, !stencil_path(p), st);
+                     tabs_of(p), G, !stencil_path(p), rs);
+    ++forked;
+  }
+  for (int k = 0; k + 1 < forked && k < (int)p->side.size(); ++k) {
+    FPM_CUDA(cudaEventRecord(p->ev_join[k], p->side[k]));
+    FPM_CUDA(cudaStreamWaitEvent(st, p->ev_join[k], 0));
   }
   FPM_TRY(launch_ok());
   if (!any_cufft) {
@@ -708,6 +736,37 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
   p->all_xpass = !p->runs.empty();
   for (auto& r : p->runs)
     if (!r.xpass) p->all_xpass = false;
+  {  // side streams for the fused runs after the first (at most three)
+    int nf = 0;
+    for (auto& r : p->runs) nf += r.fused ? 1 : 0;
+    const int ns = nf > 4 ? 3 : nf - 1;
+    bool sok = true;
+    if (ns > 0) sok = cudaEventCreateWithFlags(&p->ev_fork,
+                                               cudaEventDisableTiming) ==
+                      cudaSuccess;
+    for (int k = 0; sok && k < ns; ++k) {
+      cudaStream_t sk = nullptr;
+      cudaEvent_t ek = nullptr;
+      if (cudaStreamCreateWithFlags(&sk, cudaStreamNonBlocking) !=
+          cudaSuccess) {
+        sok = false;
+        break;
+      }
+      p->side.push_back(sk);
+      if (cudaEventCreateWithFlags(&ek, cudaEventDisableTiming) !=
+          cudaSuccess) {
+        sok = false;
+        break;
+      }
+      p->ev_join.push_back(ek);
+    }
+    if (!sok) {
+      cudaGetLastError();
+      free_all(p);
+      delete p;
+      return FPM_ERR_CUDA;
+    }
+  }
   for (auto& r : p->runs) {
     const SimDev& S = p->sims[r.first];
     if (rc == FPM_OK)
