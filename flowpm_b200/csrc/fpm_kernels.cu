@@ -37,10 +37,10 @@ k_paint_lattice(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 }
 
 __global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
-k_step(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
-       StepArgs a) {
+k_step(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
+       int64_t nchunks, StepArgs a) {
   pdl_wait();  // the force meshes of the solve before
-  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+  for (int64_t ch = ch0 + blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const int s = find_sim(sims, nsims, ch, kTraverse);
     const SimDev S = sims[s];
     const int T = a.nsteps[s];
@@ -986,11 +986,11 @@ void launch_stencil_grad_tiled(const SimDev* sims, int first, int count,
                                                    nsteps, pos);
 }
 
-void launch_step(const SimDev* sims, int nsims, int64_t nchunks,
+void launch_step(const SimDev* sims, int nsims, int64_t ch0, int64_t ch1,
                  const StepArgs& a, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  launch_pdl(k_step, dim3(grid_for(nchunks)), dim3(kThreads), 0, st, sims,
-             nsims, nchunks, a);
+  launch_pdl(k_step, dim3(grid_for(ch1 - ch0)), dim3(kThreads), 0, st, sims,
+             nsims, ch0, ch1, a);
 }
 
 void launch_pgd(const SimDev* sims, int nsims, int64_t nchunks, float* disp,

@@ -118,8 +118,9 @@ void launch_fft_xpass(const SimDev* sims, int first, int n, int nx, int ny,
                       int zmul, AxisTabs tabs, const Green& G,
                       const int32_t* nsteps, int pos, cudaStream_t st);
 
-// Fused readout + kick(end) + kick(start) + drift + paint of one iteration.
-void launch_step(const SimDev* sims, int nsims, int64_t nchunks,
+// Fused readout + kick(end) + kick(start) + drift + paint of one iteration,
+// over the traversal chunks [ch0, ch1) (whole simulations).
+void launch_step(const SimDev* sims, int nsims, int64_t ch0, int64_t ch1,
                  const StepArgs& a, cudaStream_t st);
 
 // PGD correction of one step: d += alpha * readout(PGD meshes) / bf, then

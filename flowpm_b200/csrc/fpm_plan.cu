@@ -951,6 +951,54 @@ extern "C" int fpm_nbody_set_steps(fpm_plan* p, int max_steps,
   return FPM_OK;
 }
 
+// Several runs, all on the fused solve, no PGD, no profiling: the runs'
+// simulations are independent, so each run integrates as its own chain
+// (solve, step, solve, ...) on its own stream -- the call's stream for the
+// first run, the side streams for the others, forked and joined by events
+// (parallel branches when captured).  The small runs' latency-bound
+// kernels then overlap the large run's throughout the leapfrog.
+bool chains_ok(const fpm_plan* p) {
+  if (p->runs.size() < 2 || p->pgd_on || p->profile ||
+      p->side.size() + 1 < p->runs.size())
+    return false;
+  for (const auto& r : p->runs)
+    if (!r.fused) return false;
+  return true;
+}
+
+int64_t run_chunk(const fpm_plan* p, size_t k) {
+  if (k >= p->runs.size()) return traverse_chunks(p);
+  const SimDev& S = p->sims[p->runs[k].first];
+  return FPM_STEP_BLOCKED ? S.ch_b : S.ch_p;
+}
+
+int nbody_chains(fpm_plan* p, StepArgs a, cudaStream_t st) {
+  const Green G = plan_green(p);
+  FPM_CUDA(cudaEventRecord(p->ev_fork, st));
+  for (size_t k = 0; k < p->runs.size(); ++k) {
+    Run& r = p->runs[k];
+    const SimDev& S = p->sims[r.first];
+    cudaStream_t rs = k == 0 ? st : p->side[k - 1];
+    if (k > 0) FPM_CUDA(cudaStreamWaitEvent(rs, p->ev_fork, 0));
+    const int64_t c0 = run_chunk(p, k), c1 = run_chunk(p, k + 1);
+    for (int it = 0; it <= p->max_steps; ++it) {
+      const int n = run_active(r, it);
+      if (n == 0) continue;  // every simulation of the run has finished
+      launch_fft_force(p->d_sims, r.first, n, S.mx, S.my, S.mz, p->rho,
+                       it < p->max_steps ? 1 : 0, p->dk, p->fk, p->fmesh,
+                       p->tape ? tape_phi(p, it) : p->phi, tabs_of(p), G,
+                       !stencil_path(p), rs);
+      a.it = it;
+      launch_step(p->d_sims, p->nsims, c0, c1, a, rs);
+    }
+    if (k > 0) {
+      FPM_CUDA(cudaEventRecord(p->ev_join[k - 1], rs));
+      FPM_CUDA(cudaStreamWaitEvent(st, p->ev_join[k - 1], 0));
+    }
+  }
+  return launch_ok();
+}
+
 extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
                              float* force, float* inter, unsigned flags,
                              float* ckpt, int ckpt_every, void* stream) {
@@ -981,12 +1029,13 @@ extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
   prof_mark(p, 2, st);
   FPM_TRY(launch_ok());
   if (p->tape && p->tape_floats < tape_needed(p)) return FPM_ERR_ARG;
+  if (chains_ok(p)) return nbody_chains(p, a, st);
   for (int it = 0; it <= p->max_steps; ++it) {
     FPM_TRY(force_meshes(p, st, it < p->max_steps, it,
                          p->tape ? tape_phi(p, it) : nullptr));
     a.it = it;
     prof_mark(p, 0, st);
-    launch_step(p->d_sims, p->nsims, traverse_chunks(p), a, st);
+    launch_step(p->d_sims, p->nsims, 0, traverse_chunks(p), a, st);
     prof_mark(p, 0, st);
     FPM_TRY(launch_ok());
     if (p->pgd_on && it < p->max_steps) {  // after the drift of step it
