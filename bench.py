@@ -49,8 +49,8 @@ WORKLOAD = ('C2: forward PM, 128^3 particles / 128^3 mesh, box 200 Mpc/h, '
 STEP_BYTES_PER_PART = 124
 KERNEL_BYTES_PER_PART = 64
 # DRAM bytes (read + write) of one k_step launch at 128^3, from one ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum = 84.2 + 8.7 MB).
-KSTEP_TRAFFIC_BYTES_128 = 92.9e6
+# capture (dram__bytes_read.sum + dram__bytes_write.sum = 84.1 + 8.3 MB).
+KSTEP_TRAFFIC_BYTES_128 = 92.4e6
 L2_FLUSH_BYTES = 256 << 20
 
 
