@@ -245,6 +245,8 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 // barrier) nor an interleaved force mesh (one float4 (f_x, f_y, f_z, 0) per
 // cell, 8 gathers per readout instead of 24) moved k_step by more than 1-3 %
 // at 128^3 and 256^3: it is not latency-bound and not bound by its gathers.
+// A z-adjacent pair as one 8-byte red.global.add.v2.f32 where aligned (half
+// the pairs) was 1-2 % slower than two scalar reductions.
 #ifndef FPM_STEP_MINBLOCKS
 #define FPM_STEP_MINBLOCKS 4   // resident blocks of 256 threads per SM
 #endif
