@@ -250,33 +250,6 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 #ifndef FPM_STEP_MINBLOCKS
 #define FPM_STEP_MINBLOCKS 4   // resident blocks of 256 threads per SM
 #endif
-#ifndef FPM_PAINT_VEC
-#define FPM_PAINT_VEC 0        // z-adjacent neighbour pairs as one v4 add
-#endif
-
-// m[e] += a, m[e + 1] += b as one 16-byte vector reduction when both lie
-// in the same aligned float4 and that float4 lies inside m[0, n) (three
-// quarters of the pairs), else as two scalar reductions.
-__device__ __forceinline__ void red_add_pair(float* m, int64_t n, int64_t e,
-                                             float a, float b) {
-#if FPM_PAINT_VEC
-  const int lane = (int)(((uintptr_t)(m + e) >> 2) & 3);
-  if (lane != 3 && e >= lane && e - lane + 4 <= n) {
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (lane == 0) { v.x = a; v.y = b; }
-    else if (lane == 1) { v.y = a; v.z = b; }
-    else { v.z = a; v.w = b; }
-    float* base = m + e - lane;
-    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(base),
-                 "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
-                 : "memory");
-    return;
-  }
-#endif
-  red_add(m + e, a);
-  red_add(m + e + 1, b);
-}
-
 // Programmatic dependent launch (sm_90 and later).  A kernel launched by
 // launch_pdl may be scheduled as soon as its predecessor in the stream
 // completes, without the launch gap; pdl_wait() (first statement of such
@@ -425,13 +398,6 @@ __device__ __forceinline__ float3 readout_cic8(const float* __restrict__ f0,
     r2 = __fadd_rn(r2, __fmul_rn(__ldg(f2 + o1), w1));
   }
   return make_float3(r0, r1, r2);
-}
-
-__device__ __forceinline__ float3 readout3(const float* __restrict__ f0,
-                                           int64_t mcells, int my, int mz,
-                                           const Axis& ax, const Axis& ay,
-                                           const Axis& az) {
-  return readout_cic8(f0, mcells, cic8(ax, ay, az, my, mz));
 }
 
 __device__ __forceinline__ float3 ld3(const float* p, int64_t g) {
