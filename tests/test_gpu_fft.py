@@ -36,6 +36,8 @@ SHAPES = [
     # mesh) and cuFFT runs in one plan
     [(256, 256, 256, 1)],
     [(512, 16, 16, 1)],
+    # x pass on rectangular planes (512 x 256 and 256 x 512 cells)
+    [(256, 512, 256, 1), (256, 256, 512, 1)],
     [(32, 32, 32, 1), (256, 16, 32, 1), (256, 16, 32, 1), (24, 24, 24, 1),
      (128, 24, 8, 2)],
     # three 128^3: the cuFFT plan takes the tiled gradient stencil (enough
