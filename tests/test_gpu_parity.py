@@ -247,6 +247,26 @@ def test_nbody_status_nonfinite(fpm):
   assert torch.isfinite(st).all()
 
 
+def test_plan_out_of_memory(fpm):
+  """A plan far larger than the device (400 meshes of 512^3, 215 GB of
+  density alone) fails in fpm_plan_create with a resource error
+  (FPM_ERR_OOM, or FPM_ERR_CUFFT should cuFFT refuse the batch first),
+  having freed what it allocated; the device and a normal plan work
+  afterwards."""
+  from flowpm_b200 import _lib
+  from flowpm_b200._plans import Plan
+  free0 = torch.cuda.mem_get_info()[0]
+  with pytest.raises(_lib.FlowPMError) as e:
+    Plan([(512, 512, 512, 1)] * 400)
+  print('oversized plan:', e.value)
+  assert e.value.code in (3, 5), e.value  # FPM_ERR_OOM, FPM_ERR_CUFFT
+  torch.cuda.synchronize()
+  assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
+  l = golden('lpt')
+  st = fpm.nbody(fpm.cosmology.Planck15(), l['n16_init_o1'], [0.1, 0.2], 16)
+  assert torch.isfinite(st).all()
+
+
 def test_batched_uneven_plan(fpm):
   """Simulations of different sizes, cosmologies and step counts advanced
   by one plan match the same simulations run one at a time."""
