@@ -93,7 +93,7 @@ k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
            : nullptr;
     const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
-    for (int item = 0; item < kItems; ++item) {
+    for (int item = 0; item < S.wi; ++item) {
       int i, j, k;
       int64_t local;
       if (!walk_particle(S, w, item, i, j, k, local)) continue;
@@ -167,7 +167,7 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
            : nullptr;
     const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
-    for (int item = 0; item < kItems; ++item) {
+    for (int item = 0; item < S.wi; ++item) {
       int i, j, k;
       int64_t local;
       if (!walk_particle(S, w, item, i, j, k, local)) continue;
@@ -271,7 +271,7 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float* ckp = ck ? ckd + a.total_np * 3 : nullptr;
     const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
-    for (int item = 0; item < kItems; ++item) {
+    for (int item = 0; item < S.wi; ++item) {
       int i, j, k;
       int64_t local;
       if (!walk_particle(S, w, item, i, j, k, local)) continue;
@@ -391,7 +391,7 @@ k_adj_pgd(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const unsigned my = S.my, mz = S.mz;
     const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
-    for (int item = 0; item < kItems; ++item) {
+    for (int item = 0; item < S.wi; ++item) {
       int i, j, k;
       int64_t local;
       if (!walk_particle(S, w, item, i, j, k, local)) continue;

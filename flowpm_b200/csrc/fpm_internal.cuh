@@ -13,9 +13,12 @@ constexpr int kItems = 4;        // particles (or cells) per thread per chunk
 constexpr int kChunk = kThreads * kItems;
 constexpr int kNumSMs = 148;     // B200
 
+// Lattice blocks of the particle kernels: (2 wi) x kBJ x kBK particles,
+// z fastest, wi (SimDev::wi) particles per thread, chosen per simulation.
+constexpr int kBJ = 8, kBK = 16;
+static_assert(2 * kBJ * kBK == kThreads, "two x planes per pass of a block");
+
 // One simulation of a plan, as the device kernels see it.
-// Lattice blocks: kBI x kBJ x kBK = kChunk particles, z fastest.
-constexpr int kBI = 8, kBJ = 8, kBK = 16;
 
 struct SimDev {
   int nx, ny, nz;        // particle lattice (= linear-field mesh)
@@ -38,6 +41,8 @@ struct SimDev {
   int64_t ch_ls;         // first lattice-spectrum chunk
   int64_t ch_b;          // first lattice-block chunk
   int nbi, nbj, nbk;     // lattice blocks per axis
+  int wi;                // particles per thread of a lattice block, whose
+                         // x extent is 2 wi
   int xpass;             // cuFFT plane transforms + the x-pass kernel
 };
 
@@ -230,7 +235,7 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 
 // Tuning knobs of the particle kernels (compile-time).
 #ifndef FPM_STEP_BLOCKED
-#define FPM_STEP_BLOCKED 1  // k_step walks 8x8x16 lattice blocks
+#define FPM_STEP_BLOCKED 1  // k_step walks kBI x 8 x 16 lattice blocks
 #endif
 // Measured on B200, k_step per leapfrog step at 128^3 / 256^3: 3 blocks
 // (80 registers) 87.4 / 621 us, 4 blocks (64) 84.6 / 594, 5 blocks (48)
@@ -449,7 +454,7 @@ __device__ __forceinline__ Walk walk_chunk(const SimDev& S, int64_t rel) {
   const unsigned b = (unsigned)rel;
   const unsigned r = b / (unsigned)S.nbk;
   const unsigned bi = r / (unsigned)S.nbj;
-  w.i0 = (int)bi * kBI;
+  w.i0 = (int)bi * 2 * S.wi;
   w.j0 = (int)(r - bi * (unsigned)S.nbj) * kBJ;
   w.k0 = (int)(b - r * (unsigned)S.nbk) * kBK;
   w.base = 0;

@@ -22,8 +22,8 @@ k_paint_lattice(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const SimDev S = sims[find_sim(sims, nsims, ch, kTraverse)];
     const Walk w = walk_chunk(S, ch - traverse_first(S));
     float* m = rho + S.m_off;
-#pragma unroll
-    for (int it = 0; it < kItems; ++it) {
+#pragma unroll 4
+    for (int it = 0; it < S.wi; ++it) {
       int i, j, k;
       int64_t local;
       if (!walk_particle(S, w, it, i, j, k, local)) continue;
@@ -56,7 +56,7 @@ k_step(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
     float* m = a.rho + S.m_off;
     const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
-    for (int it = 0; it < kItems; ++it) {
+    for (int it = 0; it < S.wi; ++it) {
       int i, j, k;
       int64_t local;
       // missing particles of edge blocks skip their memory accesses
@@ -139,7 +139,7 @@ k_pgd(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     float* m = rho + S.m_off;
     const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
-    for (int it = 0; it < kItems; ++it) {
+    for (int it = 0; it < S.wi; ++it) {
       int i, j, k;
       int64_t local;
       if (!walk_particle(S, w, it, i, j, k, local)) continue;
@@ -174,7 +174,7 @@ k_force_readout(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
     const float invb = 1.0f / (float)S.bf;
     const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
     const Walk w = walk_chunk(S, ch - traverse_first(S));
-    for (int it = 0; it < kItems; ++it) {
+    for (int it = 0; it < S.wi; ++it) {
       int i, j, k;
       int64_t local;
       if (!walk_particle(S, w, it, i, j, k, local)) continue;
