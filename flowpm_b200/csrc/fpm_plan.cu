@@ -30,6 +30,12 @@ namespace {
 // stencil, 8 adjoint potential solve, 9 the whole reverse step
 constexpr int kProfKinds = 10;
 
+// Particles per thread of the lattice blocks of lattices of 2^26 particles
+// or more (x extent twice that).
+#ifndef FPM_WALK_LARGE
+#define FPM_WALK_LARGE 32
+#endif
+
 struct Run {
   int first, count;        // simulations [first, first + count)
   bool fused = false;      // force meshes by the fused Fourier solve
@@ -654,12 +660,14 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
     S.ch_m = p->ch_m;
     S.ch_l = p->ch_l;
     S.ch_ls = p->ch_ls;
-    // larger lattice blocks for large lattices: measured per simulation of
-    // 2 x 512^3, k_step 9.14 / 8.90 / 8.73 ms and the reverse position
-    // 18.1 / 17.5 / 17.3 ms at wi = 4 / 8 / 16; at 128^3 wi = 4 is best
-    // (k_step 85 / 87 / 97 us), the other sizes leaving too few blocks
+    // larger lattice blocks for large lattices: the items of a thread walk
+    // along x, each reusing in L1 the cells of the previous one.  Measured
+    // at 2 x 512^3: k_step 9.14 / 8.90 / 8.73 / 8.70 ms and the reverse
+    // position 18.1 / 17.5 / 17.3 / 17.1 ms at wi = 4 / 8 / 16 / 32; at
+    // 128^3 wi = 4 is best (k_step 85 / 87 / 97 us at 4 / 8 / 16), larger
+    // blocks leaving too few of them for the SMs
     S.wi = !FPM_STEP_BLOCKED ? kItems
-           : S.np >= ((int64_t)1 << 26) ? 16
+           : S.np >= ((int64_t)1 << 26) ? FPM_WALK_LARGE
            : S.np >= ((int64_t)1 << 23) ? 8 : 4;
     S.nbi = (S.nx + 2 * S.wi - 1) / (2 * S.wi);
     S.nbj = (S.ny + kBJ - 1) / kBJ;
