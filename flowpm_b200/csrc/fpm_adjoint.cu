@@ -140,7 +140,7 @@ k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 // cotangent v = (ks_it + ke_{it-1}) lam_p (+ lam_F at the last position):
 //   lam_x += fac * sum_c grad W * (v . f[c])            (readout weights)
 //   lam_f[c] += (fac / B) * v * W                       (scatter)
-__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
+__global__ void __launch_bounds__(kThreads, FPM_ADJ_MINBLOCKS)
 k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
           AdjArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -241,7 +241,7 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 // p_it - ke_{it-1} F_it, formed here with the same two roundings, instead
 // of p_it and F_it in two buffers; the last position (it = 0) leaves p_0.
 // The force buffer is not used.
-__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
+__global__ void __launch_bounds__(kThreads, FPM_ADJ_MINBLOCKS)
 k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                AdjArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -372,7 +372,7 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 //            + the paint adjoint of the mesh part, which starts here as the
 //   scatter lf[c] += (alpha / B) lam W(x' - c)  (then divergence, PGD
 //   filter, gather at x' by the next kernel).  x' comes from the tape.
-__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
+__global__ void __launch_bounds__(kThreads, FPM_ADJ_MINBLOCKS)
 k_adj_pgd(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
           AdjArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {

@@ -255,6 +255,16 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 #ifndef FPM_STEP_MINBLOCKS
 #define FPM_STEP_MINBLOCKS 4   // resident blocks of 256 threads per SM
 #endif
+// Resident blocks of the reverse-sweep kernels that gather forces and
+// scatter their VJP (k_adj_position, k_adj_vjp, k_adj_pgd), which carry
+// more state per particle.  Measured on B200 at 2 x 512^3: k_adj_position
+// 15.9 ms with 3 blocks (78 registers), 17.3 ms with 4 (64 registers),
+// 21.6 ms with 5 (48, spills); k_adj_vjp 14.3 against 14.9 ms with 4.
+// k_adj_drift_paint, a drift and paint like k_step, keeps 4 (10.8 against
+// 11.1 ms with 3).
+#ifndef FPM_ADJ_MINBLOCKS
+#define FPM_ADJ_MINBLOCKS 3
+#endif
 // Programmatic dependent launch (sm_90 and later).  A kernel launched by
 // launch_pdl may be scheduled as soon as its predecessor in the stream
 // completes, without the launch gap; pdl_wait() (first statement of such
@@ -432,7 +442,7 @@ __device__ __forceinline__ void mode_ijl(int64_t local, int ny, int nzh,
 
 // Chunk kind and particle enumeration of the particle kernels that gather
 // from or scatter to the meshes (lattice blocks when FPM_STEP_BLOCKED, else
-// 1024 consecutive particles).
+// kChunk consecutive particles).
 constexpr int kTraverse = FPM_STEP_BLOCKED ? kBlock : kPart;
 
 __device__ __forceinline__ int64_t traverse_first(const SimDev& S) {
