@@ -13,10 +13,18 @@ constexpr int kItems = 4;        // particles (or cells) per thread per chunk
 constexpr int kChunk = kThreads * kItems;
 constexpr int kNumSMs = 148;     // B200
 
-// Lattice blocks of the particle kernels: (2 wi) x kBJ x kBK particles,
-// z fastest, wi (SimDev::wi) particles per thread, chosen per simulation.
-constexpr int kBJ = 8, kBK = 16;
-static_assert(2 * kBJ * kBK == kThreads, "two x planes per pass of a block");
+// Lattice blocks of the particle kernels: (kPlanes wi) x kBJ x kBK
+// particles, z fastest, wi (SimDev::wi) particles per thread, chosen per
+// simulation; one pass of the block's threads covers kPlanes x planes.
+// Measured on B200 with kBJ = 4 / 8 / 16 at equal particles per block:
+// k_step at 2 x 512^3 8.92 / 8.70 / 8.68 ms, at 128^3 88.1 / 84.7 / 84.0
+// us; k_adj_position 15.4 / 15.8 / 16.7 ms.
+#ifndef FPM_BJ
+#define FPM_BJ 8
+#endif
+constexpr int kBJ = FPM_BJ, kBK = 16;
+constexpr int kPlanes = kThreads / (kBJ * kBK);
+static_assert(kPlanes * kBJ * kBK == kThreads, "whole x planes per pass");
 
 // One simulation of a plan, as the device kernels see it.
 
@@ -42,7 +50,7 @@ struct SimDev {
   int64_t ch_b;          // first lattice-block chunk
   int nbi, nbj, nbk;     // lattice blocks per axis
   int wi;                // particles per thread of a lattice block, whose
-                         // x extent is 2 wi
+                         // x extent is kPlanes wi
   int xpass;             // cuFFT plane transforms + the x-pass kernel
 };
 
@@ -464,7 +472,7 @@ __device__ __forceinline__ Walk walk_chunk(const SimDev& S, int64_t rel) {
   const unsigned b = (unsigned)rel;
   const unsigned r = b / (unsigned)S.nbk;
   const unsigned bi = r / (unsigned)S.nbj;
-  w.i0 = (int)bi * 2 * S.wi;
+  w.i0 = (int)bi * kPlanes * S.wi;
   w.j0 = (int)(r - bi * (unsigned)S.nbj) * kBJ;
   w.k0 = (int)(b - r * (unsigned)S.nbk) * kBK;
   w.base = 0;

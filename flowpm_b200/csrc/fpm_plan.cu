@@ -669,7 +669,7 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
     S.wi = !FPM_STEP_BLOCKED ? kItems
            : S.np >= ((int64_t)1 << 26) ? FPM_WALK_LARGE
            : S.np >= ((int64_t)1 << 23) ? 8 : 4;
-    S.nbi = (S.nx + 2 * S.wi - 1) / (2 * S.wi);
+    S.nbi = (S.nx + kPlanes * S.wi - 1) / (kPlanes * S.wi);
     S.nbj = (S.ny + kBJ - 1) / kBJ;
     S.nbk = (S.nz + kBK - 1) / kBK;
     S.ch_b = p->ch_b;
