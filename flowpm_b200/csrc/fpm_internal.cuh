@@ -243,7 +243,7 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 
 // Tuning knobs of the particle kernels (compile-time).
 #ifndef FPM_STEP_BLOCKED
-#define FPM_STEP_BLOCKED 1  // k_step walks kBI x 8 x 16 lattice blocks
+#define FPM_STEP_BLOCKED 1  // the particle kernels walk lattice blocks
 #endif
 // Measured on B200, k_step per leapfrog step at 128^3 / 256^3: 3 blocks
 // (80 registers) 87.4 / 621 us, 4 blocks (64) 84.6 / 594, 5 blocks (48)
