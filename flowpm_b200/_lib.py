@@ -119,6 +119,7 @@ FPM_PLAN_LPT = 2
 FPM_PLAN_GRAD_ORDER0 = 4
 FPM_PLAN_ADJOINT = 8
 FPM_PLAN_CUFFT = 16
+FPM_PLAN_SMALL_BLOCKS = 32
 FPM_NBODY_INTERMEDIATE = 1
 FPM_STATUS_NONFINITE_POS = 1
 FPM_STATUS_NONFINITE_MOM = 2

@@ -667,6 +667,7 @@ extern "C" int fpm_plan_create(fpm_plan** out, int nsims, const int32_t* dims,
     // 128^3 wi = 4 is best (k_step 85 / 87 / 97 us at 4 / 8 / 16), larger
     // blocks leaving too few of them for the SMs
     S.wi = !FPM_STEP_BLOCKED ? kItems
+           : (flags & FPM_PLAN_SMALL_BLOCKS) ? 4
            : S.np >= ((int64_t)1 << 26) ? FPM_WALK_LARGE
            : S.np >= ((int64_t)1 << 23) ? 8 : 4;
     S.nbi = (S.nx + kPlanes * S.wi - 1) / (kPlanes * S.wi);

@@ -61,10 +61,15 @@ enum {
                                     4-point finite difference (order 1)   */
   FPM_PLAN_ADJOINT = 1u << 3,    /* also allocate the adjoint buffers and
                                     cuFFT plans (fpm_nbody_adjoint)         */
-  FPM_PLAN_CUFFT = 1u << 4       /* force meshes through cuFFT for every
+  FPM_PLAN_CUFFT = 1u << 4,      /* force meshes through cuFFT for every
                                     mesh shape; by default meshes of 16 to
                                     128 cells (powers of two) per axis use
                                     the library's fused Fourier solve       */
+  FPM_PLAN_SMALL_BLOCKS = 1u << 5 /* the particle kernels walk every lattice
+                                    in blocks of 8x8x16 particles; by
+                                    default lattices of 2^23 particles or
+                                    more take 16x8x16 blocks, and of 2^26 or
+                                    more 64x8x16 (faster there)             */
 };
 
 /* nbody flags (fpm_nbody). */

@@ -366,3 +366,46 @@ def test_adjoint_xpass_vs_cufft(fpm, tape):
   for u, v in zip(a, b):
     assert np.isfinite(u).all()
     assert rel_l2(u, v) < tol, rel_l2(u, v)
+
+
+@pytest.mark.parametrize('nc', [(256, 256, 256), (512, 256, 512)],
+                         ids=['256^3', '512x256x512'])
+def test_lattice_walk_sizes_agree(fpm, nc, capsys):
+  """The particle kernels walk large lattices in long blocks (16x8x16
+  particles from 2^23 particles, 64x8x16 from 2^26); FPM_PLAN_SMALL_BLOCKS
+  keeps 8x8x16. Both walks must visit every particle once: the forward
+  state of a random field (3 steps) and the adjoint of a zero field (each
+  scatter and gather then has one non-zero term) agree to FP32 rounding."""
+  from flowpm_b200 import _lib
+  rng = np.random.default_rng(53)
+  n = int(np.prod(nc))
+  sims = [(3, np.linspace(0.1, 0.5, 4))]
+  d0 = torch.tensor(rng.uniform(-1.0, 1.0, (n, 3)).astype(np.float32),
+                    device='cuda')
+  p0 = torch.tensor(rng.uniform(-0.1, 0.1, (n, 3)).astype(np.float32),
+                    device='cuda')
+  lx0 = torch.tensor(rng.standard_normal((n, 3)).astype(np.float32),
+                     device='cuda')
+  lp0 = torch.tensor(rng.standard_normal((n, 3)).astype(np.float32),
+                     device='cuda')
+  z = torch.zeros_like(d0)
+  errs = []
+  for dd, pp in ((d0, p0), (z, z)):
+    a = _run_adjoint(sims, dd, pp, lx0, lp0, True, nc)
+    b = _run_adjoint(sims, dd, pp, lx0, lp0, True, nc,
+                     _lib.FPM_PLAN_SMALL_BLOCKS)
+    for x, y in zip(a, b):
+      assert np.isfinite(x).all()
+    # relative L2 for the cotangents and the random-field state; the
+    # zero-field state is rounding noise around 0: max absolute difference
+    errs.append([rel_l2(a[0], b[0]), rel_l2(a[1], b[1])] +
+                ([rel_l2(a[k], b[k]) for k in (2, 3)] if dd is d0 else
+                 [float(np.abs(a[k] - b[k]).max()) for k in (2, 3)]))
+  with capsys.disabled():
+    print('\n  walk sizes at %s: random field (lx, lp, d, p) %s; zero field '
+          '%s' % ('x'.join(map(str, nc)),
+                  ' '.join('%.1e' % e for e in errs[0]),
+                  ' '.join('%.1e' % e for e in errs[1])))
+  assert max(errs[0][2:]) < 1e-5, errs[0]   # rebuilt state, random field
+  assert max(errs[1][:2]) < 1e-5, errs[1]   # cotangents, zero field
+  assert max(errs[1][2:]) < 1e-5, errs[1]   # rebuilt state, zero field
