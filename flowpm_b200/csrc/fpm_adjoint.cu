@@ -140,7 +140,8 @@ k_adj_drift_paint(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 // cotangent v = (ks_it + ke_{it-1}) lam_p (+ lam_F at the last position):
 //   lam_x += fac * sum_c grad W * (v . f[c])            (readout weights)
 //   lam_f[c] += (fac / B) * v * W                       (scatter)
-__global__ void __launch_bounds__(kThreads, FPM_ADJ_MINBLOCKS)
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
           AdjArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -241,7 +242,8 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
 // p_it - ke_{it-1} F_it, formed here with the same two roundings, instead
 // of p_it and F_it in two buffers; the last position (it = 0) leaves p_0.
 // The force buffer is not used.
-__global__ void __launch_bounds__(kThreads, FPM_ADJ_MINBLOCKS)
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
                AdjArgs a) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -670,7 +672,12 @@ void launch_adj_drift_paint(const SimDev* sims, int nsims, int64_t nchunks,
 void launch_adj_vjp(const SimDev* sims, int nsims, int64_t nchunks,
                     const AdjArgs& a, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_adj_vjp<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
+  if (a.long_walk)
+    k_adj_vjp<FPM_ADJ_MINBLOCKS><<<grid_for(nchunks), kThreads, 0, st>>>(
+        sims, nsims, nchunks, a);
+  else
+    k_adj_vjp<FPM_STEP_MINBLOCKS><<<grid_for(nchunks), kThreads, 0, st>>>(
+        sims, nsims, nchunks, a);
 }
 
 void launch_adj_pgd(const SimDev* sims, int nsims, int64_t nchunks,
@@ -682,8 +689,12 @@ void launch_adj_pgd(const SimDev* sims, int nsims, int64_t nchunks,
 void launch_adj_position(const SimDev* sims, int nsims, int64_t nchunks,
                          const AdjArgs& a, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_adj_position<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims,
-                                                         nchunks, a);
+  if (a.long_walk)
+    k_adj_position<FPM_ADJ_MINBLOCKS><<<grid_for(nchunks), kThreads, 0, st>>>(
+        sims, nsims, nchunks, a);
+  else
+    k_adj_position<FPM_STEP_MINBLOCKS>
+        <<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
 }
 
 void launch_adj_fourier(const SimDev* sims, int nsims, int64_t nchunks,

@@ -32,6 +32,8 @@ struct AdjArgs {
   int64_t total_np;
   int max_steps;
   int it;
+  int long_walk;  // most particles walk long lattice blocks (wi >= 16): the
+                  // launchers take the FPM_ADJ_MINBLOCKS instances
 };
 
 void launch_adj_drift_paint(const SimDev* sims, int nsims, int64_t nchunks,

@@ -265,7 +265,10 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 #endif
 // Resident blocks of the reverse-sweep kernels that gather forces and
 // scatter their VJP (k_adj_position, k_adj_vjp, k_adj_pgd), which carry
-// more state per particle.  Measured on B200 at 2 x 512^3: k_adj_position
+// more state per particle, for plans whose particles mostly walk long
+// lattice blocks (the others take FPM_STEP_MINBLOCKS: at 2 x 192^3, 8x8x16
+// blocks, k_adj_position took 838 us with 3 blocks against 784 us with 4,
+// cold and serialised).  Measured on B200 at 2 x 512^3: k_adj_position
 // 15.9 ms with 3 blocks (78 registers), 17.3 ms with 4 (64 registers),
 // 21.6 ms with 5 (48, spills); k_adj_vjp 14.3 against 14.9 ms with 4.
 // k_adj_drift_paint, a drift and paint like k_step, keeps 4 (10.8 against

@@ -1322,6 +1322,12 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   a.status = p->d_status;
   a.total_np = p->total_np;
   a.max_steps = p->max_steps;
+  {
+    int64_t long_np = 0;
+    for (const SimDev& S : p->sims)
+      if (S.wi >= 16) long_np += S.np;
+    a.long_walk = 2 * long_np > p->total_np ? 1 : 0;
+  }
   for (int it = p->max_steps; it >= 0; --it) {
     a.it = it;
     prof_mark(p, 9, st);
