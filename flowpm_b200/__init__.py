@@ -13,6 +13,7 @@ from . import tfbackground
 from . import tfbackground as background
 from . import tfpower
 from . import raytracing
+from . import io
 from .utils import cic_paint, cic_readout, r2c3d, c2r3d, white_noise
 from .tfpm import nbody, linear_field, lpt_init
 from .pk import power_spectrum
