@@ -162,3 +162,23 @@ def test_save_state_gpu_lpt(cuda, tmp_path):
   back, a, _ = io.load_state(fn)
   assert back.is_cuda and a == pytest.approx(0.1)
   assert_allclose(back[:2].cpu().numpy(), s[:2], rtol=3e-7, atol=1e-5)
+
+
+def test_read_block_of_several_files(fio, tmp_path):
+  """A block split over two data files (NFILE 2, as a parallel writer
+  makes them) reads back as one array in file order."""
+  a = np.arange(12, dtype='<f8').reshape(4, 3)
+  b = -np.arange(6, dtype='<f8').reshape(2, 3)
+  path = tmp_path / 'm' / 'blk'
+  os.makedirs(path)
+  lines = ['DTYPE: <f8', 'NMEMB: 3', 'NFILE: 2']
+  for i, part in enumerate((a, b)):
+    raw = part.tobytes()
+    (path / ('%06X' % i)).write_bytes(raw)
+    s = int(np.frombuffer(raw, np.uint8).sum()) % 2**32
+    r = (s & 0xffff) + (s >> 16)
+    lines.append('%06X: %d : %d : %d' % (i, part.shape[0], s,
+                                         (r & 0xffff) + (r >> 16)))
+  (path / 'header').write_text('\n'.join(lines) + '\n')
+  assert_array_equal(fio.read_block(str(tmp_path / 'm'), 'blk'),
+                     np.concatenate([a, b]))
