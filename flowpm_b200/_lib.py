@@ -75,6 +75,9 @@ SIGNATURES = {
                                         c_void_p, c_void_p]),
     'fpm_lpt_init': (c_int, [c_void_p, c_void_p, P_double, c_int, c_void_p,
                              c_void_p, c_void_p, c_void_p]),
+    'fpm_lpt1': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p,
+                         c_void_p]),
+    'fpm_lpt2_source': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     'fpm_linear_field': (c_int, [c_void_p, c_void_p, c_uint64, c_int,
                                  c_void_p, c_void_p, c_void_p]),
     'fpm_lattice_shift': (c_int, [c_void_p, c_void_p, c_int, c_int, c_int,

@@ -696,15 +696,17 @@ k_stencil_grad_tiled(const SimDev* __restrict__ sims, int first,
 }
 
 // LPT spectra (flowpm/tfpm.py:66-145 lpt1 / lpt2_source on the lattice).
+// dk is the unnormalised R2C of the real field (normalised: already
+// r2c3d's FFT / N^3, as the reference's lpt1 and lpt2_source take it).
 __global__ void __launch_bounds__(kThreads)
 k_lpt_fourier(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
               const float2* __restrict__ dk, float2* __restrict__ out,
-              int mode, AxisTabs tabs) {
+              int mode, AxisTabs tabs, int normalised) {
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const SimDev S = sims[find_sim(sims, nsims, ch, kLatSpec)];
     const int64_t nmodes = (int64_t)S.nx * S.ny * S.lzh;
     const int64_t ncells = (int64_t)S.nx * S.ny * S.nz;
-    const float pre = (float)(1.0 / (double)ncells);
+    const float pre = normalised ? 1.f : (float)(1.0 / (double)ncells);
     const double* kkx = tabs.kk + S.ltab;
     const double* kky = kkx + S.nx;
     const double* kkz = kky + S.ny;
@@ -747,6 +749,72 @@ k_lpt_fourier(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
         }
       }
     }
+  }
+}
+
+// Full <-> half lattice spectra.  The reference's r2c3d / c2r3d
+// (flowpm/utils.py:213-272) speak full complex spectra (nx, ny, nz); the
+// library keeps the nz/2 + 1 half that a real field's Hermitian symmetry
+// determines.  to_full == 0: half[i, j, l] = s * full[i, j, l], l <= nz/2
+// (chunks over half-spectrum modes); to_full == 1: full[i, j, l] =
+// s * half[i, j, l] for l <= nz/2, else s * conj(half[-i, -j, nz - l])
+// (indices mod n; chunks over lattice cells).  s = 1/(nx ny nz) with
+// inv_n, else 1.
+__global__ void __launch_bounds__(kThreads)
+k_lat_spectrum(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
+               const float2* __restrict__ in, float2* __restrict__ out,
+               int to_full, int inv_n) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const SimDev S =
+        sims[find_sim(sims, nsims, ch, to_full ? kLat : kLatSpec)];
+    const int64_t ncells = (int64_t)S.nx * S.ny * S.nz;
+    const int64_t nmodes = (int64_t)S.nx * S.ny * S.lzh;
+    const float s = inv_n ? (float)(1.0 / (double)ncells) : 1.f;
+    const int64_t base =
+        (ch - (to_full ? S.ch_l : S.ch_ls)) * kChunk + threadIdx.x;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const int64_t local = base + it * kThreads;
+      if (local >= (to_full ? ncells : nmodes)) break;
+      if (!to_full) {
+        int i, j, l;
+        mode_ijl(local, S.ny, S.lzh, i, j, l);
+        const float2 v =
+            in[S.l_off + ((int64_t)i * S.ny + j) * S.nz + l];
+        out[S.ls_off + local] = make_float2(__fmul_rn(v.x, s), __fmul_rn(v.y, s));
+      } else {
+        int i, j, l;
+        mode_ijl(local, S.ny, S.nz, i, j, l);
+        float2 v;
+        if (l < S.lzh) {
+          v = in[S.ls_off + ((int64_t)i * S.ny + j) * S.lzh + l];
+        } else {
+          const int ci = i ? S.nx - i : 0, cj = j ? S.ny - j : 0;
+          v = in[S.ls_off + ((int64_t)ci * S.ny + cj) * S.lzh + (S.nz - l)];
+          v.y = -v.y;
+        }
+        out[S.l_off + local] = make_float2(__fmul_rn(v.x, s), __fmul_rn(v.y, s));
+      }
+    }
+  }
+}
+
+// Three lattice meshes (psi_d of sim s at psi + 3 l_off + d ncells) read
+// out at arbitrary positions: out[s, p, d] = cic_readout(psi_d, pos[s, p]),
+// flowpm/tfpm.py:86-94 (lpt1's readout at pos).  One thread per particle.
+__global__ void __launch_bounds__(kThreads)
+k_lpt_readout(const SimDev* __restrict__ sims, int nsims,
+              const float* __restrict__ psi, const float* __restrict__ pos,
+              int64_t npart, float* __restrict__ out) {
+  const int64_t total = (int64_t)nsims * npart;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const SimDev S = sims[g / npart];
+    const int64_t ncells = (int64_t)S.nx * S.ny * S.nz;
+    const float3 x = ld3(pos, g);
+    const Cic8 c = cic8(cic_axis(x.x, S.nx), cic_axis(x.y, S.ny),
+                        cic_axis(x.z, S.nz), S.ny, S.nz);
+    st3(out, g, readout_cic8(psi + 3 * S.l_off, ncells, c));
   }
 }
 
@@ -1013,14 +1081,35 @@ void launch_force_readout(const SimDev* sims, int nsims, int64_t nchunks,
 
 void launch_lpt_fourier(const SimDev* sims, int nsims, int64_t nchunks,
                         const float2* dk, float2* out, int mode, AxisTabs tabs,
+                        cudaStream_t st, int normalised) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_lpt_fourier<<<grid_for(nchunks), kThreads, 0, st>>>(
+      sims, nsims, nchunks, dk, out, mode, tabs, normalised);
+}
+
+void launch_lat_spectrum(const SimDev* sims, int nsims, int64_t nchunks,
+                         const float2* in, float2* out, int to_full,
+                         int inv_n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_lat_spectrum<<<grid_for(nchunks), kThreads, 0, st>>>(
+      sims, nsims, nchunks, in, out, to_full, inv_n);
+}
+
+void launch_lpt_readout(const SimDev* sims, int nsims, const float* psi,
+                        const float* pos, int64_t npart, float* out,
                         cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_lpt_fourier<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks,
-                                                        dk, out, mode, tabs);
+  int64_t blocks = ((int64_t)nsims * npart + kThreads - 1) / kThreads;
+  const int64_t cap = (int64_t)kNumSMs * 32;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  k_lpt_readout<<<(unsigned)blocks, kThreads, 0, st>>>(sims, nsims, psi, pos,
+                                                       npart, out);
 }
 
 void launch_lpt2_source(const SimDev* sims, int nsims, int64_t nchunks,
                         const float* phi9, float* source, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   k_lpt2_source<<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks,
                                                         phi9, source);
 }

@@ -138,9 +138,23 @@ void launch_force_readout(const SimDev* sims, int nsims, int64_t nchunks,
 // Lattice spectra for LPT.  mode 0: from delta_L write 9 spectra
 // {psi1_x, psi1_y, psi1_z, phi_00, phi_11, phi_22, phi_12, phi_20, phi_01};
 // mode 1: write the 3 spectra psi_d.  Input is the unnormalised R2C output,
-// scaled by 1 / (nx ny nz).
+// scaled by 1 / (nx ny nz), or, with normalised, already scaled.
 void launch_lpt_fourier(const SimDev* sims, int nsims, int64_t nchunks,
                         const float2* dk, float2* out, int mode, AxisTabs tabs,
+                        cudaStream_t st, int normalised = 0);
+
+// Lattice spectra, full (nx, ny, nz) <-> half (nx, ny, nz/2 + 1):
+// to_full = 0 keeps l <= nz/2 (nchunks = lattice-spectrum chunks),
+// to_full = 1 fills l > nz/2 by Hermitian symmetry (nchunks = lattice
+// chunks); both scaled by 1 / (nx ny nz) when inv_n.
+void launch_lat_spectrum(const SimDev* sims, int nsims, int64_t nchunks,
+                         const float2* in, float2* out, int to_full,
+                         int inv_n, cudaStream_t st);
+
+// out[s, p] = CIC readout of the three lattice meshes psi + 3 l_off + d Nc
+// at pos[s, p] (npart particles per simulation).
+void launch_lpt_readout(const SimDev* sims, int nsims, const float* psi,
+                        const float* pos, int64_t npart, float* out,
                         cudaStream_t st);
 
 // 2LPT source 3/7 * sum(phi_ii phi_jj - phi_ij^2) on the lattice meshes.

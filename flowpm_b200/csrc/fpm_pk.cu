@@ -50,16 +50,22 @@ __device__ __forceinline__ double pk_w(int l, int nz) {
 
 // Accumulates, for every batch entry b, psum[b][bin] += w |F|^2 and
 // nsum[b][bin] += w into scratch (2 * batch * (nedges + 1) doubles,
-// zeroed by the caller); per-block shared-memory histograms first.
+// zeroed by the caller).  With shared, per-block shared-memory histograms
+// first (2 (nedges + 1) doubles of dynamic shared memory); without (bin
+// counts whose histogram does not fit), straight into scratch.
 __global__ void __launch_bounds__(256)
 k_pk_accumulate(const float2* __restrict__ dk, int batch, PkGeom g,
-                double* __restrict__ scratch) {
-  extern __shared__ double sh[];
+                double* __restrict__ scratch, int shared) {
+  extern __shared__ double sh_[];
   const int nb = g.nedges + 1;
   const int64_t nmodes = (int64_t)g.nx * g.ny * g.nzh;
   for (int b = 0; b < batch; ++b) {
-    for (int t = threadIdx.x; t < 2 * nb; t += blockDim.x) sh[t] = 0.0;
-    __syncthreads();
+    double* out = scratch + (int64_t)b * 2 * nb;
+    double* sh = shared ? sh_ : out;
+    if (shared) {
+      for (int t = threadIdx.x; t < 2 * nb; t += blockDim.x) sh[t] = 0.0;
+      __syncthreads();
+    }
     const float2* f = dk + (int64_t)b * nmodes;
     for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
          m < nmodes; m += (int64_t)gridDim.x * blockDim.x) {
@@ -77,11 +83,12 @@ k_pk_accumulate(const float2* __restrict__ dk, int batch, PkGeom g,
       atomicAdd(&sh[bin], w * p2);
       atomicAdd(&sh[nb + bin], w);
     }
-    __syncthreads();
-    double* out = scratch + (int64_t)b * 2 * nb;
-    for (int t = threadIdx.x; t < 2 * nb; t += blockDim.x)
-      if (sh[t] != 0.0) atomicAdd(&out[t], sh[t]);
-    __syncthreads();
+    if (shared) {
+      __syncthreads();
+      for (int t = threadIdx.x; t < 2 * nb; t += blockDim.x)
+        if (sh[t] != 0.0) atomicAdd(&out[t], sh[t]);
+      __syncthreads();
+    }
   }
 }
 
@@ -131,15 +138,17 @@ PkGeom pk_geom(int nx, int ny, int nz, const double* boxsize, double kmin,
 int pk_launch(const float2* dk, int batch, const PkGeom& g, double* scratch,
               double vol, float* power, cudaStream_t st) {
   const int nb = g.nedges + 1;
-  const size_t shmem = 2 * sizeof(double) * nb;
-  if (shmem > 48 * 1024) return FPM_ERR_UNSUPPORTED;
+  // Shared-memory histograms up to the default 48 KiB of dynamic shared
+  // memory (3071 edges); larger bin counts accumulate in global memory.
+  const size_t hist = 2 * sizeof(double) * (size_t)nb;
+  const int shared = hist <= 48 * 1024 ? 1 : 0;
   const int64_t nmodes = (int64_t)g.nx * g.ny * g.nzh;
   int64_t blocks = (nmodes + 255) / 256;
   if (blocks > kNumSMs * 8) blocks = kNumSMs * 8;
   if (blocks < 1) blocks = 1;
   g_launches.fetch_add(2, std::memory_order_relaxed);
-  k_pk_accumulate<<<(unsigned)blocks, 256, shmem, st>>>(dk, batch, g,
-                                                        scratch);
+  k_pk_accumulate<<<(unsigned)blocks, 256, shared ? hist : 0, st>>>(
+      dk, batch, g, scratch, shared);
   const double ncell = (double)g.nx * g.ny * g.nz;
   const int nout = batch * (g.nedges - 1);
   k_pk_finalize<<<(nout + 255) / 256, 256, 0, st>>>(
@@ -247,7 +256,8 @@ double* g_static_ptr[kMaxDevices] = {};
 // Device address of g_pk_static_scratch on the current device.  On host,
 // the name g_pk_static_scratch is only a stand-in for the device symbol,
 // so its device address is looked up once per device (with that device
-// current) and cached.
+// current) and cached for the life of the process: a cudaDeviceReset,
+// which unloads the module, is not supported in between.
 int static_scratch(double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return FPM_ERR_CUDA;

@@ -1402,6 +1402,55 @@ extern "C" int fpm_lpt_init(fpm_plan* p, const float* linear,
   return FPM_OK;
 }
 
+extern "C" int fpm_lpt1(fpm_plan* p, const void* dlin_kv, const float* pos,
+                        int64_t npart, float* disp, void* stream) {
+  const float2* dlin_k = (const float2*)dlin_kv;
+  if (!p || !dlin_k || !pos || !disp || npart < 0) return FPM_ERR_ARG;
+  if (!(p->flags & FPM_PLAN_LPT)) return FPM_ERR_STATE;
+  if (npart == 0) return FPM_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  launch_lat_spectrum(p->d_sims, p->nsims, p->ch_ls, dlin_k, p->lspec1, 0, 0,
+                      st);
+  launch_lpt_fourier(p->d_sims, p->nsims, p->ch_ls, p->lspec1, p->lspec9, 1,
+                     tabs_of(p), st, 1);
+  FPM_TRY(launch_ok());
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_c2r(r.lc2r3, p->lspec9 + 3 * S.ls_off,
+                     p->lreal3 + 3 * S.l_off, st));
+  }
+  launch_lpt_readout(p->d_sims, p->nsims, p->lreal3, pos, npart, disp, st);
+  return launch_ok();
+}
+
+extern "C" int fpm_lpt2_source(fpm_plan* p, const void* dlin_kv,
+                               void* source_kv, void* stream) {
+  const float2* dlin_k = (const float2*)dlin_kv;
+  float2* source_k = (float2*)source_kv;
+  if (!p || !dlin_k || !source_k) return FPM_ERR_ARG;
+  if (!(p->flags & FPM_PLAN_LPT)) return FPM_ERR_STATE;
+  cudaStream_t st = (cudaStream_t)stream;
+  launch_lat_spectrum(p->d_sims, p->nsims, p->ch_ls, dlin_k, p->lspec1, 0, 0,
+                      st);
+  launch_lpt_fourier(p->d_sims, p->nsims, p->ch_ls, p->lspec1, p->lspec9, 0,
+                     tabs_of(p), st, 1);
+  FPM_TRY(launch_ok());
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_c2r(r.lc2r9, p->lspec9 + 9 * S.ls_off,
+                     p->lreal9 + 9 * S.l_off, st));
+  }
+  launch_lpt2_source(p->d_sims, p->nsims, p->ch_l, p->lreal9, p->lreal1, st);
+  FPM_TRY(launch_ok());
+  for (auto& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    FPM_TRY(exec_r2c(r.lr2c, p->lreal1 + S.l_off, p->lspec1 + S.ls_off, st));
+  }
+  launch_lat_spectrum(p->d_sims, p->nsims, p->ch_l, p->lspec1, source_k, 1, 1,
+                      st);
+  return launch_ok();
+}
+
 extern "C" int fpm_lpt_adjoint(fpm_plan* p, const float* linear,
                                const double* coef, int order,
                                const float* lam_disp, const float* lam_mom,

@@ -18,8 +18,8 @@ from ._plans import get_plan
 from .kernels import fftk
 from .utils import as_cuda, _seed
 
-__all__ = ['linear_field', 'lpt_init', 'nbody', 'force', 'kick', 'drift',
-           'pgd',
+__all__ = ['linear_field', 'lpt1', 'lpt2_source', 'lpt_init', 'nbody',
+           'force', 'kick', 'drift', 'pgd',
            'linear_amplitude']
 
 
@@ -99,6 +99,51 @@ def linear_field(nc, boxsize, pk, kvec=None, batch_size=1, seed=None,
   else:
     _lib.call('fpm_linear_field', plan.handle, _lib.ptr(amp), _seed(seed), 1,
               None, _lib.ptr(out), _lib.stream_ptr())
+  return out
+
+
+def _spectrum(dlin_k):
+  """Full complex spectra (batch, nx, ny, nz) as contiguous complex64 CUDA."""
+  if not torch.is_tensor(dlin_k):
+    dlin_k = torch.as_tensor(np.asarray(dlin_k))
+  if not dlin_k.is_complex():
+    raise ValueError('dlin_k must be a complex spectrum (batch, nx, ny, nz)')
+  if dlin_k.dim() != 4:
+    raise ValueError('dlin_k must be (batch, nx, ny, nz)')
+  return dlin_k.to(device='cuda', dtype=torch.complex64).contiguous()
+
+
+def lpt1(dlin_k, pos, kvec=None, name='LTP1'):
+  """First-order LPT displacement read out at ``pos`` (flowpm/tfpm.py:66-95):
+  psi_d = c2r3d(dlin_k * laplace_kernel * gradient_kernel_d), then
+  cic_readout(psi_d, pos).  ``dlin_k`` is the full spectrum r2c3d(linear)
+  (batch, nx, ny, nz) complex64; ``pos`` (batch, npart, 3) in mesh units.
+  Returns (batch, npart, 3) float32."""
+  dlin_k = _spectrum(dlin_k)
+  B, nx, ny, nz = dlin_k.shape
+  _check_kvec(kvec, [nx, ny, nz])
+  pos = as_cuda(pos)
+  if pos.dim() != 3 or pos.shape[0] != B or pos.shape[2] != 3:
+    raise ValueError('pos must be (batch, npart, 3)')
+  plan = get_plan([(nx, ny, nz, 1)] * B, flags=_lib.FPM_PLAN_LPT)
+  out = torch.empty_like(pos)
+  _lib.call('fpm_lpt1', plan.handle, _lib.ptr(dlin_k), _lib.ptr(pos),
+            pos.shape[1], _lib.ptr(out), _lib.stream_ptr())
+  return out
+
+
+def lpt2_source(dlin_k, kvec=None, name='LPT2Source'):
+  """Second-order LPT source term (flowpm/tfpm.py:98-145):
+  3/7 sum_{i<j} (phi_ii phi_jj - phi_ij^2) with
+  phi_ij = c2r3d(dlin_k * laplace_kernel * g_i g_j), returned as its full
+  spectrum r2c3d(source), (batch, nx, ny, nz) complex64."""
+  dlin_k = _spectrum(dlin_k)
+  B, nx, ny, nz = dlin_k.shape
+  _check_kvec(kvec, [nx, ny, nz])
+  plan = get_plan([(nx, ny, nz, 1)] * B, flags=_lib.FPM_PLAN_LPT)
+  out = torch.empty_like(dlin_k)
+  _lib.call('fpm_lpt2_source', plan.handle, _lib.ptr(dlin_k), _lib.ptr(out),
+            _lib.stream_ptr())
   return out
 
 

@@ -288,6 +288,26 @@ int fpm_lpt_init(fpm_plan* plan, const float* linear, const double* coef,
                  int order, float* disp, float* mom, float* force,
                  void* stream);
 
+/* First-order LPT displacement read out at arbitrary positions,
+ * flowpm/tfpm.py:66-95 lpt1: for each simulation s of the plan,
+ *   psi_d = c2r3d(dlin_k * laplace_kernel * gradient_kernel_d)
+ *   disp[s, p, d] = cic_readout(psi_d, pos[s, p]).
+ * dlin_k is the full complex spectrum r2c3d(linear) (FFT / N^3) of each
+ * simulation, (nx, ny, nz) complex64 concatenated; only l <= nz/2 is read
+ * (the spectrum of a real field).  pos and disp are (nsims, npart, 3) in
+ * lattice units.  Needs FPM_PLAN_LPT. */
+int fpm_lpt1(fpm_plan* plan, const void* dlin_k, const float* pos,
+             int64_t npart, float* disp, void* stream);
+
+/* Second-order LPT source, flowpm/tfpm.py:98-145 lpt2_source:
+ *   phi_ij = c2r3d(dlin_k * laplace_kernel * g_i g_j),
+ *   source = 3/7 sum_{i<j} (phi_ii phi_jj - phi_ij^2),
+ *   source_k = r2c3d(source) (FFT / N^3),
+ * written as full complex spectra (nx, ny, nz) complex64 per simulation.
+ * dlin_k as in fpm_lpt1.  Needs FPM_PLAN_LPT. */
+int fpm_lpt2_source(fpm_plan* plan, const void* dlin_k, void* source_k,
+                    void* stream);
+
 /* CUDA graphs: capture one fpm_nbody_run (or fpm_nbody_adjoint) with the
  * given buffers into an executable graph, then replay it with
  * fpm_graph_launch on any stream, with one launch instead of ~10 per
@@ -349,7 +369,9 @@ int fpm_saxpy(float* y, const float* x, float a, int64_t n, void* stream);
 
 /* From the unnormalised R2C half spectrum (batch, nx, ny, nz/2 + 1) of the
  * field.  Takes its bin accumulators (2 x batch x (nedges + 1) doubles)
- * from the stream-ordered allocator. */
+ * from the stream-ordered allocator.  Any nedges >= 2: up to 3071 edges
+ * the bins are summed in shared memory first, above that directly in the
+ * accumulators. */
 int fpm_pk_bin(const void* delta_k, int batch, int nx, int ny, int nz,
                const double* boxsize, double kmin, double dk, int nedges,
                float* power, void* stream);
@@ -367,9 +389,12 @@ int fpm_pk_bin(const void* delta_k, int batch, int nx, int ny, int nz,
  * inside this library (FPM_PK_NOALLOC_MAX_DOUBLES doubles), which every GPU
  * that loads the library holds until the process exits; requests with
  * 2 * batch * (nedges + 1) above that return FPM_ERR_LIMIT.  The caller
- * passes the inputs and the output as for fpm_pk_bin.  The first call on a
+ * passes the inputs and the output as for fpm_pk_bin; every nedges that
+ * fpm_pk_bin takes is accepted within that limit.  The first call on a
  * device looks up the array's device address (once per device) -- make
- * that first call before any stream capture.  All calls share the one
+ * that first call before any stream capture; the address is kept for the
+ * life of the process, so do not cudaDeviceReset in between.  All calls
+ * share the one
  * array and each clears the part it uses before summing, so calls whose
  * execution overlaps on the GPU (several streams, several host threads)
  * race; order them on one stream. */
@@ -377,8 +402,9 @@ int fpm_pk_bin_noalloc(const void* delta_k, int batch, int nx, int ny, int nz,
                        const double* boxsize, double kmin, double dk,
                        int nedges, float* power, void* stream);
 
-/* From the real field (batch, nx, ny, nz): R2C (cached cuFFT plan) then
- * fpm_pk_bin. */
+/* From the real field (batch, nx, ny, nz): R2C then fpm_pk_bin.  The
+ * cuFFT plan of each (device, batch, nx, ny, nz) is created on first use
+ * and kept, with its work area, until the process exits. */
 int fpm_power_spectrum(const float* field, int batch, int nx, int ny, int nz,
                        const double* boxsize, double kmin, double dk,
                        int nedges, float* power, void* stream);

@@ -1,21 +1,36 @@
-"""Gradient check of configuration C4 at full size (128^3, 20 steps) against
-the FP64 oracle.  Not collected by pytest: it runs in two halves.
+"""Gradient check of configuration C4 at full size (128^3 particles and mesh,
+box 200 Mpc/h, 20 KDK steps) against the FP64 oracle.  Not collected by
+pytest: it runs in two halves, the first on a GPU, the second on the CPU
+(about two hours on 8 cores for the default sweep).
 
-  python tests/c4_gradient_check.py export OUT.npz           # on a GPU
-  python tests/c4_gradient_check.py check OUT.npz [N] [tape]  # on the CPU
+  python tests/c4_gradient_check.py export OUT.npz             # GPU
+  python tests/c4_gradient_check.py check OUT.npz RESULT.json  # CPU
+      [--ndir 32] [--eps 1e-2,1e-3,1e-4,1e-5] [--no-tape]
 
-`export` builds the C4 problem on the GPU (seeded Eisenstein-Hu linear field,
-2LPT at a0 = 0.1, 20 KDK steps, chi^2 of the final CIC density against that
-density + N(0, 1) noise), computes d chi^2 / d linear with the reverse-time
-adjoint (checkpoints every 5 steps) and saves the linear field, the target
-and the gradient.  `check` recomputes in float64 with the CPU oracle N
-(default 32) central differences along random unit directions and prints
-the relative errors of the GPU gradient against them; with `tape` it also
-takes the oracle's autograd gradient (tens of GB of host memory at 128^3).
+`export` builds the C4 problem on the GPU: seeded Eisenstein-Hu linear field,
+2LPT at a0 = 0.1, 20 KDK steps, chi^2 of the final CIC density against a
+target = that density + N(0, 1) noise (NumPy seed, so the CPU half draws the
+same).  It computes d chi^2 / d linear with the reverse-time adjoint
+(checkpoints every 5 steps) twice: rebuilding the trajectory from the final
+state, and with the stored force potentials (the potential tape).
+
+`check` runs the same problem through the oracle in float64 and compares:
+* the FP64 tape gradient (autograd through the oracle, the stand-in for
+  TensorFlow's tape; each step checkpointed so that it fits in about 20 GB
+  of host memory) with both GPU gradients over all 2^21 components
+  (relative L2) and along `ndir` random unit directions;
+* float64 central differences at each relative step eps (times the field's
+  standard deviation) along the same directions, against the FP64 tape
+  (this shows the finite differences converging, and where they stop) and
+  against the GPU gradients.
+Each direction's numbers are appended to RESULT.json as they come, so a
+partial run still reports.
 """
+import argparse
 import json
 import os
 import sys
+import time
 
 import numpy as np
 
@@ -23,6 +38,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
 N, BOX, A0, STEPS, CKPT = 128, 200.0, 0.1, 20, 5
+LIN_SEED, NOISE_SEED, DIR_SEED = 4242, 77, 5
 
 
 def export(path):
@@ -34,25 +50,30 @@ def export(path):
   pkv = tfpower.linear_matter_power(cosmo, kk)
   pk = lambda k: np.interp(np.log(np.maximum(k, 1e-30)), np.log(kk), pkv,
                            left=0.0)
-  lin = fpm.linear_field(N, BOX, pk, seed=4242)
+  lin = fpm.linear_field(N, BOX, pk, seed=LIN_SEED)
   stages = np.linspace(A0, 1.0, STEPS + 1)
+  zeros = lambda: torch.zeros((1, N, N, N), device='cuda')
   with torch.no_grad():
     st = fpm.nbody(cosmo, fpm.lpt_init(cosmo, lin, A0), stages, N)
-    rho = fpm.cic_paint(torch.zeros((1, N, N, N), device='cuda'), st[0])
-  g = torch.Generator(device='cuda').manual_seed(77)
-  target = rho + torch.randn(rho.shape, generator=g, device='cuda')
-  x = lin.clone().requires_grad_(True)
-  st = fpm.nbody(cosmo, fpm.lpt_init(cosmo, x, A0), stages, N,
-                 checkpoint_every=CKPT)
-  rho = fpm.cic_paint(torch.zeros((1, N, N, N), device='cuda'), st[0])
-  loss = ((rho - target)**2).sum()
-  (grad,) = torch.autograd.grad(loss, x)
-  np.savez(path, linear=lin.cpu().numpy(), target=target.cpu().numpy(),
-           grad=grad.cpu().numpy(), loss=float(loss.detach()))
-  print("exported", path, "loss", float(loss.detach()))
+    rho = fpm.cic_paint(zeros(), st[0])
+  noise = np.random.default_rng(NOISE_SEED).standard_normal(
+      (1, N, N, N)).astype(np.float32)
+  target = rho + torch.tensor(noise, device='cuda')
+  out = {'linear': lin.cpu().numpy(), 'target': target.cpu().numpy()}
+  for name, tape in (('rebuilt', False), ('tape', True)):
+    x = lin.clone().requires_grad_(True)
+    st = fpm.nbody(cosmo, fpm.lpt_init(cosmo, x, A0), stages, N,
+                   checkpoint_every=CKPT, store_potential=tape)
+    rho = fpm.cic_paint(zeros(), st[0])
+    loss = ((rho - target)**2).sum()
+    (grad,) = torch.autograd.grad(loss, x)
+    out['grad_' + name] = grad.cpu().numpy()
+    out['loss_' + name] = float(loss.detach())
+  np.savez(path, **out)
+  print('exported', path, 'loss', out['loss_rebuilt'], out['loss_tape'])
 
 
-def check(path, ndir=32, tape=False):
+def check(path, result, ndir, eps_list, tape):
   import torch
   from oracle import background as obg
   from oracle import pm as opm
@@ -60,7 +81,7 @@ def check(path, ndir=32, tape=False):
   z = np.load(path)
   lin = z['linear'].astype(np.float64)
   target = torch.tensor(z['target'].astype(np.float64))
-  g_gpu = z['grad'].astype(np.float64)
+  g_gpu = {k: z['grad_' + k].astype(np.float64) for k in ('rebuilt', 'tape')}
   b = obg.Background({}, dtype=np.float64)
   stages = np.linspace(A0, 1.0, STEPS + 1)
 
@@ -68,7 +89,7 @@ def check(path, ndir=32, tape=False):
     with torch.set_grad_enabled(grad):
       x = torch.tensor(field, requires_grad=grad)
       s = opm.lpt_init(b, x, A0, order=2)
-      st = opm.nbody(b, s, stages, N)
+      st = (opm.nbody_checkpointed if grad else opm.nbody)(b, s, stages, N)
       rho = opm.cic_paint(torch.zeros((1, N, N, N), dtype=torch.float64),
                           st[0])
       l = ((rho - target)**2).sum()
@@ -77,43 +98,95 @@ def check(path, ndir=32, tape=False):
         return float(l), g.numpy()
       return float(l), None
 
-  res = {'loss_gpu_fp32': float(z['loss'])}
+  res = {'config': 'C4: 128^3, box %g, 20 KDK steps, 2LPT at a0 = %g, '
+                   'chi^2(final CIC density, density + N(0,1))' % (BOX, A0),
+         'loss_gpu_fp32': {k: float(z['loss_' + k]) for k in g_gpu},
+         'cores': torch.get_num_threads()}
+
+  def save():
+    with open(result, 'w') as f:
+      json.dump(res, f, indent=1)
+
+  t0 = time.time()
   g_tape = None
   if tape:
     l0, g_tape = loss(lin, grad=True)
-    res['grad_rel_l2_vs_fp64_tape'] = float(
-        np.linalg.norm(g_gpu - g_tape) / np.linalg.norm(g_tape))
+    res['grad_rel_l2_vs_fp64_tape'] = {
+        k: float(np.linalg.norm(g - g_tape) / np.linalg.norm(g_tape))
+        for k, g in g_gpu.items()}
   else:
     l0, _ = loss(lin)
   res['loss_fp64'] = l0
-  rng = np.random.default_rng(5)
-  eps = 1e-3 * float(np.std(lin))
-  errs, errs_tape = [], []
-  for _ in range(ndir):
+  res['tape_seconds'] = time.time() - t0
+  save()
+  print(json.dumps(res), flush=True)
+  rng = np.random.default_rng(DIR_SEED)
+  sd = float(np.std(lin))
+  res['eps_rel_to_std'] = eps_list
+  res['field_std'] = sd
+  res['directions'] = []
+  for i in range(ndir):
     u = rng.standard_normal(lin.shape)
     u /= np.linalg.norm(u)
-    lp, _ = loss(lin + eps * u)
-    lm, _ = loss(lin - eps * u)
-    fd = (lp - lm) / (2 * eps)
-    errs.append(abs(float(np.sum(g_gpu * u)) - fd) / abs(fd))
+    row = {k: float(np.sum(g * u)) for k, g in g_gpu.items()}
     if g_tape is not None:
-      errs_tape.append(abs(float(np.sum(g_tape * u)) - fd) / abs(fd))
-    print('direction', len(errs), 'fd', fd, 'gpu', float(np.sum(g_gpu * u)),
-          flush=True)
-  res.update({
-      'fd_directions': ndir, 'fd_eps': eps,
-      'gpu_vs_fd_median_rel': float(np.median(errs)),
-      'gpu_vs_fd_max_rel': float(np.max(errs)),
-  })
-  if errs_tape:
-    res['fp64_tape_vs_fd_median_rel'] = float(np.median(errs_tape))
-    res['fp64_tape_vs_fd_max_rel'] = float(np.max(errs_tape))
-  print(json.dumps(res))
+      row['fp64_tape'] = float(np.sum(g_tape * u))
+    row['fd'] = {}
+    for e in eps_list:
+      h = e * sd
+      lp, _ = loss(lin + h * u)
+      lm, _ = loss(lin - h * u)
+      row['fd']['%g' % e] = (lp - lm) / (2 * h)
+    res['directions'].append(row)
+    save()
+    print('direction', i, json.dumps(row), flush=True)
+  res['summary'] = summarize(res)
+  save()
+  print(json.dumps(res['summary'], indent=1))
+
+
+def summarize(res):
+  """Median and max relative errors over the directions: GPU gradients and
+  FD against the FP64 tape, GPU gradients against FD at each eps."""
+  rows = res['directions']
+  out = {'directions': len(rows)}
+
+  def stats(vals):
+    v = np.abs(np.asarray(vals))
+    return {'median': float(np.median(v)), 'max': float(np.max(v))}
+
+  if rows and 'fp64_tape' in rows[0]:
+    t = np.array([r['fp64_tape'] for r in rows])
+    scale = np.abs(t)
+    for k in ('rebuilt', 'tape'):
+      out['gpu_%s_vs_fp64_tape' % k] = stats(
+          (np.array([r[k] for r in rows]) - t) / scale)
+    for e in res['eps_rel_to_std']:
+      fd = np.array([r['fd']['%g' % e] for r in rows])
+      out['fd64_eps_%g_vs_fp64_tape' % e] = stats((fd - t) / scale)
+  for e in res['eps_rel_to_std']:
+    fd = np.array([r['fd']['%g' % e] for r in rows])
+    for k in ('rebuilt', 'tape'):
+      out['gpu_%s_vs_fd64_eps_%g' % (k, e)] = stats(
+          (np.array([r[k] for r in rows]) - fd) / np.abs(fd))
+  return out
 
 
 if __name__ == '__main__':
-  if sys.argv[1] == 'export':
-    export(sys.argv[2])
+  ap = argparse.ArgumentParser()
+  ap.add_argument('phase', choices=['export', 'check', 'summary'])
+  ap.add_argument('npz')
+  ap.add_argument('result', nargs='?', default='c4_gradient_check.json')
+  ap.add_argument('--ndir', type=int, default=32)
+  ap.add_argument('--eps', default='1e-2,1e-3,1e-4,1e-5')
+  ap.add_argument('--no-tape', action='store_true')
+  a = ap.parse_args()
+  if a.phase == 'export':
+    export(a.npz)
+  elif a.phase == 'summary':
+    with open(a.result) as f:
+      r = json.load(f)
+    print(json.dumps(summarize(r), indent=1))
   else:
-    check(sys.argv[2], int(sys.argv[3]) if len(sys.argv) > 3 else 32,
-          len(sys.argv) > 4 and sys.argv[4] == 'tape')
+    check(a.npz, a.result, a.ndir, [float(e) for e in a.eps.split(',')],
+          not a.no_tape)

@@ -1,10 +1,10 @@
 """Generate the golden fixtures under ``tests/golden/`` by executing the
 reference FlowPM source itself.
 
-Run in a container that has the reference tree (read-only) at
-``$FLOWPM_REF`` (default ``/root/reference``)::
+Run with ``FLOWPM_REF`` set to a checkout of the reference (the directory
+that holds ``flowpm/``; it is only read)::
 
-    python tests/golden/make_golden.py
+    FLOWPM_REF=<reference checkout> python tests/golden/make_golden.py
 
 TensorFlow is not installable here, so ``tfshim.py`` (a NumPy emulation of the
 TF 2.5 / TFP 0.13 ops the reference calls) is registered as ``tensorflow``;
@@ -25,10 +25,13 @@ import numpy as np
 from scipy.interpolate import InterpolatedUnivariateSpline as iuspline
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get('FLOWPM_REF', '/root/reference')
+REF = os.environ.get('FLOWPM_REF')
 
 
 def load_reference():
+  if not REF or not os.path.isdir(os.path.join(REF, 'flowpm')):
+    raise SystemExit('set FLOWPM_REF to a checkout of the reference (the '
+                     'directory holding flowpm/)')
   sys.path.insert(0, HERE)
   import tfshim
   tfshim.install()

@@ -149,6 +149,43 @@ def test_lpt_init_golden(fpm, nc, order):
                                                       keepdims=True).max())
 
 
+def test_lpt1_lpt2_source_golden(fpm):
+  """flowpm/tfpm.py:66-95 lpt1 and :98-145 lpt2_source as drop-ins, on the
+  reference's own outputs (lpt1 at the lattice points, c2r3d of the 2LPT
+  source spectrum)."""
+  z = golden('lpt')
+  lk = fpm.r2c3d(z['n16_linear'], norm=16**3)
+  grid = np.indices([16] * 3).reshape(3, -1).T.astype(np.float32)[None]
+  psi = host(fpm.tfpm.lpt1(lk, grid))
+  ref = z['n16_lpt1']
+  assert_allclose(psi, ref, atol=3e-5 * np.abs(ref).max())
+  src = fpm.tfpm.lpt2_source(lk)
+  assert src.shape == (1, 16, 16, 16) and src.dtype == torch.complex64
+  ref = z['n16_lpt2src']
+  assert_allclose(host(fpm.c2r3d(src, norm=16**3)), ref,
+                  atol=3e-5 * np.abs(ref).max())
+
+
+def test_lpt1_lpt2_source_oracle(fpm):
+  """The drop-ins against the oracle on a batch of two rectangular meshes:
+  lpt1 read out at displaced positions (faces and periodic wraps), and the
+  full 2LPT source spectrum, including its Hermitian half l > nz/2."""
+  rng = np.random.default_rng(11)
+  nc = [16, 8, 12]
+  lin = rng.standard_normal([2] + nc).astype(np.float32)
+  lk = opm.r2c3d(torch.tensor(lin))
+  grid = np.indices(nc).reshape(3, -1).T.astype(np.float32)
+  pos = np.stack([grid + rng.uniform(-3, 3, grid.shape).astype(np.float32),
+                  grid - 0.5]).astype(np.float32)
+  pos[0, :4] = [[0, 0, 0], [15.999999, 7.5, -1e-6], [-16, 8, 12], [3, 4, 5]]
+  ref = opm.lpt1(lk, torch.tensor(pos)).numpy()
+  got = host(fpm.tfpm.lpt1(lk.numpy(), pos))
+  assert_allclose(got, ref, atol=2e-5 * np.abs(ref).max())
+  ref = opm.lpt2_source(lk).numpy()
+  got = host(fpm.tfpm.lpt2_source(lk.numpy()))
+  assert_allclose(got, ref, atol=2e-5 * np.abs(ref).max())
+
+
 def test_lpt_init_rectangular_alt_cosmology(fpm):
   z = golden('nbody')
   c = fpm.cosmology.Planck15(**ALT)

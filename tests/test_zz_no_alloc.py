@@ -55,9 +55,26 @@ def test_pk_bin_noalloc_matches_allocating_entry(cuda):
     assert _call(lib, 'fpm_pk_bin_noalloc', spec, box, nedges, got) == 0
     torch.cuda.synchronize()
     assert_allclose(got.cpu().numpy(), ref.cpu().numpy(), rtol=1e-6)
+  # Exactly at the limit (2 * 8 * 1024 = 16384 doubles, bins summed in
+  # shared memory first), and at the limit with more bins than a
+  # shared-memory histogram holds (2 * 2 * 4096), both twice in a row.
+  for batch, nedges in ((8, 1023), (2, 4095), (1, 4000)):
+    for seed in (4, 5):
+      spec = _spectrum(seed, (batch, 8, 8, 8))
+      ref = torch.empty((batch, nedges - 1), device='cuda')
+      got = torch.full_like(ref, float('nan'))
+      assert _call(lib, 'fpm_pk_bin', spec, box, nedges, ref) == 0
+      assert _call(lib, 'fpm_pk_bin_noalloc', spec, box, nedges, got) == 0
+      torch.cuda.synchronize()
+      # bins that no mode reaches are 0/0 in both
+      assert_allclose(got.cpu().numpy(), ref.cpu().numpy(), rtol=1e-6,
+                      equal_nan=True)
   # Requests beyond the fixed array are refused before any work.
   assert _lib.FPM_ERR_LIMIT == 9
   big = torch.empty((64, 8200), device='cuda')
   spec = _spectrum(3, (64, 4, 4, 4))
   assert _call(lib, 'fpm_pk_bin_noalloc', spec, box, 8200, big) == 9
+  # one double past the array: 2 * 1 * (8192 + 1) > 16384
+  spec = _spectrum(3, (1, 4, 4, 4))
+  assert _call(lib, 'fpm_pk_bin_noalloc', spec, box, 8192, big) == 9
   assert lib.fpm_error_string(9).startswith(b'request exceeds')
