@@ -48,9 +48,10 @@ WORKLOAD = ('C2: forward PM, 128^3 particles / 128^3 mesh, box 200 Mpc/h, '
 # force meshes (12 Nc) + paint the density (4 Nc) = 64 B per particle.
 STEP_BYTES_PER_PART = 124
 KERNEL_BYTES_PER_PART = 64
-# DRAM bytes (read + write) of one k_step launch at 128^3, from one ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum = 84.1 + 8.3 MB).
-KSTEP_TRAFFIC_BYTES_128 = 92.4e6
+# DRAM bytes (read + write) of one step-kernel launch at 128^3, from one
+# ncu capture each, by tile (0: the lattice walk's k_step,
+# dram__bytes_read.sum + dram__bytes_write.sum = 84.1 + 8.3 MB).
+KSTEP_TRAFFIC_BYTES_128 = {0: 92.4e6}
 L2_FLUSH_BYTES = 256 << 20
 # seed of replica r's linear field: replicas.replica_seed(1000, r)
 REPLICA_SEED_BASE = 1000
@@ -68,6 +69,12 @@ def parse():
   ap.add_argument('--impl', default='flowpm_b200',
                   choices=['flowpm_b200', 'reference'])
   ap.add_argument('--no-cpu-baseline', action='store_true')
+  ap.add_argument('--no-autotune', action='store_true',
+                  help='keep the lattice walk instead of the autotuned '
+                  'traversal')
+  ap.add_argument('--binning', default=None,
+                  help='TILE,SORT_EVERY: this traversal instead of the '
+                  'autotuned one (0,1: the lattice walk)')
   ap.add_argument('--c5', action='store_true',
                   help='measure the 2 x 512^3 forward + adjoint config even '
                   'with --no-extras (it runs by default otherwise)')
@@ -392,6 +399,7 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5):
   # the forward's potential at every position, for the reverse sweep
   phi_tape = torch.empty((steps + 1) * np_, device='cuda')
   graphs = {}
+  choice, _ = plan.autotune(d0, p0, reps=1, retune=True)
 
   def capture(method):
     if method == 'potential_tape':
@@ -436,6 +444,7 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5):
                   '%d' % ckpt,
       'unit': 'particle-updates/s (forward + adjoint)',
       'gradient_check': GRAD_CHECK_C4,
+      'traversal': list(choice),
   }
   grads = {}
   for method in ('potential_tape', 'rebuilt'):
@@ -456,6 +465,7 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5):
                    'forward_ms': ms_fwd,
                    'adjoint_over_forward': (ms - ms_fwd) / ms_fwd}
   _lib.call('fpm_nbody_set_tape', plan.handle, None, 0)
+  plan.set_binning(0)
   a, b = grads['potential_tape'].double(), grads['rebuilt'].double()
   out['method'] = 'potential_tape'
   out['value'] = out['potential_tape']['value']
@@ -508,10 +518,15 @@ def measure_batched(fpm, flush, reps):
     runner.load(states)
     runner.run()
 
+  batched()  # the first run applies the autotuning policy
+  choice = runner.plan.binning
+
   # plain: one simulation at a time through fpm_nbody, no graph
   singles = []
   for i, (n, box, c, T, seed) in enumerate(sims):
     sp = get_plan([(n, n, n, 1)])
+    # the batch's traversal, so that the two differ only by batching
+    sp.set_binning(*choice)
     singles.append((sp, d0s[i], p0s[i], torch.empty_like(d0s[i]),
                     torch.empty_like(p0s[i]), torch.empty_like(d0s[i]),
                     coefs[i][:T].ravel(), T, ffac[i]))
@@ -545,6 +560,8 @@ def measure_batched(fpm, flush, reps):
   # their plain time.
   tp128 = _timed(lambda: plain(only=128**3), reps, flush)
   runner.close()
+  for sp, *_ in singles:
+    sp.set_binning(0)
   nsim = len(sims)
   return {
       'workload': 'C3: 8x32^3 + 8x64^3 + 4x128^3, per-sim cosmology, 10-20 '
@@ -564,6 +581,7 @@ def measure_batched(fpm, flush, reps):
       'particle_updates_per_s': float(
           sum(n**3 * T for n, _, _, T, _ in sims)) / (tb * 1e-3),
       'max_abs_diff_batched_vs_plain': err,
+      'traversal': list(choice),
   }
 
 
@@ -613,6 +631,7 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
   if tape:
     _lib.call('fpm_nbody_set_tape', plan.handle, _lib.ptr(phi_tape),
               phi_tape.numel())
+  choice, tune_ms = plan.autotune(D0, P0, reps=1, retune=True)
   gf, ga = _lib.ctypes.c_void_p(), _lib.ctypes.c_void_p()
   _lib.call('fpm_graph_capture_nbody', plan.handle, _lib.ptr(D), _lib.ptr(P),
             _lib.ptr(F), None, 0, _lib.ptr(ck), ckpt, _lib.ctypes.byref(gf))
@@ -780,6 +799,8 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
       'value': upd / (t_all * 1e-3),
       'unit': 'particle-updates/s (forward + adjoint)',
       'method': 'potential_tape' if tape else 'rebuilt',
+      'traversal': list(choice),
+      'autotune_ms': tune_ms,
       'forward_ms': t_fwd,
       'forward_adjoint_ms': t_all,
       'sims_per_s_forward_adjoint': 2 / (t_all * 1e-3),
@@ -840,6 +861,19 @@ def main():
   d, p = torch.empty_like(d0), torch.empty_like(p0)
   f = torch.empty_like(d0)
   flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device='cuda')
+  # the library's autotuner: lattice walk or binned step (tile, sort period),
+  # timed on this workload; the choice is cached for equal plans
+  tuning = None
+  if args.binning:
+    plan.set_binning(*[int(v) for v in args.binning.split(',')])
+  elif args.no_autotune:
+    plan.set_binning(0)
+  else:
+    choice, tms = plan.autotune(d0, p0, reps=2, retune=True)
+    tuning = {'choice': list(choice), 'ms_per_config': tms,
+              'how': 'fpm_plan_autotune: one graph replay of the 40-step '
+                     'run per configuration, best of 2 after a warm-up'}
+  tile, every, mode = plan.binning
 
   # the whole 40-step leapfrog as one CUDA graph (kernels + cuFFT)
   graph = _lib.ctypes.c_void_p()
@@ -890,7 +924,7 @@ def main():
   one_step_profiled()
   torch.cuda.synchronize()
   kt, kn = {}, {}
-  for kind, name in [(0, 'step'), (1, 'fourier'), (2, 'paint')]:
+  for kind, name in [(0, 'step'), (1, 'fourier'), (2, 'paint'), (10, 'sort')]:
     tot, cnt = _lib.c_double(), _lib.c_int64()
     _lib.call('fpm_plan_profile_read', plan.handle, kind,
               _lib.ctypes.byref(tot), _lib.ctypes.byref(cnt))
@@ -898,6 +932,13 @@ def main():
   _lib.call('fpm_plan_profile', plan.handle, 0)
   if plan.status(st):
     raise RuntimeError('non-finite state in the timed region')
+  # final density of the timed simulation, for the parity leg at the end
+  X = torch.empty_like(d)
+  _lib.call('fpm_lattice_shift', _lib.ptr(d), _lib.ptr(X), 1, N_MESH, N_MESH,
+            N_MESH, 1, st)
+  rho_final = fpm.cic_paint(torch.zeros([1] + nc, device='cuda'),
+                            X).cpu().numpy()
+  del X
   ms_max = replicas.max_over_ranks(ms, device='cuda')
   updates = float(npart) * N_STEPS * args.steps * world
   value = updates / (ms_max * 1e-3)
@@ -951,7 +992,8 @@ def main():
 
   peak, peak_kind = peaks()
   step_ms = kt['step'] / max(kn['step'], 1)
-  kbytes = KERNEL_BYTES_PER_PART * npart
+  # the binned step also reads each particle's Lagrangian index (4 B)
+  kbytes = (KERNEL_BYTES_PER_PART + (4 if tile else 0)) * npart
   achieved = kbytes / (step_ms * 1e-3) / 1e9
   whole = STEP_BYTES_PER_PART * npart * N_STEPS * args.steps / (ms * 1e-3) / 1e9
   line = {
@@ -983,15 +1025,24 @@ def main():
           },
       },
       'gpu_launches': int(n_launch),
+      'traversal': ('particles sorted by cell (keys in tiles of %d^3 '
+                    'cells) every %d steps, %s' % (
+                        tile, every, 'equal chunks' if mode == 1 else
+                        'one block per tile, shared-memory paint'))
+                   if tile else 'lattice walk',
+      'autotune': tuning,
       'roofline': {
-          'kernel': 'k_step (fused readout + kick + drift + CIC paint)',
+          'kernel': (('k_step_sorted' if mode == 1 else 'k_step_binned')
+                     if tile else 'k_step') +
+                    ' (fused readout + kick + drift + CIC paint)',
           'bound': 'hbm',
           'achieved': achieved,
           'peak': peak,
           'peak_kind': peak_kind,
           'unit': 'GB/s',
           'frac': achieved / peak,
-          'traffic': KSTEP_TRAFFIC_BYTES_128 if N_MESH == 128 else None,
+          'traffic': KSTEP_TRAFFIC_BYTES_128.get(tile) if N_MESH == 128
+                     else None,
           'algorithmic_bytes_per_launch': kbytes,
           'avg_launch_ms': step_ms,
       },
@@ -1022,14 +1073,8 @@ def main():
     # final density of the timed simulation, against the oracle run from
     # the same linear field (FP32 and FP64); the FP32 run is also the CPU
     # baseline
-    reset()
-    one_step()
-    X = torch.empty_like(d)
-    _lib.call('fpm_lattice_shift', _lib.ptr(d), _lib.ptr(X), 1, N_MESH,
-              N_MESH, N_MESH, 1, st)
-    rho = fpm.cic_paint(torch.zeros([1] + nc, device='cuda'), X)
     line['parity'], line['cpu_baseline'] = parity_and_cpu_baseline(
-        lin.cpu(), rho.cpu().numpy())
+        lin.cpu(), rho_final)
   _lib.lib.fpm_graph_destroy(graph)
   if rank == 0:
     print(json.dumps(line))

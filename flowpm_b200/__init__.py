@@ -19,6 +19,6 @@ from .tfpm import nbody, linear_field, lpt_init
 from .pk import power_spectrum
 from .batch import BatchRunner, nbody_many
 from .stream import NBodyStream, nbody_stream
-from ._plans import clear_plans
+from ._plans import clear_plans, set_autotune
 
 __version__ = '0.1.0'

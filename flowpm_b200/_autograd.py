@@ -14,7 +14,7 @@ import torch
 
 from . import _lib
 from . import tfbackground as bg
-from ._plans import get_plan
+from ._plans import get_plan, tune
 
 
 class CicPaint(torch.autograd.Function):
@@ -203,6 +203,8 @@ class NBody(torch.autograd.Function):
       _lib.call('fpm_nbody_set_tape', plan.handle, _lib.ptr(tape),
                 tape.numel())
     try:
+      if pgd is None:
+        tune(plan, d, p, (T, tape is not None))
       _lib.call('fpm_nbody_run', plan.handle, _lib.ptr(d), _lib.ptr(p),
                 _lib.ptr(f), None, 0, _lib.ptr(ckpt), k, st)
     finally:

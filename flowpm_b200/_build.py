@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libflowpm_b200.so')
 SOURCES = ['fpm_cic.cu', 'fpm_kernels.cu', 'fpm_adjoint.cu', 'fpm_pk.cu',
-           'fpm_fft.cu', 'fpm_planes.cu',
+           'fpm_fft.cu', 'fpm_planes.cu', 'fpm_bin.cu',
            'fpm_plan.cu']
 CUDA_HOME = os.environ.get('CUDA_HOME', '/usr/local/cuda')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']

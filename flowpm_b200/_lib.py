@@ -48,6 +48,10 @@ SIGNATURES = {
     'fpm_nbody_set_steps': (c_int, [c_void_p, c_int, P_int32, P_double,
                                     P_double, c_void_p]),
     'fpm_nbody_set_pgd': (c_int, [c_void_p, c_int, P_double, c_void_p]),
+    'fpm_plan_set_binning': (c_int, [c_void_p, c_int, c_int, c_int]),
+    'fpm_plan_autotune': (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                  P_int32, ctypes.POINTER(c_float),
+                                  c_void_p]),
     'fpm_pgd': (c_int, [c_void_p, c_void_p, P_double, c_void_p]),
     'fpm_nbody_run': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p,
                               c_void_p, c_uint, c_void_p, c_int, c_void_p]),
@@ -124,6 +128,9 @@ FPM_PLAN_ADJOINT = 8
 FPM_PLAN_CUFFT = 16
 FPM_PLAN_SMALL_BLOCKS = 32
 FPM_NBODY_INTERMEDIATE = 1
+FPM_TUNE_CONFIGS = 8
+FPM_BIN_TILES = 0
+FPM_BIN_CHUNKS = 1
 FPM_STATUS_NONFINITE_POS = 1
 FPM_STATUS_NONFINITE_MOM = 2
 

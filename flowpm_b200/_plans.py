@@ -29,6 +29,57 @@ class Plan(object):
     self.device_bytes = nbytes.value
     self._work = None
     self._graphs = {}
+    self.binning = (0, 1, _lib.FPM_BIN_CHUNKS)
+
+  def set_binning(self, tile, sort_every=1, mode=_lib.FPM_BIN_CHUNKS):
+    """Binned forward step (``fpm_plan_set_binning``): particles sorted by
+    force-mesh cell, keys tile-major in tiles of ``tile``^3 cells (8 or 16;
+    0: the lattice walk), re-sorted every ``sort_every`` steps; ``mode``
+    FPM_BIN_CHUNKS (equal particle chunks) or FPM_BIN_TILES (one block per
+    tile, shared-memory paint).  Drops captured graphs."""
+    _lib.call('fpm_plan_set_binning', self.handle, int(tile), int(sort_every),
+              int(mode))
+    self.binning = (int(tile), int(sort_every), int(mode)) if tile else (
+        0, 1, _lib.FPM_BIN_CHUNKS)
+    for g in self._graphs.values():
+      _lib.lib.fpm_graph_destroy(g)
+    self._graphs = {}
+
+  def autotune(self, disp, mom, reps=2, retune=False):
+    """``fpm_plan_autotune`` on the plan's current step tables from the state
+    (disp, mom) (each (total_particles, 3), left unchanged): the fastest of
+    the lattice walk and the binned configurations is set on the plan.
+    Returns ((tile, sort_every), {config: ms}); configurations the meshes do
+    not support, or a cached choice, report no time."""
+    choice = (ctypes.c_int32 * 3)()
+    ms = (ctypes.c_float * _lib.FPM_TUNE_CONFIGS)()
+    _lib.call('fpm_plan_autotune', self.handle, _lib.ptr(disp), _lib.ptr(mom),
+              int(reps), int(bool(retune)), choice, ms, _lib.stream_ptr())
+    self.binning = (choice[0], choice[1], choice[2])
+    for g in self._graphs.values():
+      _lib.lib.fpm_graph_destroy(g)
+    self._graphs = {}
+    names = ['walk', 'chunks8/1', 'chunks8/2', 'chunks8/4', 'chunks16/2',
+             'chunks16/4', 'tiles8/4', 'tiles16/4']
+    return self.binning, {n: (float(t) if t >= 0 else None)
+                          for n, t in zip(names, ms)}
+
+  def apply_tuned(self):
+    """Apply the autotuner's cached choice for this plan's key (device,
+    flags, step tables' length, PGD, tape, shapes), if there is one;
+    returns the (tile, sort_every) set, or None."""
+    choice = (ctypes.c_int32 * 3)()
+    code = _lib.lib.fpm_plan_autotune(self.handle, None, None, 1, 0, choice,
+                                      None, _lib.stream_ptr())
+    if code == _lib.FPM_ERR_STATE:
+      return None
+    _lib.check('fpm_plan_autotune', code)
+    if (choice[0], choice[1], choice[2]) != self.binning:
+      for g in self._graphs.values():
+        _lib.lib.fpm_graph_destroy(g)
+      self._graphs = {}
+    self.binning = (choice[0], choice[1], choice[2])
+    return self.binning
 
   @property
   def nsims(self):
@@ -86,6 +137,32 @@ class Plan(object):
 
 
 _cache = {}
+
+# Autotuning policy of the drop-in API (nbody, the batch runner, the stream):
+# plans of at least min_particles particles time the lattice walk against
+# the binned step configurations on their first run (fpm_plan_autotune) and
+# keep the fastest; smaller plans, and every plan when disabled, apply a
+# choice already cached for their key or keep the lattice walk.
+TUNING = {'enabled': True, 'min_particles': 1 << 21, 'reps': 2}
+
+
+def set_autotune(enabled=True, min_particles=1 << 21):
+  """Switch the autotuning policy of nbody / BatchRunner / NBodyStream."""
+  TUNING['enabled'] = bool(enabled)
+  TUNING['min_particles'] = int(min_particles)
+
+
+def tune(plan, disp, mom, key):
+  """Apply the policy to ``plan`` (step tables set, ``disp``/``mom`` its
+  initial state): once per plan and ``key`` (the step count, tape use)."""
+  if getattr(plan, '_tuned_for', None) == key:
+    return plan.binning
+  plan._tuned_for = key
+  if plan.apply_tuned() is not None:
+    return plan.binning
+  if TUNING['enabled'] and plan.total_particles >= TUNING['min_particles']:
+    return plan.autotune(disp, mom, reps=TUNING['reps'])[0]
+  return plan.binning
 
 
 def get_plan(dims, r_split=0.0, flags=0):

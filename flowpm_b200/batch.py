@@ -15,7 +15,7 @@ import torch
 
 from . import _lib
 from . import tfbackground as bg
-from ._plans import Plan
+from ._plans import Plan, tune
 from .utils import as_cuda
 
 __all__ = ['BatchRunner', 'nbody_many']
@@ -67,6 +67,7 @@ class BatchRunner(object):
                    ffac)
     self.d, self.p, self.f = self.plan.work()
     self._graph = None
+    self._binning_set = False
 
   def _set_steps(self, st):
     T, nsteps, coefs, ffac = self._steps
@@ -91,6 +92,8 @@ class BatchRunner(object):
     st = _lib.stream_ptr()
     if self._graph is None:
       self._set_steps(st)
+      if not self._binning_set:
+        tune(self.plan, self.d, self.p, (self.max_steps, False))
       g = ctypes.c_void_p()
       _lib.call('fpm_graph_capture_nbody', self.plan.handle,
                 _lib.ptr(self.d), _lib.ptr(self.p), _lib.ptr(self.f), None, 0,
@@ -119,6 +122,14 @@ class BatchRunner(object):
       s[2, 0].copy_(self.f[off:off + npart])
       out[i] = s
     return out
+
+  def set_binning(self, tile, sort_every=1, mode=_lib.FPM_BIN_CHUNKS):
+    """Binned forward step for this batch (see ``Plan.set_binning``)."""
+    if self._graph is not None:
+      _lib.lib.fpm_graph_destroy(self._graph)
+      self._graph = None
+    self.plan.set_binning(tile, sort_every, mode)
+    self._binning_set = True
 
   def status(self):
     return self.plan.status()

@@ -1,0 +1,542 @@
+// Eulerian binning of the particles and the binned leapfrog step.
+//
+// The lattice-walk step (k_step) visits particles in Lagrangian order: as
+// the run goes on, the 32 particles of a warp spread over many cells, so its
+// CIC gathers and deposits touch many L2 sectors (at 128^3 the step grows
+// from 63 us at the first leapfrog step to 114 us at the last, nearly all of
+// it in the paint's reductions).  The binned step keeps the particle state
+// sorted by force-mesh cell instead, cell keys tile-major (tiles of T^3
+// cells, z fastest inside a tile), each particle carrying its Lagrangian
+// index, so:
+// * one block owns one tile: it reads its particles as one contiguous,
+//   coalesced range, and consecutive lanes sit in the same or neighbouring
+//   cells, so each CIC gather touches few sectors;
+// * the block deposits the paint into a shared-memory copy of its tile plus
+//   a halo, and adds that copy to the density with one 16-byte vector
+//   reduction per four cells; only deposits that fall outside the halo (a
+//   particle that drifted more than a cell out of its tile since the last
+//   sort) go to global memory directly.
+// Particles are re-sorted every few steps by a counting sort on the cell
+// key (count, exclusive scan, scatter), which replaces tf.scatter_nd's role
+// in flowpm/utils.py:87-89 (the reference deposits in arbitrary order).
+// Outputs that the caller sees in Lagrangian order (final state, force,
+// checkpoints, intermediate states) are written through the carried index.
+#include "fpm_bin.cuh"
+
+namespace fpm {
+
+namespace {
+
+// Tile-major key of force-mesh cell (cx, cy, cz) inside its simulation.
+template <int T>
+__device__ __forceinline__ unsigned cell_key(const BinRun& R, int cx, int cy,
+                                             int cz) {
+  const unsigned tx = (unsigned)cx / T, ty = (unsigned)cy / T,
+                 tz = (unsigned)cz / T;
+  const unsigned lx = (unsigned)cx % T, ly = (unsigned)cy % T,
+                 lz = (unsigned)cz % T;
+  return ((tx * (unsigned)R.nty + ty) * (unsigned)R.ntz + tz) * (T * T * T) +
+         (lx * T + ly) * T + lz;
+}
+
+// Run-relative cell key (simulation r of the run: + r * ncell) of the
+// particle in slot t of the run, and its Lagrangian index.
+template <int T>
+__device__ __forceinline__ uint64_t particle_key(const BinRun& R,
+                                                 const float* __restrict__ d,
+                                                 const uint32_t* __restrict__ lag,
+                                                 int64_t t, uint32_t& l) {
+  const int64_t r = t / R.np;
+  l = lag ? lag[R.p0 + t] : (uint32_t)(t - r * R.np);
+  const unsigned tt = l / (unsigned)R.nz;
+  const int k = (int)(l - tt * (unsigned)R.nz);
+  const int i = (int)(tt / (unsigned)R.ny);
+  const int j = (int)(tt - (unsigned)i * (unsigned)R.ny);
+  const float3 dv = ld3(d, R.p0 + t);
+  const float b = (float)R.bf;
+  const float x = __fmul_rn(__fadd_rn(index_float(i), dv.x), b);
+  const float y = __fmul_rn(__fadd_rn(index_float(j), dv.y), b);
+  const float z = __fmul_rn(__fadd_rn(index_float(k), dv.z), b);
+  const int cx = cic_axis(x, R.mx).i0, cy = cic_axis(y, R.my).i0,
+            cz = cic_axis(z, R.mz).i0;
+  return (uint64_t)r * (uint64_t)R.ncell + cell_key<T>(R, cx, cy, cz);
+}
+
+// cnt[m0 + key] += 1 for every particle of the run (warp-aggregated: lanes
+// with equal keys add once).
+template <int T>
+__global__ void __launch_bounds__(256)
+k_bin_count(BinRun R, const float* __restrict__ d,
+            const uint32_t* __restrict__ lag, int32_t* __restrict__ cnt) {
+  const int64_t n = (int64_t)R.count * R.np;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t l;
+    const uint64_t key = particle_key<T>(R, d, lag, t, l);
+    const unsigned m = __match_any_sync(__activemask(), key);
+    if ((threadIdx.x & 31) == __ffs(m) - 1)
+      atomicAdd(cnt + R.m0 + key, (int32_t)__popc(m));
+  }
+}
+
+// Scatter: slot = off[key]++ (warp-aggregated, lanes of equal keys keep
+// their order); writes d, p and the Lagrangian index to the output arrays.
+template <int T>
+__global__ void __launch_bounds__(256)
+k_bin_scatter(BinRun R, const float* __restrict__ d,
+              const float* __restrict__ p, const uint32_t* __restrict__ lag,
+              int32_t* __restrict__ off, float* __restrict__ d_out,
+              float* __restrict__ p_out, uint32_t* __restrict__ lag_out) {
+  const int64_t n = (int64_t)R.count * R.np;
+  const int lane = threadIdx.x & 31;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t l;
+    const uint64_t key = particle_key<T>(R, d, lag, t, l);
+    const unsigned m = __match_any_sync(__activemask(), key);
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(off + R.m0 + key, (int32_t)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    const int64_t dst = base + __popc(m & ((1u << lane) - 1));
+    st3(d_out, dst, ld3(d, R.p0 + t));
+    st3(p_out, dst, ld3(p, R.p0 + t));
+    lag_out[dst] = l;
+  }
+}
+
+// Exclusive scan of v[0..n) in place (n a multiple of 4, v 16-byte
+// aligned), plus base: three passes over chunks of kScanChunk values.
+constexpr int kScanThreads = 256, kScanPer = 16;
+constexpr int kScanChunk = kScanThreads * kScanPer;
+
+__device__ __forceinline__ int block_excl_scan(int v, int& total) {
+  __shared__ int ws[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = lane < kScanThreads / 32 ? ws[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < kScanThreads / 32) ws[lane] = s;
+  }
+  __syncthreads();
+  total = ws[kScanThreads / 32 - 1];
+  const int excl = x - v + (w > 0 ? ws[w - 1] : 0);
+  __syncthreads();  // ws is reused by the next call
+  return excl;
+}
+
+__device__ __forceinline__ int4 load_part(const int32_t* v, int64_t i,
+                                          int64_t n) {
+  return i < n ? *reinterpret_cast<const int4*>(v + i) : make_int4(0, 0, 0, 0);
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_sums(const int32_t* __restrict__ v, int64_t n, int32_t* sums) {
+  const int64_t b0 = (int64_t)blockIdx.x * kScanChunk;
+  int s = 0;
+#pragma unroll
+  for (int q = 0; q < kScanPer / 4; ++q) {
+    const int4 a = load_part(v, b0 + (q * kScanThreads + threadIdx.x) * 4, n);
+    s += a.x + a.y + a.z + a.w;
+  }
+  int total;
+  block_excl_scan(s, total);
+  if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// One block: exclusive scan of the nb chunk sums, plus base.
+__global__ void __launch_bounds__(1024)
+k_scan_top(int32_t* sums, int nb, int32_t base) {
+  __shared__ int part[1024];
+  const int per = (nb + 1023) / 1024;
+  const int b0 = threadIdx.x * per;
+  int s = 0;
+  for (int i = 0; i < per && b0 + i < nb; ++i) s += sums[b0 + i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = base;
+    for (int t = 0; t < 1024; ++t) {
+      const int x = part[t];
+      part[t] = acc;
+      acc += x;
+    }
+  }
+  __syncthreads();
+  int acc = part[threadIdx.x];
+  for (int i = 0; i < per && b0 + i < nb; ++i) {
+    const int x = sums[b0 + i];
+    sums[b0 + i] = acc;
+    acc += x;
+  }
+}
+
+// Thread t of block b scans the 16 values [b0 + 4 (q 256 + t), + 4) for
+// q < 4 -- four int4 groups, strided for coalescing -- so its prefix runs
+// over the groups in block order: group (q, t) precedes (q, t + 1) and
+// (q + 1, 0).  The block scan runs once per q.
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_apply(int32_t* __restrict__ v, int64_t n,
+             const int32_t* __restrict__ sums) {
+  const int64_t b0 = (int64_t)blockIdx.x * kScanChunk;
+  int carry = sums[blockIdx.x];
+#pragma unroll
+  for (int q = 0; q < kScanPer / 4; ++q) {
+    const int64_t i = b0 + (q * kScanThreads + threadIdx.x) * 4;
+    int4 a = load_part(v, i, n);
+    const int s = a.x + a.y + a.z + a.w;
+    int total;
+    const int e = block_excl_scan(s, total) + carry;
+    carry += total;
+    if (i < n) {
+      int4 o;
+      o.x = e;
+      o.y = e + a.x;
+      o.z = o.y + a.y;
+      o.w = o.z + a.z;
+      *reinterpret_cast<int4*>(v + i) = o;
+    }
+  }
+}
+
+// Offset of periodic cell c from the origin o of a tile of T cells: the
+// representative of c - o (mod m) nearest the tile's centre, in
+// [T/2 - m/2, T/2 + m/2) (so every cell of the tile maps into [0, T) even
+// when m = T).
+template <int T>
+__device__ __forceinline__ int rel_cell(int c, int o, int m) {
+  int r = c - o - T / 2;
+  if (r >= (m >> 1)) r -= m;
+  else if (r < -(m >> 1)) r += m;
+  return r + T / 2;
+}
+
+// The binned leapfrog step: one tile of T^3 force-mesh cells per block
+// iteration.  Per particle the arithmetic is k_step's (readout, closing
+// kick, opening kick, drift, paint), in the same order and rounding.  The
+// paint goes into a shared-memory copy of the cells [o - 1, o + T + 1] in
+// x and y and [o - 4, o + T + 4) in z (z padded so that it flushes as
+// aligned float4), then into rho with one vector reduction per nonzero
+// group of four cells; a deposit outside that region goes to rho directly.
+template <int T>
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
+k_step_binned(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
+              int64_t nchunks, BinStepArgs b) {
+  constexpr int RX = T + 3, RZ = T + 8, RN = RX * RX * RZ;
+  constexpr int T3 = T * T * T;
+  __shared__ __align__(16) float tile[RN];
+  pdl_wait();  // the force meshes of the solve before
+  const StepArgs& a = b.a;
+  for (int64_t ch = ch0 + blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kTile);
+    const SimDev S = sims[s];
+    const int Tn = a.nsteps[s];
+    if (a.it > Tn) continue;  // this sim has finished
+    const float* cf = a.coefs + (int64_t)s * a.max_steps * 3;
+    const float ke = a.it >= 1 ? cf[(a.it - 1) * 3 + 2] : 0.f;
+    const bool last = (a.it == Tn);
+    const float ks = last ? 0.f : cf[a.it * 3 + 0];
+    const float dr = last ? 0.f : cf[a.it * 3 + 1];
+    const float fac = a.ffac[s];
+    const float invb = 1.0f / (float)S.bf;
+    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
+    float* m = a.rho + S.m_off;
+    const unsigned t = (unsigned)(ch - S.ch_t);
+    const unsigned r = t / (unsigned)S.ntz;
+    const int oz = (int)(t - r * (unsigned)S.ntz) * T;
+    const int ox = (int)(r / (unsigned)S.nty) * T;
+    const int oy = (int)(r - (unsigned)(ox / T) * (unsigned)S.nty) * T;
+    const int64_t kf = S.m_off + (int64_t)t * T3;
+    // a simulation's first tile starts at its first particle (the cell
+    // before it belongs to another simulation, possibly of another run
+    // whose sort may be in flight on another stream)
+    const int begin = t == 0 ? (int)S.p_off : b.cell_end[kf - 1];
+    const int end = b.cell_end[kf + T3 - 1];
+    if (!last) {
+      for (int q = threadIdx.x; q < RN / 4; q += blockDim.x)
+        reinterpret_cast<float4*>(tile)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncthreads();
+    }
+    for (int i = begin + (int)threadIdx.x; i < end; i += blockDim.x) {
+      const uint32_t l = b.blag[i];
+      int qi, qj, qk;
+      lattice_ijk(S, l, qi, qj, qk);
+      const int64_t g = S.p_off + l;  // Lagrangian slot
+      float3 d = ld3(b.bd, i), p = ld3(b.bp, i);
+      const float3 x = mesh_pos(S, qi, qj, qk, d);
+      const Cic8 c0 = cic8(cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
+                           cic_axis(x.z, S.mz), S.my, S.mz);
+      float3 f = readout_cic8(a.fmesh + 3 * S.m_off, mcells, c0);
+      // force = readout * factor / pm_nc_factor (flowpm/tfpm.py:218, :356)
+      f.x = __fmul_rn(__fmul_rn(f.x, fac), invb);
+      f.y = __fmul_rn(__fmul_rn(f.y, fac), invb);
+      f.z = __fmul_rn(__fmul_rn(f.z, fac), invb);
+      if (a.it >= 1) p = axpy(p, ke, f);  // closing kick of step it-1
+      if (a.ckpt && a.it % a.ckpt_every == 0) {
+        float* o = a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3;
+        st3(o, g, d);
+        st3(o + a.total_np * 3, g, p);
+      }
+      if (a.inter && a.it >= 1) {
+        float* o = a.inter + (int64_t)(a.it - 1) * 3 * a.total_np * 3;
+        st3(o, g,
+            make_float3(__fadd_rn(index_float(qi), d.x),
+                        __fadd_rn(index_float(qj), d.y),
+                        __fadd_rn(index_float(qk), d.z)));
+        st3(o + a.total_np * 3, g, p);
+        st3(o + 2 * a.total_np * 3, g, f);
+      }
+      if (last) {  // uniform over the block: one sim per tile
+        st3(a.force_out, g, f);
+        st3(a.mom, g, p);
+        st3(a.disp, g, d);
+        if (!finite3(p.x, p.y, p.z) || !finite3(f.x, f.y, f.z))
+          atomicOr(a.status, FPM_STATUS_NONFINITE_MOM);
+        continue;
+      }
+      p = axpy(p, ks, f);  // opening kick of step it
+      d = axpy(d, dr, p);  // drift of step it
+      st3(b.bp, i, p);
+      st3(b.bd, i, d);
+      const float3 xn = mesh_pos(S, qi, qj, qk, d);
+      if (!finite3(xn.x, xn.y, xn.z))
+        atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
+      const Axis ax = cic_axis(xn.x, S.mx), ay = cic_axis(xn.y, S.my),
+                 az = cic_axis(xn.z, S.mz);
+      const int rx = rel_cell<T>(ax.i0, ox, S.mx),
+                ry = rel_cell<T>(ay.i0, oy, S.my),
+                rz = rel_cell<T>(az.i0, oz, S.mz);
+      const Cic8 c1 = cic8(ax, ay, az, S.my, S.mz);
+      if (rx >= -1 && rx <= T && ry >= -1 && ry <= T && rz >= -4 &&
+          rz <= T + 2) {
+        float* t0 = tile + ((rx + 1) * RX + (ry + 1)) * RZ + (rz + 4);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float* tq = t0 + (q & 1) * (RX * RZ) + (q >> 1) * RZ;
+          atomicAdd(tq, __fmul_rn(c1.wxy[q], c1.wz0));
+          atomicAdd(tq + 1, __fmul_rn(c1.wxy[q], c1.wz1));
+        }
+      } else {
+        paint_cic8(m, c1, 1.f);
+      }
+    }
+    if (last) continue;
+    __syncthreads();
+    for (int q = threadIdx.x; q < RN / 4; q += blockDim.x) {
+      const float4 v = reinterpret_cast<const float4*>(tile)[q];
+      if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+      const int zg = q % (RZ / 4), row = q / (RZ / 4);
+      const int cy = wrap_near(oy - 1 + row % RX, S.my);
+      const int cx = wrap_near(ox - 1 + row / RX, S.mx);
+      const int cz = wrap_near(oz - 4 + 4 * zg, S.mz);
+      red_add_f4(m + ((int64_t)cx * S.my + cy) * S.mz + cz, v);
+    }
+    __syncthreads();  // the next tile zeroes the shared copy
+  }
+}
+
+// The step over the sorted particles in equal chunks (kChunk slots of one
+// simulation per block iteration, the chunks of the lattice order, so the
+// work per block does not depend on the clustering), CIC gathers and
+// deposits straight from and to global memory.  Consecutive lanes sit in
+// the same or neighbouring cells, so the gathers and reductions of a warp
+// touch few sectors.  Lanes that deposit into the same base cell are
+// contiguous in the sorted order: when a warp has such runs, each of the 8
+// corner weights is summed over its run with a segmented shuffle reduction
+// (5 steps) and only the run's first lane issues the reductions.  The sums
+// of a run are formed in a different order than one deposit at a time
+// (FP32 rounding, as any order of the reference's scatter).
+__global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
+k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
+              int64_t nchunks, BinStepArgs b) {
+  pdl_wait();  // the force meshes of the solve before
+  const StepArgs& a = b.a;
+  const int lane = threadIdx.x & 31;
+  for (int64_t ch = ch0 + blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kPart);
+    const SimDev S = sims[s];
+    const int Tn = a.nsteps[s];
+    if (a.it > Tn) continue;  // this sim has finished
+    const float* cf = a.coefs + (int64_t)s * a.max_steps * 3;
+    const float ke = a.it >= 1 ? cf[(a.it - 1) * 3 + 2] : 0.f;
+    const bool last = (a.it == Tn);
+    const float ks = last ? 0.f : cf[a.it * 3 + 0];
+    const float dr = last ? 0.f : cf[a.it * 3 + 1];
+    const float fac = a.ffac[s];
+    const float invb = 1.0f / (float)S.bf;
+    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
+    float* m = a.rho + S.m_off;
+    const int64_t first = S.p_off + (ch - S.ch_p) * kChunk;
+    const int64_t end = S.p_off + S.np;
+#pragma unroll 1
+    for (int item = 0; item < kItems; ++item) {
+      const int64_t i = first + item * kThreads + threadIdx.x;
+      const bool valid = i < end;  // warp-uniform except in a sim's last chunk
+      uint32_t l = 0;
+      float3 d = make_float3(0.f, 0.f, 0.f), p = d;
+      if (valid) {
+        l = b.blag[i];
+        d = ld3(b.bd, i);
+        p = ld3(b.bp, i);
+      }
+      int qi, qj, qk;
+      lattice_ijk(S, l, qi, qj, qk);
+      const int64_t g = S.p_off + l;  // Lagrangian slot
+      const float3 x = mesh_pos(S, qi, qj, qk, d);
+      const Cic8 c0 = cic8(cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
+                           cic_axis(x.z, S.mz), S.my, S.mz);
+      float3 f = valid ? readout_cic8(a.fmesh + 3 * S.m_off, mcells, c0)
+                       : make_float3(0.f, 0.f, 0.f);
+      // force = readout * factor / pm_nc_factor (flowpm/tfpm.py:218, :356)
+      f.x = __fmul_rn(__fmul_rn(f.x, fac), invb);
+      f.y = __fmul_rn(__fmul_rn(f.y, fac), invb);
+      f.z = __fmul_rn(__fmul_rn(f.z, fac), invb);
+      if (a.it >= 1) p = axpy(p, ke, f);  // closing kick of step it-1
+      if (valid && a.ckpt && a.it % a.ckpt_every == 0) {
+        float* o = a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3;
+        st3(o, g, d);
+        st3(o + a.total_np * 3, g, p);
+      }
+      if (valid && a.inter && a.it >= 1) {
+        float* o = a.inter + (int64_t)(a.it - 1) * 3 * a.total_np * 3;
+        st3(o, g,
+            make_float3(__fadd_rn(index_float(qi), d.x),
+                        __fadd_rn(index_float(qj), d.y),
+                        __fadd_rn(index_float(qk), d.z)));
+        st3(o + a.total_np * 3, g, p);
+        st3(o + 2 * a.total_np * 3, g, f);
+      }
+      if (last) {  // uniform over the block: one sim per chunk
+        if (valid) {
+          st3(a.force_out, g, f);
+          st3(a.mom, g, p);
+          st3(a.disp, g, d);
+          if (!finite3(p.x, p.y, p.z) || !finite3(f.x, f.y, f.z))
+            atomicOr(a.status, FPM_STATUS_NONFINITE_MOM);
+        }
+        continue;
+      }
+      p = axpy(p, ks, f);  // opening kick of step it
+      d = axpy(d, dr, p);  // drift of step it
+      const float3 xn = mesh_pos(S, qi, qj, qk, d);
+      if (valid) {
+        st3(b.bp, i, p);
+        st3(b.bd, i, d);
+        if (!finite3(xn.x, xn.y, xn.z))
+          atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
+      }
+      const Cic8 c1 = cic8(cic_axis(xn.x, S.mx), cic_axis(xn.y, S.my),
+                           cic_axis(xn.z, S.mz), S.my, S.mz);
+      // base cell of the deposit; a lane past the sim's end gets a key of
+      // its own
+      const unsigned key = valid ? c1.row[0] + c1.z0 : 0xffffffffu - lane;
+      const unsigned up = __shfl_up_sync(0xffffffffu, key, 1);
+      const bool head = lane == 0 || up != key;
+      float w[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        w[2 * q] = __fmul_rn(c1.wxy[q], c1.wz0);
+        w[2 * q + 1] = __fmul_rn(c1.wxy[q], c1.wz1);
+      }
+      const unsigned heads = __ballot_sync(0xffffffffu, head);
+      if (heads != 0xffffffffu) {
+        // segmented sums over runs of contiguous lanes with equal keys (a
+        // key can recur in a later run after the particles drifted since
+        // their sort; each run deposits its own sum): lane + o is in this
+        // lane's run when no run starts in (lane, lane + o]
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const bool same =
+              lane + o < 32 &&
+              ((unsigned long long)heads >> (lane + 1) & ((1ull << o) - 1)) == 0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const float t = __shfl_down_sync(0xffffffffu, w[q], o);
+            if (same) w[q] = __fadd_rn(w[q], t);
+          }
+        }
+      }
+      if (valid && head) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          red_add(m + c1.row[q] + c1.z0, w[2 * q]);
+          red_add(m + c1.row[q] + c1.z1, w[2 * q + 1]);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+void launch_step_sorted(const SimDev* sims, int nsims, int64_t ch0,
+                        int64_t ch1, const BinStepArgs& b, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  launch_pdl(k_step_sorted, dim3(grid_for(ch1 - ch0)), dim3(kThreads), 0, st,
+             sims, nsims, ch0, ch1, b);
+}
+
+void launch_step_binned(int tile, const SimDev* sims, int nsims, int64_t ch0,
+                        int64_t ch1, const BinStepArgs& b, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (tile == 8)
+    launch_pdl(k_step_binned<8>, dim3(grid_for(ch1 - ch0)), dim3(kThreads), 0,
+               st, sims, nsims, ch0, ch1, b);
+  else
+    launch_pdl(k_step_binned<16>, dim3(grid_for(ch1 - ch0)), dim3(kThreads),
+               0, st, sims, nsims, ch0, ch1, b);
+}
+
+bool bin_tile_supported(int tile, int mx, int my, int mz) {
+  if (tile != 8 && tile != 16) return false;
+  return mx % tile == 0 && my % tile == 0 && mz % tile == 0;
+}
+
+size_t bin_scan_blocks(int64_t ncells) {
+  return (size_t)((ncells + kScanChunk - 1) / kScanChunk);
+}
+
+int launch_bin_sort(int tile, const BinRun& R, const float* d,
+                    const float* p, const uint32_t* lag, int32_t* cell,
+                    int32_t* sums, float* d_out, float* p_out,
+                    uint32_t* lag_out, cudaStream_t st) {
+  const int64_t ncells = (int64_t)R.count * R.ncell;
+  const int64_t n = (int64_t)R.count * R.np;
+  if (cudaMemsetAsync(cell + R.m0, 0, sizeof(int32_t) * ncells, st) !=
+      cudaSuccess)
+    return FPM_ERR_CUDA;
+  int64_t blocks = (n + 255) / 256;
+  const int64_t cap = (int64_t)kNumSMs * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  g_launches.fetch_add(5, std::memory_order_relaxed);
+  if (tile == 8)
+    k_bin_count<8><<<(unsigned)blocks, 256, 0, st>>>(R, d, lag, cell);
+  else
+    k_bin_count<16><<<(unsigned)blocks, 256, 0, st>>>(R, d, lag, cell);
+  const int nb = (int)bin_scan_blocks(ncells);
+  k_scan_sums<<<nb, kScanThreads, 0, st>>>(cell + R.m0, ncells, sums);
+  k_scan_top<<<1, 1024, 0, st>>>(sums, nb, (int32_t)R.p0);
+  k_scan_apply<<<nb, kScanThreads, 0, st>>>(cell + R.m0, ncells, sums);
+  if (tile == 8)
+    k_bin_scatter<8><<<(unsigned)blocks, 256, 0, st>>>(
+        R, d, p, lag, cell, d_out, p_out, lag_out);
+  else
+    k_bin_scatter<16><<<(unsigned)blocks, 256, 0, st>>>(
+        R, d, p, lag, cell, d_out, p_out, lag_out);
+  return cudaGetLastError() == cudaSuccess ? FPM_OK : FPM_ERR_CUDA;
+}
+
+}  // namespace fpm

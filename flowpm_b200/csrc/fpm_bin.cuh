@@ -1,0 +1,61 @@
+// Eulerian binning of the particles (fpm_bin.cu): counting sort by
+// force-mesh cell and the binned leapfrog step, used by the plan
+// orchestration in fpm_plan.cu.
+#pragma once
+
+#include "fpm_kernels.cuh"
+
+namespace fpm {
+
+// One run of a plan (consecutive simulations of equal shape) as the sort
+// kernels see it: slot p0 + r * np + t is particle t of simulation r, whose
+// force-mesh cells start at m0 + r * ncell.
+struct BinRun {
+  int nx, ny, nz, bf, mx, my, mz;
+  int ntx, nty, ntz;       // tiles per axis
+  int count;               // simulations
+  int64_t np, ncell, p0, m0;
+};
+
+// Tile sizes the binned step is built for (8 or 16 cells per side) and
+// whether a force mesh divides into them.
+bool bin_tile_supported(int tile, int mx, int my, int mz);
+
+// Chunk sums the scan of ncells cell counts needs.
+size_t bin_scan_blocks(int64_t ncells);
+
+// Counting sort of the run's particles by tile-major cell key: cell counts
+// into cell[m0 ..), their exclusive scan (plus p0: absolute slots), then the
+// scatter of (d, p, Lagrangian index) into the output arrays; afterwards
+// cell[c] holds the end slot of cell c.  lag NULL: the input is in
+// Lagrangian order (slot p0 + r np + t is lattice site t).  sums: at least
+// bin_scan_blocks(count * ncell) ints.
+int launch_bin_sort(int tile, const BinRun& R, const float* d,
+                    const float* p, const uint32_t* lag, int32_t* cell,
+                    int32_t* sums, float* d_out, float* p_out,
+                    uint32_t* lag_out, cudaStream_t st);
+
+// State of the binned step: the sorted particles (updated in place), their
+// Lagrangian indices and the cells' end slots of the last sort.  The
+// StepArgs' disp, mom and force_out are the caller's Lagrangian arrays,
+// written at the last step (and ckpt / inter through the index).
+struct BinStepArgs {
+  StepArgs a;
+  float* bd;
+  float* bp;
+  const uint32_t* blag;
+  const int32_t* cell_end;
+};
+
+// The step over the tile chunks [ch0, ch1) (whole simulations), painting
+// through shared-memory tiles.
+void launch_step_binned(int tile, const SimDev* sims, int nsims, int64_t ch0,
+                        int64_t ch1, const BinStepArgs& b, cudaStream_t st);
+
+// The step over the sorted particles in equal chunks (the particle chunks
+// [ch0, ch1), whole simulations), painting straight into the density with
+// warp-segmented sums of equal deposits.
+void launch_step_sorted(const SimDev* sims, int nsims, int64_t ch0,
+                        int64_t ch1, const BinStepArgs& b, cudaStream_t st);
+
+}  // namespace fpm

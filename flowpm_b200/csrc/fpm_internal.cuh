@@ -52,6 +52,11 @@ struct SimDev {
   int wi;                // particles per thread of a lattice block, whose
                          // x extent is kPlanes wi
   int xpass;             // cuFFT plane transforms + the x-pass kernel
+  // Eulerian cell tiles of the binned step (fpm_plan_set_binning): tiles of
+  // T^3 force-mesh cells, ntx x nty x ntz of them, the first one at ch_t in
+  // the plan's tile enumeration
+  int ntx, nty, ntz;
+  int64_t ch_t;
 };
 
 // Per-axis Fourier tables.  For an axis of n cells and index i,
@@ -109,7 +114,8 @@ __device__ __forceinline__ float green_w(const Green& G, int s, double kk,
 }
 
 enum ChunkKind {
-  kPart = 0, kSpec = 1, kMesh = 2, kLat = 3, kLatSpec = 4, kBlock = 5
+  kPart = 0, kSpec = 1, kMesh = 2, kLat = 3, kLatSpec = 4, kBlock = 5,
+  kTile = 6
 };
 
 __device__ __forceinline__ int64_t chunk_first(const SimDev& s, int kind) {
@@ -119,6 +125,7 @@ __device__ __forceinline__ int64_t chunk_first(const SimDev& s, int kind) {
     case kMesh: return s.ch_m;
     case kLat: return s.ch_l;
     case kBlock: return s.ch_b;
+    case kTile: return s.ch_t;
     default: return s.ch_ls;
   }
 }
@@ -230,6 +237,13 @@ __host__ __device__ __forceinline__ int conn_z(int c) {
 
 __device__ __forceinline__ void red_add(float* p, float v) {
   asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
+// p[0..3] += v as one 16-byte vector reduction (p 16-byte aligned).
+__device__ __forceinline__ void red_add_f4(float* p, float4 v) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p),
+               "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+               : "memory");
 }
 
 // p[0..2] += (a, b, c) as one 16-byte vector reduction (p 16-byte aligned;

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "fpm_adjoint.cuh"
+#include "fpm_bin.cuh"
 
 using namespace fpm;
 
@@ -27,8 +28,9 @@ namespace {
 // 0 step, 1 Fourier solve, 2 initial paint, and on the cuFFT path of the
 // solve 3 the Green's-function kernel, 4 the stencil gradient kernel;
 // reverse sweep: 5 reverse drift + paint, 6 force VJP, 7 divergence
-// stencil, 8 adjoint potential solve, 9 the whole reverse step
-constexpr int kProfKinds = 10;
+// stencil, 8 adjoint potential solve, 9 the whole reverse step; 10 the
+// particle sort of the binned step (fpm_plan_set_binning)
+constexpr int kProfKinds = 11;
 
 // Particles per thread of the lattice blocks of lattices of 2^26 particles
 // or more (x extent twice that).
@@ -46,6 +48,7 @@ struct Run {
   // when the run is ordered by non-increasing step count), and the batched
   // cuFFT plans of each smaller active count.
   std::vector<int> active;
+  int64_t bsum_off = 0;    // this run's chunk sums in fpm_plan::bsums
   std::map<int, cufftHandle> r2c_n, c2r3_n, r2c3_n, c2r1_n;
   cufftHandle r2c = 0, c2r3 = 0;     // force mesh
   cufftHandle r2c3 = 0, c2r1 = 0;    // force mesh, adjoint
@@ -130,6 +133,20 @@ struct fpm_plan {
   int64_t coef_gen = 0;   // bumped whenever d_coefs is reallocated
   int64_t sched_gen = 0;  // bumped whenever the active-prefix schedule moves
   size_t work_bytes = 0;  // size of the shared cuFFT work area
+  // Eulerian binning of the forward step (fpm_plan_set_binning): tile size
+  // (0: the lattice walk), sort period, the sorted state in two buffers,
+  // the carried Lagrangian indices, per-cell counts / end slots and the
+  // scan's chunk sums
+  int bin_tile = 0;
+  int bin_every = 1;
+  int bin_mode = FPM_BIN_TILES;
+  int64_t total_tiles = 0;
+  float* bd[2] = {nullptr, nullptr};
+  float* bp[2] = {nullptr, nullptr};
+  uint32_t* blag[2] = {nullptr, nullptr};
+  int32_t* bcell = nullptr;
+  int32_t* bsums = nullptr;
+  size_t bin_bytes = 0;
   // optional per-kernel timing (fpm_plan_profile)
   bool profile = false;
   std::vector<cudaEvent_t> ev[kProfKinds];
@@ -201,6 +218,10 @@ void free_all(fpm_plan* p) {
                   p->d_pgd1,
                   p->lmesh,  p->lrho,   p->fpart,   p->phi};
   for (void* b : bufs)
+    if (b) cudaFree(b);
+  void* bins[] = {p->bd[0], p->bd[1], p->bp[0], p->bp[1], p->blag[0],
+                  p->blag[1], p->bcell, p->bsums};
+  for (void* b : bins)
     if (b) cudaFree(b);
 }
 
@@ -1015,6 +1036,131 @@ int nbody_chains(fpm_plan* p, StepArgs a, cudaStream_t st) {
   return launch_ok();
 }
 
+// ---------------------------------------------------------------------------
+// Binned forward step (fpm_plan_set_binning)
+// ---------------------------------------------------------------------------
+BinRun bin_run(const fpm_plan* p, const Run& r) {
+  const SimDev& S = p->sims[r.first];
+  BinRun R;
+  R.nx = S.nx;
+  R.ny = S.ny;
+  R.nz = S.nz;
+  R.bf = S.bf;
+  R.mx = S.mx;
+  R.my = S.my;
+  R.mz = S.mz;
+  R.ntx = S.ntx;
+  R.nty = S.nty;
+  R.ntz = S.ntz;
+  R.count = r.count;
+  R.np = S.np;
+  R.ncell = (int64_t)S.mx * S.my * S.mz;
+  R.p0 = S.p_off;
+  R.m0 = S.m_off;
+  return R;
+}
+
+// Counting sort of run k's particles from (d, pm, lag) -- lag NULL: the
+// caller's Lagrangian order -- into the plan's sorted buffer dst.
+int bin_sort_run(fpm_plan* p, size_t k, const float* d, const float* pm,
+                 const uint32_t* lag, int dst, cudaStream_t st) {
+  const Run& r = p->runs[k];
+  return launch_bin_sort(p->bin_tile, bin_run(p, r), d, pm, lag, p->bcell,
+                         p->bsums + r.bsum_off, p->bd[dst], p->bp[dst],
+                         p->blag[dst], st);
+}
+
+int64_t run_part_chunk(const fpm_plan* p, size_t k) {
+  if (k >= p->runs.size()) return p->ch_p;
+  return p->sims[p->runs[k].first].ch_p;
+}
+
+int64_t run_tile_chunk(const fpm_plan* p, size_t k) {
+  if (k >= p->runs.size()) return p->total_tiles;
+  return p->sims[p->runs[k].first].ch_t;
+}
+
+BinStepArgs bin_args(const fpm_plan* p, const StepArgs& a, int cur) {
+  BinStepArgs b;
+  b.a = a;
+  b.bd = p->bd[cur];
+  b.bp = p->bp[cur];
+  b.blag = p->blag[cur];
+  b.cell_end = p->bcell;
+  return b;
+}
+
+// The leapfrog on the binned step: the caller's Lagrangian state is sorted
+// into buffer 0, then every step runs the solve and the binned step, and
+// every bin_every steps the particles are sorted into the other buffer.
+// The last step writes the final d, p and F back in Lagrangian order.
+int nbody_binned(fpm_plan* p, StepArgs a, cudaStream_t st) {
+  for (size_t k = 0; k < p->runs.size(); ++k)
+    FPM_TRY(bin_sort_run(p, k, a.disp, a.mom, nullptr, 0, st));
+  if (chains_ok(p)) {
+    const Green G = plan_green(p);
+    FPM_CUDA(cudaEventRecord(p->ev_fork, st));
+    for (size_t k = 0; k < p->runs.size(); ++k) {
+      Run& r = p->runs[k];
+      const SimDev& S = p->sims[r.first];
+      cudaStream_t rs = k == 0 ? st : p->side[k - 1];
+      if (k > 0) FPM_CUDA(cudaStreamWaitEvent(rs, p->ev_fork, 0));
+      const int64_t c0 = run_tile_chunk(p, k), c1 = run_tile_chunk(p, k + 1);
+      int cur = 0;
+      for (int it = 0; it <= p->max_steps; ++it) {
+        const int n = run_active(r, it);
+        if (n == 0) continue;  // every simulation of the run has finished
+        launch_fft_force(p->d_sims, r.first, n, S.mx, S.my, S.mz, p->rho,
+                         it < p->max_steps ? 1 : 0, p->dk, p->fk, p->fmesh,
+                         p->tape ? tape_phi(p, it) : p->phi, tabs_of(p), G,
+                         !stencil_path(p), rs);
+        a.it = it;
+        if (p->bin_mode == FPM_BIN_CHUNKS)
+          launch_step_sorted(p->d_sims, p->nsims, run_part_chunk(p, k),
+                             run_part_chunk(p, k + 1), bin_args(p, a, cur),
+                             rs);
+        else
+          launch_step_binned(p->bin_tile, p->d_sims, p->nsims, c0, c1,
+                             bin_args(p, a, cur), rs);
+        if (it < p->max_steps && (it + 1) % p->bin_every == 0) {
+          FPM_TRY(bin_sort_run(p, k, p->bd[cur], p->bp[cur], p->blag[cur],
+                               1 - cur, rs));
+          cur = 1 - cur;
+        }
+      }
+      if (k > 0) {
+        FPM_CUDA(cudaEventRecord(p->ev_join[k - 1], rs));
+        FPM_CUDA(cudaStreamWaitEvent(st, p->ev_join[k - 1], 0));
+      }
+    }
+    return launch_ok();
+  }
+  int cur = 0;
+  for (int it = 0; it <= p->max_steps; ++it) {
+    FPM_TRY(force_meshes(p, st, it < p->max_steps, it,
+                         p->tape ? tape_phi(p, it) : nullptr));
+    a.it = it;
+    prof_mark(p, 0, st);
+    if (p->bin_mode == FPM_BIN_CHUNKS)
+      launch_step_sorted(p->d_sims, p->nsims, 0, p->ch_p, bin_args(p, a, cur),
+                         st);
+    else
+      launch_step_binned(p->bin_tile, p->d_sims, p->nsims, 0, p->total_tiles,
+                         bin_args(p, a, cur), st);
+    prof_mark(p, 0, st);
+    FPM_TRY(launch_ok());
+    if (it < p->max_steps && (it + 1) % p->bin_every == 0) {
+      prof_mark(p, 10, st);
+      for (size_t k = 0; k < p->runs.size(); ++k)
+        FPM_TRY(bin_sort_run(p, k, p->bd[cur], p->bp[cur], p->blag[cur],
+                             1 - cur, st));
+      prof_mark(p, 10, st);
+      cur = 1 - cur;
+    }
+  }
+  return FPM_OK;
+}
+
 extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
                              float* force, float* inter, unsigned flags,
                              float* ckpt, int ckpt_every, void* stream) {
@@ -1045,6 +1191,7 @@ extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
   prof_mark(p, 2, st);
   FPM_TRY(launch_ok());
   if (p->tape && p->tape_floats < tape_needed(p)) return FPM_ERR_ARG;
+  if (p->bin_tile && !p->pgd_on) return nbody_binned(p, a, st);
   if (chains_ok(p)) return nbody_chains(p, a, st);
   for (int it = 0; it <= p->max_steps; ++it) {
     FPM_TRY(force_meshes(p, st, it < p->max_steps, it,
@@ -1113,6 +1260,95 @@ extern "C" int fpm_nbody_set_pgd(fpm_plan* p, int enable, const double* params,
     p->pgd_on = true;
     p->sched_gen++;
   }
+  return FPM_OK;
+}
+
+namespace {
+
+void free_bins(fpm_plan* p) {
+  void* bins[] = {p->bd[0], p->bd[1], p->bp[0], p->bp[1], p->blag[0],
+                  p->blag[1], p->bcell, p->bsums};
+  for (void* b : bins)
+    if (b) cudaFree(b);
+  p->bd[0] = p->bd[1] = p->bp[0] = p->bp[1] = nullptr;
+  p->blag[0] = p->blag[1] = nullptr;
+  p->bcell = p->bsums = nullptr;
+  p->device_bytes -= p->bin_bytes;
+  p->bin_bytes = 0;
+}
+
+}  // namespace
+
+extern "C" int fpm_plan_set_binning(fpm_plan* p, int tile, int sort_every,
+                                    int mode) {
+  if (!p || tile < 0 || sort_every < 1 ||
+      (mode != FPM_BIN_TILES && mode != FPM_BIN_CHUNKS))
+    return FPM_ERR_ARG;
+  if (tile == 0) {
+    if (p->bin_tile) {
+      if (cudaDeviceSynchronize() != cudaSuccess) return FPM_ERR_CUDA;
+      free_bins(p);
+      p->bin_tile = 0;
+      p->sched_gen++;
+    }
+    return FPM_OK;
+  }
+  if (p->total_np >= ((int64_t)1 << 31) - 1) return FPM_ERR_UNSUPPORTED;
+  for (const SimDev& S : p->sims)
+    if (!bin_tile_supported(tile, S.mx, S.my, S.mz) || S.m_off % 4 != 0)
+      return FPM_ERR_UNSUPPORTED;
+  if (tile == p->bin_tile) {
+    if (sort_every != p->bin_every || mode != p->bin_mode) {
+      p->bin_every = sort_every;
+      p->bin_mode = mode;
+      p->sched_gen++;  // captured graphs hold the old schedule and kernel
+    }
+    return FPM_OK;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return FPM_ERR_CUDA;
+  free_bins(p);
+  std::vector<SimDev> sims = p->sims;
+  int64_t tiles = 0;
+  for (SimDev& S : sims) {
+    S.ntx = S.mx / tile;
+    S.nty = S.my / tile;
+    S.ntz = S.mz / tile;
+    S.ch_t = tiles;
+    tiles += (int64_t)S.ntx * S.nty * S.ntz;
+  }
+  int64_t nsum = 0;
+  for (auto& r : p->runs) {
+    r.bsum_off = nsum;
+    const SimDev& S = sims[r.first];
+    nsum += (int64_t)bin_scan_blocks((int64_t)r.count * S.mx * S.my * S.mz);
+  }
+  bool ok = true;
+  size_t tot = 0;
+  for (int b = 0; b < 2; ++b) {
+    p->bd[b] = dalloc<float>(3 * p->total_np, tot, ok);
+    p->bp[b] = dalloc<float>(3 * p->total_np, tot, ok);
+    p->blag[b] = dalloc<uint32_t>(p->total_np, tot, ok);
+  }
+  p->bcell = dalloc<int32_t>(p->total_m, tot, ok);
+  p->bsums = dalloc<int32_t>(nsum, tot, ok);
+  p->bin_bytes = tot;
+  p->device_bytes += tot;
+  if (!ok) {
+    cudaGetLastError();
+    free_bins(p);
+    return FPM_ERR_OOM;
+  }
+  if (cudaMemcpy(p->d_sims, sims.data(), sizeof(SimDev) * sims.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    free_bins(p);
+    return FPM_ERR_CUDA;
+  }
+  p->sims = sims;
+  p->total_tiles = tiles;
+  p->bin_tile = tile;
+  p->bin_every = sort_every;
+  p->bin_mode = mode;
+  p->sched_gen++;
   return FPM_OK;
 }
 
@@ -1813,4 +2049,145 @@ extern "C" int fpm_c2r3d(const void* cfield, void* rfield, int batch, int nx,
   cudaFreeAsync(tmp, st);
   if (rc != FPM_OK) return rc;
   return launch_ok();
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the forward step's particle traversal
+// ---------------------------------------------------------------------------
+namespace {
+
+// (tile, sort period, mode) of each configuration fpm_plan_autotune times:
+// the lattice walk; the sorted particles in equal chunks (keys tile-major
+// in tiles of 8 or 16 cells) re-sorted every 1, 2 or 4 leapfrog steps; the
+// shared-memory tiles of 8 or 16 cells re-sorted every 4 steps.
+constexpr int kTune[FPM_TUNE_CONFIGS][3] = {
+    {0, 1, FPM_BIN_CHUNKS},  {8, 1, FPM_BIN_CHUNKS},  {8, 2, FPM_BIN_CHUNKS},
+    {8, 4, FPM_BIN_CHUNKS},  {16, 2, FPM_BIN_CHUNKS}, {16, 4, FPM_BIN_CHUNKS},
+    {8, 4, FPM_BIN_TILES},   {16, 4, FPM_BIN_TILES}};
+
+std::mutex g_tune_mu;
+// choice per (device, plan flags, step count, PGD, tape, dims...)
+std::map<std::vector<int64_t>, int> g_tune_cache;
+
+std::vector<int64_t> tune_key(const fpm_plan* p) {
+  int dev = -1;
+  cudaGetDevice(&dev);
+  std::vector<int64_t> k = {dev, (int64_t)p->flags, p->max_steps,
+                            p->pgd_on ? 1 : 0, p->tape ? 1 : 0, p->nsims};
+  for (const SimDev& S : p->sims) {
+    k.push_back(S.nx);
+    k.push_back(S.ny);
+    k.push_back(S.nz);
+    k.push_back(S.bf);
+  }
+  return k;
+}
+
+}  // namespace
+
+extern "C" int fpm_plan_autotune(fpm_plan* p, const float* disp,
+                                 const float* mom, int reps, int retune,
+                                 int32_t* choice, float* ms, void* stream) {
+  if (!p || !choice || reps < 1 || (!retune && !disp) != (!retune && !mom) ||
+      (retune && (!disp || !mom)))
+    return FPM_ERR_ARG;
+  if (!p->steps_set) return FPM_ERR_STATE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const std::vector<int64_t> key = tune_key(p);
+  if (!retune) {
+    int c = -1;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) c = it->second;
+    }
+    if (c >= 0) {
+      FPM_TRY(fpm_plan_set_binning(p, kTune[c][0], kTune[c][1], kTune[c][2]));
+      choice[0] = kTune[c][0];
+      choice[1] = kTune[c][1];
+      choice[2] = kTune[c][2];
+      if (ms)
+        for (int k = 0; k < FPM_TUNE_CONFIGS; ++k) ms[k] = -1.f;
+      return FPM_OK;
+    }
+    if (!disp) return FPM_ERR_STATE;  // nothing cached, nothing to time on
+  }
+  // candidates run on scratch copies of the state, each as one graph replay
+  const size_t nb = sizeof(float) * 3 * (size_t)p->total_np;
+  float *sd = nullptr, *sp = nullptr, *sf = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = FPM_OK;
+  if (cudaMalloc(&sd, nb) != cudaSuccess || cudaMalloc(&sp, nb) != cudaSuccess ||
+      cudaMalloc(&sf, nb) != cudaSuccess)
+    rc = FPM_ERR_OOM;
+  if (rc == FPM_OK && (cudaEventCreate(&e0) != cudaSuccess ||
+                       cudaEventCreate(&e1) != cudaSuccess))
+    rc = FPM_ERR_CUDA;
+  int best = -1;
+  float best_ms = 0.f;
+  for (int c = 0; rc == FPM_OK && c < FPM_TUNE_CONFIGS; ++c) {
+    if (ms) ms[c] = -1.f;
+    const int src =
+        fpm_plan_set_binning(p, kTune[c][0], kTune[c][1], kTune[c][2]);
+    if (src == FPM_ERR_UNSUPPORTED) continue;
+    if (src == FPM_ERR_OOM) {  // larger configurations will not fit either
+      cudaGetLastError();
+      continue;
+    }
+    if (src != FPM_OK) {
+      rc = src;
+      break;
+    }
+    fpm_graph* g = nullptr;
+    rc = fpm_graph_capture_nbody(p, sd, sp, sf, nullptr, 0, nullptr, 0, &g);
+    float tmin = 0.f;
+    for (int r = 0; rc == FPM_OK && r <= reps; ++r) {
+      if (cudaMemcpyAsync(sd, disp, nb, cudaMemcpyDeviceToDevice, st) !=
+              cudaSuccess ||
+          cudaMemcpyAsync(sp, mom, nb, cudaMemcpyDeviceToDevice, st) !=
+              cudaSuccess ||
+          cudaEventRecord(e0, st) != cudaSuccess) {
+        rc = FPM_ERR_CUDA;
+        break;
+      }
+      rc = fpm_graph_launch(g, st);
+      if (rc != FPM_OK) break;
+      float t = 0.f;
+      if (cudaEventRecord(e1, st) != cudaSuccess ||
+          cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
+        rc = FPM_ERR_CUDA;
+        break;
+      }
+      if (r > 0 && (r == 1 || t < tmin)) tmin = t;  // r = 0 warms up
+    }
+    if (g) fpm_graph_destroy(g);
+    if (rc != FPM_OK) break;
+    if (ms) ms[c] = tmin;
+    if (best < 0 || tmin < best_ms) {
+      best = c;
+      best_ms = tmin;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(sd);
+  cudaFree(sp);
+  cudaFree(sf);
+  if (rc == FPM_OK && best < 0) rc = FPM_ERR_UNSUPPORTED;
+  if (rc != FPM_OK) {
+    cudaGetLastError();
+    fpm_plan_set_binning(p, 0, 1, FPM_BIN_CHUNKS);
+    return rc;
+  }
+  FPM_TRY(fpm_plan_set_binning(p, kTune[best][0], kTune[best][1],
+                               kTune[best][2]));
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  choice[0] = kTune[best][0];
+  choice[1] = kTune[best][1];
+  choice[2] = kTune[best][2];
+  return FPM_OK;
 }

@@ -14,7 +14,7 @@ import torch
 from . import _autograd
 from . import _lib
 from . import tfbackground as bg
-from ._plans import get_plan
+from ._plans import get_plan, tune
 from .kernels import fftk
 from .utils import as_cuda, _seed
 
@@ -319,6 +319,8 @@ def nbody(cosmo, state, stages, nc, pm_nc_factor=1,
   _lib.call('fpm_lattice_shift', _lib.ptr(state[0]), _lib.ptr(d), B, nc[0],
             nc[1], nc[2], -1, st)
   p.copy_(state[1].reshape(-1, 3))
+  if par is None:
+    tune(plan, d, p, (T, False))
   inter = None
   if return_intermediate_states and T > 0:
     inter = torch.empty((T, 3) + tuple(state.shape[1:]), dtype=torch.float32,

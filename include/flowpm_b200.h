@@ -232,6 +232,49 @@ int fpm_nbody_set_pgd(fpm_plan* plan, int enable, const double* params,
  * kl, ks) per simulation, nsims x 3 doubles.  Synchronises the stream. */
 int fpm_pgd(fpm_plan* plan, float* disp, const double* params, void* stream);
 
+/* Eulerian binning of the forward leapfrog (replaces the particle order of
+ * the reference's tf.scatter_nd / tf.gather_nd, flowpm/utils.py:87-89,
+ * :207-209, which is arbitrary): with tile 8 or 16, fpm_nbody_run keeps the
+ * particle state sorted by force-mesh cell, cell keys tile-major in tiles
+ * of tile^3 cells, and re-sorts it every sort_every leapfrog steps
+ * (counting sort carrying each particle's Lagrangian index).  mode
+ * FPM_BIN_CHUNKS steps the sorted particles in equal chunks, painting into
+ * the density directly with warp-summed deposits of neighbouring lanes;
+ * FPM_BIN_TILES gives each tile to one block, which paints into a
+ * shared-memory copy of the tile.  The caller's arrays stay in Lagrangian
+ * order; the results equal the lattice walk's up to the order of the
+ * density's FP32 sums.  tile 0 returns to the lattice walk.  Allocates 56
+ * bytes per particle and 4 per force-mesh cell (freed by tile 0 or
+ * fpm_plan_destroy), synchronising the device; every force mesh must divide
+ * into tiles (else FPM_ERR_UNSUPPORTED).  Plans with PGD switched on keep
+ * the lattice walk.  Captured graphs of the plan must be captured again. */
+enum { FPM_BIN_TILES = 0, FPM_BIN_CHUNKS = 1 };
+int fpm_plan_set_binning(fpm_plan* plan, int tile, int sort_every, int mode);
+
+/* Autotuner of the forward step's particle traversal.  No counterpart in
+ * the reference (TensorFlow picks its own kernels).  Times, on the plan's
+ * current step tables (fpm_nbody_set_steps first) and on scratch copies of
+ * the state (disp, mom: total_particles x 3, left unchanged), one graph
+ * replay of fpm_nbody_run for each of FPM_TUNE_CONFIGS configurations --
+ * the lattice walk; the binned step (fpm_plan_set_binning) in chunks with
+ * keys in tiles of 8 cells re-sorted every 1, 2 or 4 steps and of 16 cells
+ * every 2 or 4; in shared-memory tiles of 8 or 16 cells every 4 -- keeping
+ * the best of reps timed replays after one warm-up, and leaves the fastest
+ * set on the plan.  choice[0..2] = its (tile, sort_every, mode); ms
+ * (FPM_TUNE_CONFIGS
+ * floats, or NULL) the times, -1 for configurations the plan's meshes do
+ * not support.  The choice is cached per device, plan flags, step count,
+ * PGD and tape setting and simulation shapes: a later call with the same
+ * key and retune == 0 applies it without timing (ms all -1); with
+ * retune == 0, disp and mom may be NULL to apply a cached choice only
+ * (FPM_ERR_STATE, plan unchanged, when there is none).  Allocates scratch
+ * state and synchronises the stream; captured graphs of the plan must be
+ * captured again. */
+#define FPM_TUNE_CONFIGS 8
+int fpm_plan_autotune(fpm_plan* plan, const float* disp, const float* mom,
+                      int reps, int retune, int32_t* choice, float* ms,
+                      void* stream);
+
 /* Checkpoints: when ckpt is not NULL, fpm_nbody_run stores the state
  * (disp, mom) at every position j (after the closing kick of step j-1,
  * j = 0 the initial state) with j % ckpt_every == 0 in slot j / ckpt_every

@@ -429,23 +429,34 @@ def test_nbody_adjoint_64_20_steps_vs_tape(fpm, capsys, store):
   nc = [n] * 3
   rng = np.random.default_rng(64)
   target = _rho_oracle(lin, stages, nc) + rng.standard_normal([1] + nc)
-  b64 = obg.Background({}, dtype=np.float64)
-  x = torch.tensor(lin, requires_grad=True)
-  st = opm.nbody_checkpointed(b64, opm.lpt_init(b64, x, 0.1, order=2),
-                              stages, nc)
-  rho = opm.cic_paint(torch.zeros([1] + nc, dtype=torch.float64), st[0])
-  (go,) = torch.autograd.grad(((rho - torch.tensor(target))**2).sum(), x)
-  go = go.numpy()
+  def oracle_grad(dtype):
+    b = obg.Background({}, dtype=np.float64 if dtype == torch.float64
+                       else np.float32)
+    x = torch.tensor(lin, dtype=dtype, requires_grad=True)
+    st = opm.nbody_checkpointed(b, opm.lpt_init(b, x, 0.1, order=2), stages,
+                                nc)
+    rho = opm.cic_paint(torch.zeros([1] + nc, dtype=dtype), st[0])
+    (go,) = torch.autograd.grad(
+        ((rho - torch.tensor(target, dtype=dtype))**2).sum(), x)
+    return go.double().numpy()
+
+  go = oracle_grad(torch.float64)
+  g32 = oracle_grad(torch.float32)  # the reference's own FP32 arithmetic
   _, g = _chi2_ours(fpm, lin, target, stages, nc, ckpt=5, store=store)
-  err = rel_l2(g, go)
-  dirs = []
+  err, floor = rel_l2(g, go), rel_l2(g32, go)
+  dirs, dirs32 = [], []
   for _ in range(32):
     u = rng.standard_normal(lin.shape)
     t = float(np.sum(go * u))
     dirs.append(abs(float(np.sum(g * u)) - t) / abs(t))
+    dirs32.append(abs(float(np.sum(g32 * u)) - t) / abs(t))
   with capsys.disabled():
     print('\n  adjoint 64^3 / 20 steps vs FP64 tape (stored potential %s): '
-          'rel-L2 %.2e; 32 directions: median %.2e, max %.2e' %
-          (store, err, np.median(dirs), np.max(dirs)))
-  assert err < 1e-3
-  assert np.median(dirs) < 1e-3
+          'rel-L2 %.2e, 32 directions median %.2e max %.2e; the FP32 '
+          'oracle tape: rel-L2 %.2e, median %.2e max %.2e' %
+          (store, err, np.median(dirs), np.max(dirs), floor,
+           np.median(dirs32), np.max(dirs32)))
+  # an FP32 forward of this length is chaotic at the 1e-4 level: the bar is
+  # the FP32 oracle's own distance from FP64 (and 1e-3 overall)
+  assert err < 1e-3 and err < 2 * floor
+  assert np.median(dirs) < 1e-3 and np.median(dirs) < 2 * np.median(dirs32)
