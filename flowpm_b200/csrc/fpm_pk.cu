@@ -184,8 +184,19 @@ extern "C" int fpm_pk_bin(const void* delta_k, int batch, int nx, int ny,
 }
 
 namespace {
+// R2C plans of fpm_power_spectrum per (device, batch, nx, ny, nz), at most
+// kMaxPkPlans of them: past that the least recently used one is destroyed
+// (cufftDestroy frees its work area with cudaFree, which waits for the work
+// already queued on the device).  The lock is held while a plan is bound to
+// the caller's stream and its transform is queued.
+constexpr size_t kMaxPkPlans = 8;
+struct PkPlan {
+  cufftHandle h;
+  uint64_t used;
+};
 std::mutex g_pk_mu;
-std::map<std::tuple<int, int, int, int, int>, cufftHandle> g_pk_plans;
+std::map<std::tuple<int, int, int, int, int>, PkPlan> g_pk_plans;
+uint64_t g_pk_tick = 0;
 }  // namespace
 
 extern "C" int fpm_power_spectrum(const float* field, int batch, int nx,
@@ -198,21 +209,6 @@ extern "C" int fpm_power_spectrum(const float* field, int batch, int nx,
   cudaStream_t st = (cudaStream_t)stream;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return FPM_ERR_CUDA;
-  cufftHandle h;
-  {
-    std::lock_guard<std::mutex> lk(g_pk_mu);
-    auto key = std::make_tuple(dev, batch, nx, ny, nz);
-    auto it = g_pk_plans.find(key);
-    if (it == g_pk_plans.end()) {
-      int n[3] = {nx, ny, nz};
-      if (cufftPlanMany(&h, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C,
-                        batch) != CUFFT_SUCCESS)
-        return FPM_ERR_CUFFT;
-      g_pk_plans[key] = h;
-    } else {
-      h = it->second;
-    }
-  }
   const size_t nmodes = (size_t)batch * nx * ny * (nz / 2 + 1);
   float2* spec = nullptr;
   if (cudaMallocAsync((void**)&spec, nmodes * sizeof(float2), st) !=
@@ -220,10 +216,33 @@ extern "C" int fpm_power_spectrum(const float* field, int batch, int nx,
     cudaGetLastError();
     return FPM_ERR_OOM;
   }
-  if (cufftSetStream(h, st) != CUFFT_SUCCESS ||
-      cufftExecR2C(h, (cufftReal*)field, (cufftComplex*)spec) !=
-          CUFFT_SUCCESS)
-    rc = FPM_ERR_CUFFT;
+  {
+    std::lock_guard<std::mutex> lk(g_pk_mu);
+    const auto key = std::make_tuple(dev, batch, nx, ny, nz);
+    auto it = g_pk_plans.find(key);
+    if (it == g_pk_plans.end()) {
+      if (g_pk_plans.size() >= kMaxPkPlans) {
+        auto old = g_pk_plans.begin();
+        for (auto j = g_pk_plans.begin(); j != g_pk_plans.end(); ++j)
+          if (j->second.used < old->second.used) old = j;
+        cufftDestroy(old->second.h);
+        g_pk_plans.erase(old);
+      }
+      int n[3] = {nx, ny, nz};
+      cufftHandle h;
+      if (cufftPlanMany(&h, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C,
+                        batch) != CUFFT_SUCCESS) {
+        cudaFreeAsync(spec, st);
+        return FPM_ERR_CUFFT;
+      }
+      it = g_pk_plans.emplace(key, PkPlan{h, 0}).first;
+    }
+    it->second.used = ++g_pk_tick;
+    if (cufftSetStream(it->second.h, st) != CUFFT_SUCCESS ||
+        cufftExecR2C(it->second.h, (cufftReal*)field, (cufftComplex*)spec) !=
+            CUFFT_SUCCESS)
+      rc = FPM_ERR_CUFFT;
+  }
   if (rc == FPM_OK)
     rc = fpm_pk_bin(spec, batch, nx, ny, nz, boxsize, kmin, dk, nedges,
                     power, stream);

@@ -447,7 +447,9 @@ int fpm_pk_bin_noalloc(const void* delta_k, int batch, int nx, int ny, int nz,
 
 /* From the real field (batch, nx, ny, nz): R2C then fpm_pk_bin.  The
  * cuFFT plan of each (device, batch, nx, ny, nz) is created on first use
- * and kept, with its work area, until the process exits. */
+ * and kept, with its work area; at most 8 such plans are kept, and making
+ * a ninth destroys the least recently used one (which waits for the work
+ * queued on the device). */
 int fpm_power_spectrum(const float* field, int batch, int nx, int ny, int nz,
                        const double* boxsize, double kmin, double dk,
                        int nedges, float* power, void* stream);
