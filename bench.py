@@ -53,6 +53,11 @@ KERNEL_BYTES_PER_PART = 64
 # dram__bytes_read.sum + dram__bytes_write.sum = 84.1 + 8.3 MB).
 KSTEP_TRAFFIC_BYTES_128 = {0: 92.4e6}
 L2_FLUSH_BYTES = 256 << 20
+# sort periods (in positions) of the reverse sweep over the binned particle
+# order that C4 and C5 time beside the lattice walk's, and the cell tile of
+# the keys when the forward keeps the lattice walk
+ADJ_SORT_PERIODS = (1, 2, 4)
+ADJ_TILE = 16
 # seed of replica r's linear field: replicas.replica_seed(1000, r)
 REPLICA_SEED_BASE = 1000
 # Accuracy of the C4 gradient at full size, from the offline check against
@@ -447,8 +452,18 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5):
       'traversal': list(choice),
   }
   grads = {}
-  for method in ('potential_tape', 'rebuilt'):
-    capture(method)
+  # the reverse sweep over the binned particle order (re-sorted every k
+  # positions) takes its cell tiles from the forward's binning, or, when
+  # the forward keeps the lattice walk, from tiles set for it alone
+  sorted_k = ADJ_SORT_PERIODS
+  methods = ['potential_tape', 'rebuilt'] + [
+      'potential_tape_sorted%d' % k for k in sorted_k]
+  for method in methods:
+    if method.startswith('potential_tape_sorted'):
+      if not plan.binning[0]:
+        plan.set_binning(ADJ_TILE, 1, _lib.FPM_BIN_WALK)
+      plan.set_adjoint_binning(int(method[len('potential_tape_sorted'):]))
+    capture('rebuilt' if method == 'rebuilt' else 'potential_tape')
     if method == 'potential_tape':
       forward()
       gen = torch.Generator(device='cuda').manual_seed(77)
@@ -465,13 +480,22 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5):
                    'forward_ms': ms_fwd,
                    'adjoint_over_forward': (ms - ms_fwd) / ms_fwd}
   _lib.call('fpm_nbody_set_tape', plan.handle, None, 0)
+  if sorted_k:
+    plan.set_adjoint_binning(0)
   plan.set_binning(0)
-  a, b = grads['potential_tape'].double(), grads['rebuilt'].double()
-  out['method'] = 'potential_tape'
-  out['value'] = out['potential_tape']['value']
-  out['ms_per_step'] = out['potential_tape']['ms_per_step']
+  b = grads['rebuilt'].double()
+  rel = lambda m: float((grads[m].double() - b).norm() / b.norm())
+  tape = ['potential_tape'] + ['potential_tape_sorted%d' % k
+                               for k in sorted_k]
+  best = max(tape, key=lambda m: out[m]['value'])
+  out['method'] = best
+  out['value'] = out[best]['value']
+  out['ms_per_step'] = out[best]['ms_per_step']
   out['potential_tape_gb'] = phi_tape.numel() * 4 / 1e9
-  out['lam_x_rel_l2_tape_vs_rebuilt'] = float((a - b).norm() / b.norm())
+  out['lam_x_rel_l2_tape_vs_rebuilt'] = rel('potential_tape')
+  for k in sorted_k:
+    out['lam_x_rel_l2_sorted%d_vs_rebuilt' % k] = rel(
+        'potential_tape_sorted%d' % k)
   return out
 
 
@@ -709,6 +733,52 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
               (8, 'adj_potential'), (9, 'adj_position'),
               (1, 'adj_force_solve')])
   _lib.call('fpm_plan_profile', plan.handle, 0)
+  # the same reverse sweep over the binned particle order, re-sorted every
+  # k positions (needs the forward's binning)
+  sorted_adj = None
+  if tape:
+    sorted_adj = {}
+    if not plan.binning[0]:  # tiles for the reverse sweep alone
+      plan.set_binning(ADJ_TILE, 1, _lib.FPM_BIN_WALK)
+    for k in ADJ_SORT_PERIODS[-1:]:  # the C4 sweep's longest period
+      try:
+        plan.set_adjoint_binning(k)
+      except _lib.FlowPMError as e:  # e.g. its buffers do not fit
+        sorted_adj['error'] = str(e)[:200]
+        break
+      # a changed schedule invalidates both graphs
+      _lib.lib.fpm_graph_destroy(gf)
+      _lib.lib.fpm_graph_destroy(ga)
+      gf, ga = _lib.ctypes.c_void_p(), _lib.ctypes.c_void_p()
+      _lib.call('fpm_graph_capture_nbody', plan.handle, _lib.ptr(D),
+                _lib.ptr(P), _lib.ptr(F), None, 0, _lib.ptr(ck), ckpt,
+                _lib.ctypes.byref(gf))
+      _lib.call('fpm_graph_capture_adjoint', plan.handle, _lib.ptr(D),
+                _lib.ptr(P), _lib.ptr(F), _lib.ptr(LX), _lib.ptr(LP), None,
+                _lib.ptr(ck), ckpt, _lib.ctypes.byref(ga))
+      fwd_adj()
+      t_k = _timed(fwd_adj, reps, flush)
+      status |= plan.status(st)
+      fwd_seed()
+      _lib.call('fpm_plan_profile', plan.handle, 1)
+      torch.cuda._sleep(100_000_000)
+      _lib.call('fpm_nbody_adjoint', plan.handle, _lib.ptr(D), _lib.ptr(P),
+                _lib.ptr(F), _lib.ptr(LX), _lib.ptr(LP), None, _lib.ptr(ck),
+                ckpt, st)
+      torch.cuda.synchronize()
+      kk = {}
+      for kind, name in [(6, 'adj_drift_vjp'), (10, 'sort'),
+                         (9, 'adj_position')]:
+        tot, cnt = _lib.c_double(), _lib.c_int64()
+        _lib.call('fpm_plan_profile_read', plan.handle, kind,
+                  _lib.ctypes.byref(tot), _lib.ctypes.byref(cnt))
+        if cnt.value:
+          kk[name] = {'avg_launch_ms': tot.value / cnt.value,
+                      'launches': cnt.value}
+      _lib.call('fpm_plan_profile', plan.handle, 0)
+      sorted_adj[k] = {'value': 2.0 * np_ * steps / (t_k * 1e-3),
+                       'forward_adjoint_ms': t_k, 'kernels': kk}
+    plan.set_adjoint_binning(0)
   kb, pk = fpm.power_spectrum(rho, kmin=0.01, dk=0.01, boxsize=[box] * 3)
   peak, peak_kind = peaks()
   tot_np, nc_tot = 2 * np_, 2 * np_
@@ -790,20 +860,35 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
   _lib.call('fpm_nbody_set_tape', plan.handle, None, 0)
   plan.close()
   upd = 2.0 * np_ * steps
+  method, t_best = 'potential_tape' if tape else 'rebuilt', t_all
+  for k, v in (sorted_adj or {}).items():
+    if k != 'error' and v['forward_adjoint_ms'] < t_best:
+      method, t_best = 'potential_tape_sorted%d' % k, v['forward_adjoint_ms']
+  if sorted_adj:
+    for v in sorted_adj.values():
+      a = v.get('kernels', {}).get('adj_drift_vjp') if isinstance(
+          v, dict) else None
+      if a:
+        a['achieved_gbs'] = kbytes['adj_drift_vjp'] / (
+            a['avg_launch_ms'] * 1e-3) / 1e9
+        a['frac'] = a['achieved_gbs'] / peak
   return {
       'workload': ('C5: ' if n == 512 else '') +
                   '2 x %d^3, box %g Mpc/h, %d KDK steps, forward + '
                   'reverse-time adjoint, checkpoint every %d, different '
                   'seeds and cosmologies' % (n, box, steps, ckpt),
       'forward_value': upd / (t_fwd * 1e-3),
-      'value': upd / (t_all * 1e-3),
+      'value': upd / (t_best * 1e-3),
       'unit': 'particle-updates/s (forward + adjoint)',
-      'method': 'potential_tape' if tape else 'rebuilt',
+      'method': method,
+      'lattice_walk_adjoint': {'value': upd / (t_all * 1e-3),
+                               'forward_adjoint_ms': t_all},
+      'sorted_adjoint': sorted_adj,
       'traversal': list(choice),
       'autotune_ms': tune_ms,
       'forward_ms': t_fwd,
-      'forward_adjoint_ms': t_all,
-      'sims_per_s_forward_adjoint': 2 / (t_all * 1e-3),
+      'forward_adjoint_ms': t_best,
+      'sims_per_s_forward_adjoint': 2 / (t_best * 1e-3),
       'rebuilt': rebuilt,
       'kernel_roofline': roof,
       'peak_gbs': peak,

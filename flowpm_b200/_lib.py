@@ -49,6 +49,7 @@ SIGNATURES = {
                                     P_double, c_void_p]),
     'fpm_nbody_set_pgd': (c_int, [c_void_p, c_int, P_double, c_void_p]),
     'fpm_plan_set_binning': (c_int, [c_void_p, c_int, c_int, c_int]),
+    'fpm_plan_set_adjoint_binning': (c_int, [c_void_p, c_int]),
     'fpm_plan_autotune': (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int,
                                   P_int32, ctypes.POINTER(c_float),
                                   c_void_p]),
@@ -131,6 +132,7 @@ FPM_NBODY_INTERMEDIATE = 1
 FPM_TUNE_CONFIGS = 8
 FPM_BIN_TILES = 0
 FPM_BIN_CHUNKS = 1
+FPM_BIN_WALK = 2
 FPM_STATUS_NONFINITE_POS = 1
 FPM_STATUS_NONFINITE_MOM = 2
 

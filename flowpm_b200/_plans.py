@@ -30,17 +30,31 @@ class Plan(object):
     self._work = None
     self._graphs = {}
     self.binning = (0, 1, _lib.FPM_BIN_CHUNKS)
+    self.adjoint_binning = 0
 
   def set_binning(self, tile, sort_every=1, mode=_lib.FPM_BIN_CHUNKS):
     """Binned forward step (``fpm_plan_set_binning``): particles sorted by
     force-mesh cell, keys tile-major in tiles of ``tile``^3 cells (8 or 16;
     0: the lattice walk), re-sorted every ``sort_every`` steps; ``mode``
-    FPM_BIN_CHUNKS (equal particle chunks) or FPM_BIN_TILES (one block per
-    tile, shared-memory paint).  Drops captured graphs."""
+    FPM_BIN_CHUNKS (equal particle chunks), FPM_BIN_TILES (one block per
+    tile, shared-memory paint) or FPM_BIN_WALK (the forward keeps the
+    lattice walk; tiles and buffers for ``set_adjoint_binning`` only).
+    Drops captured graphs."""
     _lib.call('fpm_plan_set_binning', self.handle, int(tile), int(sort_every),
               int(mode))
     self.binning = (int(tile), int(sort_every), int(mode)) if tile else (
         0, 1, _lib.FPM_BIN_CHUNKS)
+    for g in self._graphs.values():
+      _lib.lib.fpm_graph_destroy(g)
+    self._graphs = {}
+
+  def set_adjoint_binning(self, sort_every):
+    """Reverse sweep of a potential-tape adjoint in the binned order
+    (``fpm_plan_set_adjoint_binning``): re-sorted every ``sort_every``
+    positions, 0 for the lattice walk.  Needs binning on.  Drops captured
+    graphs."""
+    _lib.call('fpm_plan_set_adjoint_binning', self.handle, int(sort_every))
+    self.adjoint_binning = int(sort_every)
     for g in self._graphs.values():
       _lib.lib.fpm_graph_destroy(g)
     self._graphs = {}

@@ -233,6 +233,138 @@ k_adj_vjp(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
   }
 }
 
+// Per-simulation constants of one reverse position of k_adj_position.
+struct AdjPos {
+  float b, dr, ks, kep, cv, fac, invb, uf;
+  bool rec, last;
+  int64_t mcells;
+  const float* lr;
+  const float* f0;
+  float* l0;
+  const float* ckd;
+  const float* ckp;
+};
+
+// false when simulation s has no position a.it (it has fewer steps).
+__device__ __forceinline__ bool adj_pos_setup(const SimDev& S, int s,
+                                              const AdjArgs& a, AdjPos& c) {
+  const int T = a.nsteps[s];
+  if (a.it > T) return false;
+  const float* cf = a.coefs + (int64_t)s * a.max_steps * 3;
+  c.b = (float)S.bf;
+  c.rec = a.it < T;  // a.it >= 0 here
+  c.dr = c.rec ? cf[a.it * 3 + 1] : 0.f;
+  c.ks = c.rec ? cf[a.it * 3 + 0] : 0.f;
+  c.kep = a.it >= 1 ? cf[(a.it - 1) * 3 + 2] : 0.f;
+  c.cv = c.ks + c.kep;
+  c.last = !c.rec;
+  c.fac = a.ffac[s];
+  c.invb = 1.0f / c.b;
+  c.uf = c.fac * c.invb;
+  c.mcells = (int64_t)S.mx * S.my * S.mz;
+  c.lr = a.lrho + S.m_off;
+  c.f0 = a.fmesh + 3 * S.m_off;
+  c.l0 = a.lmesh + (a.lvec4 ? 4 : 3) * S.m_off;
+  const bool ck = c.rec && a.ckpt && (a.it % a.ckpt_every == 0);
+  c.ckd = ck ? a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3
+             : nullptr;
+  c.ckp = ck ? c.ckd + a.total_np * 3 : nullptr;
+  return true;
+}
+
+// One particle of k_adj_position: its state in slot `slot` of the
+// per-particle arrays, its lattice site (i, j, k), and g its Lagrangian
+// slot in the checkpoints and lam_f.
+__device__ __forceinline__ void adj_position_one(const SimDev& S,
+                                                 const AdjArgs& a,
+                                                 const AdjPos& c, int64_t slot,
+                                                 int64_t g, int i, int j,
+                                                 int k) {
+  float3 d = ld3(a.disp, slot);
+  float3 lx = ld3(a.lam_x, slot);
+  float3 lp = ld3(a.lam_p, slot);
+  // rec: p_half of step it (left by the position after); else p_T
+  const float3 ph = ld3(a.mom, slot);
+  if (c.rec) {  // reverse drift from x_{it+1} (k_adj_drift_paint)
+    const float3 gg = gather_grad(c.lr, S.mx, S.my, S.mz,
+                                  mesh_pos(S, i, j, k, d));
+    lx.x += c.b * gg.x;
+    lx.y += c.b * gg.y;
+    lx.z += c.b * gg.z;
+    d = make_float3(__fsub_rn(d.x, __fmul_rn(c.dr, ph.x)),
+                    __fsub_rn(d.y, __fmul_rn(c.dr, ph.y)),
+                    __fsub_rn(d.z, __fmul_rn(c.dr, ph.z)));
+    if (c.ckd) d = ld3(c.ckd, g);
+    lp.x += c.dr * lx.x;
+    lp.y += c.dr * lx.y;
+    lp.z += c.dr * lx.z;
+    st3(a.disp, slot, d);
+    st3(a.lam_p, slot, lp);
+  }
+  // force VJP at x_it (k_adj_vjp)
+  float3 v = make_float3(c.cv * lp.x, c.cv * lp.y, c.cv * lp.z);
+  if (c.last && a.lam_f) {
+    const float3 lf = ld3(a.lam_f, g);
+    v.x += lf.x;
+    v.y += lf.y;
+    v.z += lf.z;
+  }
+  const float3 y = mesh_pos(S, i, j, k, d);
+  if (!finite3(y.x, y.y, y.z)) atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
+  const Axis ax = cic_axis(y.x, S.mx), ay = cic_axis(y.y, S.my),
+             az = cic_axis(y.z, S.mz);
+  const DAxis dx = cic_daxis(y.x), dy = cic_daxis(y.y), dz = cic_daxis(y.z);
+  float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+  float3 acc = make_float3(0.f, 0.f, 0.f);
+  const float u0 = c.uf * v.x, u1 = c.uf * v.y, u2 = c.uf * v.z;
+  // 32-bit offsets inside the simulation's mesh (< 2^31 cells)
+  const unsigned my = S.my, mz = S.mz;
+  const unsigned rx0 = (unsigned)ax.i0 * my, rx1 = (unsigned)ax.i1 * my;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int cx = conn_x(q), cy = conn_y(q), cz = conn_z(q);
+    const float wc = cic_w(ax, ay, az, cx, cy, cz);
+    const unsigned o =
+        ((cx ? rx1 : rx0) + (unsigned)(cy ? ay.i1 : ay.i0)) * mz +
+        (unsigned)(cz ? az.i1 : az.i0);
+    const float a0 = __ldg(c.f0 + o), a1 = __ldg(c.f0 + c.mcells + o),
+                a2 = __ldg(c.f0 + 2 * c.mcells + o);
+    r0 = __fadd_rn(r0, __fmul_rn(a0, wc));
+    r1 = __fadd_rn(r1, __fmul_rn(a1, wc));
+    r2 = __fadd_rn(r2, __fmul_rn(a2, wc));
+    grad_acc(ax, ay, az, dx, dy, dz, cx, cy, cz,
+             v.x * a0 + v.y * a1 + v.z * a2, acc);
+    if (a.lvec4) {
+      red_add_v4(c.l0 + 4 * o, u0 * wc, u1 * wc, u2 * wc);
+    } else {
+      red_add(c.l0 + o, u0 * wc);
+      red_add(c.l0 + c.mcells + o, u1 * wc);
+      red_add(c.l0 + 2 * c.mcells + o, u2 * wc);
+    }
+  }
+  const float3 f = make_float3(__fmul_rn(__fmul_rn(r0, c.fac), c.invb),
+                               __fmul_rn(__fmul_rn(r1, c.fac), c.invb),
+                               __fmul_rn(__fmul_rn(r2, c.fac), c.invb));
+  lx.x += c.fac * acc.x;
+  lx.y += c.fac * acc.y;
+  lx.z += c.fac * acc.z;
+  st3(a.lam_x, slot, lx);
+  // p_it (rec: p_half - ks F_it, or the checkpoint; else p_T), then
+  // p_half of step it-1 for the next position
+  float3 p = ph;
+  if (c.rec) {
+    p = make_float3(__fsub_rn(ph.x, __fmul_rn(c.ks, f.x)),
+                    __fsub_rn(ph.y, __fmul_rn(c.ks, f.y)),
+                    __fsub_rn(ph.z, __fmul_rn(c.ks, f.z)));
+    if (c.ckp) p = ld3(c.ckp, g);
+  }
+  if (a.it >= 1)
+    p = make_float3(__fsub_rn(p.x, __fmul_rn(c.kep, f.x)),
+                    __fsub_rn(p.y, __fmul_rn(c.kep, f.y)),
+                    __fsub_rn(p.z, __fmul_rn(c.kep, f.z)));
+  if (c.rec || a.it >= 1) st3(a.mom, slot, p);
+}
+
 // k_adj_drift_paint (without its paint) and k_adj_vjp of the same position
 // it in one pass over the particles, for reverse sweeps whose force meshes
 // of x_it are ready before the reverse drift (the stencil of a stored
@@ -249,28 +381,8 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const int s = find_sim(sims, nsims, ch, kTraverse);
     const SimDev S = sims[s];
-    const int T = a.nsteps[s];
-    if (a.it > T) continue;
-    const float* cf = a.coefs + (int64_t)s * a.max_steps * 3;
-    const float b = (float)S.bf;
-    const bool rec = a.it < T;  // a.it >= 0 here
-    const float dr = rec ? cf[a.it * 3 + 1] : 0.f;
-    const float ks = rec ? cf[a.it * 3 + 0] : 0.f;
-    const float kep = a.it >= 1 ? cf[(a.it - 1) * 3 + 2] : 0.f;
-    const float cv = ks + kep;
-    const bool last = !rec;
-    const float fac = a.ffac[s];
-    const float invb = 1.0f / b;
-    const float uf = fac * invb;
-    const int64_t mcells = (int64_t)S.mx * S.my * S.mz;
-    const float* lr = a.lrho + S.m_off;
-    const float* f0 = a.fmesh + 3 * S.m_off;
-    float* l0 = a.lmesh + (a.lvec4 ? 4 : 3) * S.m_off;
-    const bool ck = rec && a.ckpt && (a.it % a.ckpt_every == 0);
-    const float* ckd =
-        ck ? a.ckpt + (int64_t)(a.it / a.ckpt_every) * 2 * a.total_np * 3
-           : nullptr;
-    const float* ckp = ck ? ckd + a.total_np * 3 : nullptr;
+    AdjPos c;
+    if (!adj_pos_setup(S, s, a, c)) continue;
     const Walk w = walk_chunk(S, ch - traverse_first(S));
 #pragma unroll 1
     for (int item = 0; item < S.wi; ++item) {
@@ -278,90 +390,37 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       int64_t local;
       if (!walk_particle(S, w, item, i, j, k, local)) continue;
       const int64_t g = S.p_off + local;
-      float3 d = ld3(a.disp, g);
-      float3 lx = ld3(a.lam_x, g);
-      float3 lp = ld3(a.lam_p, g);
-      // rec: p_half of step it (left by the position after); else p_T
-      const float3 ph = ld3(a.mom, g);
-      if (rec) {  // reverse drift from x_{it+1} (k_adj_drift_paint)
-        const float3 gg = gather_grad(lr, S.mx, S.my, S.mz,
-                                      mesh_pos(S, i, j, k, d));
-        lx.x += b * gg.x;
-        lx.y += b * gg.y;
-        lx.z += b * gg.z;
-        d = make_float3(__fsub_rn(d.x, __fmul_rn(dr, ph.x)),
-                        __fsub_rn(d.y, __fmul_rn(dr, ph.y)),
-                        __fsub_rn(d.z, __fmul_rn(dr, ph.z)));
-        if (ckd) d = ld3(ckd, g);
-        lp.x += dr * lx.x;
-        lp.y += dr * lx.y;
-        lp.z += dr * lx.z;
-        st3(a.disp, g, d);
-        st3(a.lam_p, g, lp);
-      }
-      // force VJP at x_it (k_adj_vjp)
-      float3 v = make_float3(cv * lp.x, cv * lp.y, cv * lp.z);
-      if (last && a.lam_f) {
-        const float3 lf = ld3(a.lam_f, g);
-        v.x += lf.x;
-        v.y += lf.y;
-        v.z += lf.z;
-      }
-      const float3 y = mesh_pos(S, i, j, k, d);
-      if (!finite3(y.x, y.y, y.z)) atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
-      const Axis ax = cic_axis(y.x, S.mx), ay = cic_axis(y.y, S.my),
-                 az = cic_axis(y.z, S.mz);
-      const DAxis dx = cic_daxis(y.x), dy = cic_daxis(y.y),
-                  dz = cic_daxis(y.z);
-      float r0 = 0.f, r1 = 0.f, r2 = 0.f;
-      float3 acc = make_float3(0.f, 0.f, 0.f);
-      const float u0 = uf * v.x, u1 = uf * v.y, u2 = uf * v.z;
-      // 32-bit offsets inside the simulation's mesh (< 2^31 cells)
-      const unsigned my = S.my, mz = S.mz;
-      const unsigned rx0 = (unsigned)ax.i0 * my, rx1 = (unsigned)ax.i1 * my;
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const int cx = conn_x(c), cy = conn_y(c), cz = conn_z(c);
-        const float wc = cic_w(ax, ay, az, cx, cy, cz);
-        const unsigned o =
-            ((cx ? rx1 : rx0) + (unsigned)(cy ? ay.i1 : ay.i0)) * mz +
-            (unsigned)(cz ? az.i1 : az.i0);
-        const float a0 = __ldg(f0 + o), a1 = __ldg(f0 + mcells + o),
-                    a2 = __ldg(f0 + 2 * mcells + o);
-        r0 = __fadd_rn(r0, __fmul_rn(a0, wc));
-        r1 = __fadd_rn(r1, __fmul_rn(a1, wc));
-        r2 = __fadd_rn(r2, __fmul_rn(a2, wc));
-        grad_acc(ax, ay, az, dx, dy, dz, cx, cy, cz,
-                 v.x * a0 + v.y * a1 + v.z * a2, acc);
-        if (a.lvec4) {
-          red_add_v4(l0 + 4 * o, u0 * wc, u1 * wc, u2 * wc);
-        } else {
-          red_add(l0 + o, u0 * wc);
-          red_add(l0 + mcells + o, u1 * wc);
-          red_add(l0 + 2 * mcells + o, u2 * wc);
-        }
-      }
-      const float3 f = make_float3(__fmul_rn(__fmul_rn(r0, fac), invb),
-                                   __fmul_rn(__fmul_rn(r1, fac), invb),
-                                   __fmul_rn(__fmul_rn(r2, fac), invb));
-      lx.x += fac * acc.x;
-      lx.y += fac * acc.y;
-      lx.z += fac * acc.z;
-      st3(a.lam_x, g, lx);
-      // p_it (rec: p_half - ks F_it, or the checkpoint; else p_T), then
-      // p_half of step it-1 for the next position
-      float3 p = ph;
-      if (rec) {
-        p = make_float3(__fsub_rn(ph.x, __fmul_rn(ks, f.x)),
-                        __fsub_rn(ph.y, __fmul_rn(ks, f.y)),
-                        __fsub_rn(ph.z, __fmul_rn(ks, f.z)));
-        if (ckp) p = ld3(ckp, g);
-      }
-      if (a.it >= 1)
-        p = make_float3(__fsub_rn(p.x, __fmul_rn(kep, f.x)),
-                        __fsub_rn(p.y, __fmul_rn(kep, f.y)),
-                        __fsub_rn(p.z, __fmul_rn(kep, f.z)));
-      if (rec || a.it >= 1) st3(a.mom, g, p);
+      adj_position_one(S, a, c, g, g, i, j, k);
+    }
+  }
+}
+
+// k_adj_position over the particles in their binned order (sorted by the
+// cell of x_{it+1}, or of a later position, keys tile-major): chunks of
+// kChunk consecutive slots of one simulation.  Consecutive lanes then sit
+// in the same or neighbouring cells, so the gathers and the vector
+// reductions of a warp touch few L2 sectors at every time, where the
+// lattice walk's warps spread over more and more of them as structure
+// grows.  Per particle the arithmetic is k_adj_position's.
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
+k_adj_position_sorted(const SimDev* __restrict__ sims, int nsims,
+                      int64_t nchunks, AdjArgs a) {
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int s = find_sim(sims, nsims, ch, kPart);
+    const SimDev S = sims[s];
+    AdjPos c;
+    if (!adj_pos_setup(S, s, a, c)) continue;
+    const int64_t first = S.p_off + (ch - S.ch_p) * kChunk;
+    const int64_t end = S.p_off + S.np;
+#pragma unroll 1
+    for (int item = 0; item < kItems; ++item) {
+      const int64_t i = first + item * kThreads + threadIdx.x;
+      if (i >= end) break;
+      const uint32_t l = a.lag[i];
+      int qi, qj, qk;
+      lattice_ijk(S, l, qi, qj, qk);
+      adj_position_one(S, a, c, i, S.p_off + l, qi, qj, qk);
     }
   }
 }
@@ -695,6 +754,14 @@ void launch_adj_position(const SimDev* sims, int nsims, int64_t nchunks,
   else
     k_adj_position<FPM_STEP_MINBLOCKS>
         <<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
+}
+
+void launch_adj_position_sorted(const SimDev* sims, int nsims,
+                                int64_t nchunks, const AdjArgs& a,
+                                cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_adj_position_sorted<FPM_ADJ_SORTED_MINBLOCKS>
+      <<<grid_for(nchunks), kThreads, 0, st>>>(sims, nsims, nchunks, a);
 }
 
 void launch_adj_fourier(const SimDev* sims, int nsims, int64_t nchunks,

@@ -7,6 +7,9 @@ namespace fpm {
 
 struct AdjArgs {
   float* disp;            // (total_np, 3) displacement, reconstructed in place
+                          // (the per-particle arrays disp, mom, lam_x,
+                          // lam_p are in Lagrangian order, or with lag set
+                          // in the binned order of launch_adj_position_sorted)
   float* mom;             // (total_np, 3) momentum, reconstructed in place
   float* lam_x;           // (total_np, 3) dL/dX
   float* lam_p;           // (total_np, 3) dL/dp
@@ -29,6 +32,7 @@ struct AdjArgs {
   const float* ckpt;      // checkpoint slots (d, p) or null
   int ckpt_every;
   int32_t* status;
+  const uint32_t* lag;    // binned order: Lagrangian index of each slot
   int64_t total_np;
   int max_steps;
   int it;
@@ -44,6 +48,13 @@ void launch_adj_vjp(const SimDev* sims, int nsims, int64_t nchunks,
 // position (a.it >= 0), in one pass; the force meshes of x_it must be ready.
 void launch_adj_position(const SimDev* sims, int nsims, int64_t nchunks,
                          const AdjArgs& a, cudaStream_t st);
+// launch_adj_position over particles kept sorted by cell (the binned order
+// of fpm_bin.cu): the particle chunks [0, nchunks) of the plan, slot i of
+// disp, mom, lam_x and lam_p holding Lagrangian particle a.lag[i] of its
+// simulation; checkpoints and lam_f are read in Lagrangian order.
+void launch_adj_position_sorted(const SimDev* sims, int nsims,
+                                int64_t nchunks, const AdjArgs& a,
+                                cudaStream_t st);
 // The PGD move of step a.it (x' -> x_{it+1}) in reverse, sims with
 // nsteps > a.it: lam_x += B sum_c lam_rho[c] grad W at x_{it+1} (the force
 // paint adjoint), then at x' = q + pgd_disp with the PGD displacement

@@ -80,28 +80,43 @@ k_bin_count(BinRun R, const float* __restrict__ d,
 }
 
 // Scatter: slot = off[key]++ (warp-aggregated, lanes of equal keys keep
-// their order); writes d, p and the Lagrangian index to the output arrays.
-template <int T>
+// their order); writes the NP float3 arrays of the payload (the first is
+// the displacement the keys come from) and the Lagrangian index to the
+// output arrays.
+template <int T, int NP>
 __global__ void __launch_bounds__(256)
-k_bin_scatter(BinRun R, const float* __restrict__ d,
-              const float* __restrict__ p, const uint32_t* __restrict__ lag,
-              int32_t* __restrict__ off, float* __restrict__ d_out,
-              float* __restrict__ p_out, uint32_t* __restrict__ lag_out) {
+k_bin_scatter(BinRun R, BinPayload pay, const uint32_t* __restrict__ lag,
+              int32_t* __restrict__ off, uint32_t* __restrict__ lag_out) {
   const int64_t n = (int64_t)R.count * R.np;
   const int lane = threadIdx.x & 31;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x) {
     uint32_t l;
-    const uint64_t key = particle_key<T>(R, d, lag, t, l);
+    const uint64_t key = particle_key<T>(R, pay.src[0], lag, t, l);
     const unsigned m = __match_any_sync(__activemask(), key);
     const int leader = __ffs(m) - 1;
     int base = 0;
     if (lane == leader) base = atomicAdd(off + R.m0 + key, (int32_t)__popc(m));
     base = __shfl_sync(m, base, leader);
     const int64_t dst = base + __popc(m & ((1u << lane) - 1));
-    st3(d_out, dst, ld3(d, R.p0 + t));
-    st3(p_out, dst, ld3(p, R.p0 + t));
+#pragma unroll
+    for (int q = 0; q < NP; ++q) st3(pay.dst[q], dst, ld3(pay.src[q], R.p0 + t));
     lag_out[dst] = l;
+  }
+}
+
+// Back to Lagrangian order: slot p0 + t, holding lattice site lag of
+// simulation r = t / np of the run, goes to p0 + r np + lag.
+template <int NP>
+__global__ void __launch_bounds__(256)
+k_bin_unsort(BinRun R, BinPayload pay, const uint32_t* __restrict__ lag) {
+  const int64_t n = (int64_t)R.count * R.np;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = t / R.np;
+    const int64_t g = R.p0 + r * R.np + lag[R.p0 + t];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) st3(pay.dst[q], g, ld3(pay.src[q], R.p0 + t));
   }
 }
 
@@ -508,34 +523,75 @@ size_t bin_scan_blocks(int64_t ncells) {
   return (size_t)((ncells + kScanChunk - 1) / kScanChunk);
 }
 
-int launch_bin_sort(int tile, const BinRun& R, const float* d,
-                    const float* p, const uint32_t* lag, int32_t* cell,
-                    int32_t* sums, float* d_out, float* p_out,
+namespace {
+
+int64_t sort_blocks(int64_t n) {
+  int64_t blocks = (n + 255) / 256;
+  const int64_t cap = (int64_t)kNumSMs * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return blocks;
+}
+
+template <int NP>
+void launch_scatter(int tile, unsigned blocks, const BinRun& R,
+                    const BinPayload& pay, const uint32_t* lag, int32_t* cell,
                     uint32_t* lag_out, cudaStream_t st) {
+  if (tile == 8)
+    k_bin_scatter<8, NP><<<blocks, 256, 0, st>>>(R, pay, lag, cell, lag_out);
+  else
+    k_bin_scatter<16, NP><<<blocks, 256, 0, st>>>(R, pay, lag, cell, lag_out);
+}
+
+}  // namespace
+
+int launch_bin_sort(int tile, const BinRun& R, const BinPayload& pay,
+                    const uint32_t* lag, int32_t* cell, int32_t* sums,
+                    uint32_t* lag_out, cudaStream_t st) {
+  if (pay.n != 2 && pay.n != 4) return FPM_ERR_ARG;
   const int64_t ncells = (int64_t)R.count * R.ncell;
   const int64_t n = (int64_t)R.count * R.np;
   if (cudaMemsetAsync(cell + R.m0, 0, sizeof(int32_t) * ncells, st) !=
       cudaSuccess)
     return FPM_ERR_CUDA;
-  int64_t blocks = (n + 255) / 256;
-  const int64_t cap = (int64_t)kNumSMs * 16;
-  if (blocks > cap) blocks = cap;
-  if (blocks < 1) blocks = 1;
+  const unsigned blocks = (unsigned)sort_blocks(n);
   g_launches.fetch_add(5, std::memory_order_relaxed);
   if (tile == 8)
-    k_bin_count<8><<<(unsigned)blocks, 256, 0, st>>>(R, d, lag, cell);
+    k_bin_count<8><<<blocks, 256, 0, st>>>(R, pay.src[0], lag, cell);
   else
-    k_bin_count<16><<<(unsigned)blocks, 256, 0, st>>>(R, d, lag, cell);
+    k_bin_count<16><<<blocks, 256, 0, st>>>(R, pay.src[0], lag, cell);
   const int nb = (int)bin_scan_blocks(ncells);
   k_scan_sums<<<nb, kScanThreads, 0, st>>>(cell + R.m0, ncells, sums);
   k_scan_top<<<1, 1024, 0, st>>>(sums, nb, (int32_t)R.p0);
   k_scan_apply<<<nb, kScanThreads, 0, st>>>(cell + R.m0, ncells, sums);
-  if (tile == 8)
-    k_bin_scatter<8><<<(unsigned)blocks, 256, 0, st>>>(
-        R, d, p, lag, cell, d_out, p_out, lag_out);
+  if (pay.n == 2)
+    launch_scatter<2>(tile, blocks, R, pay, lag, cell, lag_out, st);
   else
-    k_bin_scatter<16><<<(unsigned)blocks, 256, 0, st>>>(
-        R, d, p, lag, cell, d_out, p_out, lag_out);
+    launch_scatter<4>(tile, blocks, R, pay, lag, cell, lag_out, st);
+  return cudaGetLastError() == cudaSuccess ? FPM_OK : FPM_ERR_CUDA;
+}
+
+int launch_bin_sort(int tile, const BinRun& R, const float* d,
+                    const float* p, const uint32_t* lag, int32_t* cell,
+                    int32_t* sums, float* d_out, float* p_out,
+                    uint32_t* lag_out, cudaStream_t st) {
+  BinPayload pay;
+  pay.n = 2;
+  pay.src[0] = d;
+  pay.src[1] = p;
+  pay.dst[0] = d_out;
+  pay.dst[1] = p_out;
+  pay.src[2] = pay.src[3] = nullptr;
+  pay.dst[2] = pay.dst[3] = nullptr;
+  return launch_bin_sort(tile, R, pay, lag, cell, sums, lag_out, st);
+}
+
+int launch_bin_unsort(const BinRun& R, const BinPayload& pay,
+                      const uint32_t* lag, cudaStream_t st) {
+  if (pay.n != 4) return FPM_ERR_ARG;
+  const unsigned blocks = (unsigned)sort_blocks((int64_t)R.count * R.np);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_bin_unsort<4><<<blocks, 256, 0, st>>>(R, pay, lag);
   return cudaGetLastError() == cudaSuccess ? FPM_OK : FPM_ERR_CUDA;
 }
 

@@ -17,6 +17,15 @@ struct BinRun {
   int64_t np, ncell, p0, m0;
 };
 
+// Particle arrays a sort moves: n float3 arrays (2: displacement and
+// momentum; 4: displacement, momentum and the two cotangents of the
+// reverse sweep), src[0] the displacement the cell keys come from.
+struct BinPayload {
+  int n;
+  const float* src[4];
+  float* dst[4];
+};
+
 // Tile sizes the binned step is built for (8 or 16 cells per side) and
 // whether a force mesh divides into them.
 bool bin_tile_supported(int tile, int mx, int my, int mz);
@@ -34,6 +43,16 @@ int launch_bin_sort(int tile, const BinRun& R, const float* d,
                     const float* p, const uint32_t* lag, int32_t* cell,
                     int32_t* sums, float* d_out, float* p_out,
                     uint32_t* lag_out, cudaStream_t st);
+
+// The same sort of the payload's arrays.
+int launch_bin_sort(int tile, const BinRun& R, const BinPayload& pay,
+                    const uint32_t* lag, int32_t* cell, int32_t* sums,
+                    uint32_t* lag_out, cudaStream_t st);
+
+// Sorted slots back to Lagrangian order (payload of 4 arrays): slot p0 + t
+// with Lagrangian index lag[p0 + t] goes to p0 + (t / np) np + lag.
+int launch_bin_unsort(const BinRun& R, const BinPayload& pay,
+                      const uint32_t* lag, cudaStream_t st);
 
 // State of the binned step: the sorted particles (updated in place), their
 // Lagrangian indices and the cells' end slots of the last sort.  The

@@ -290,6 +290,10 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b,
 #ifndef FPM_ADJ_MINBLOCKS
 #define FPM_ADJ_MINBLOCKS 3
 #endif
+// Resident blocks of k_adj_position over the binned particle order.
+#ifndef FPM_ADJ_SORTED_MINBLOCKS
+#define FPM_ADJ_SORTED_MINBLOCKS 3
+#endif
 // Programmatic dependent launch (sm_90 and later).  A kernel launched by
 // launch_pdl may be scheduled as soon as its predecessor in the stream
 // completes, without the launch gap; pdl_wait() (first statement of such

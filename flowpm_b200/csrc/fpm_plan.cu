@@ -147,6 +147,14 @@ struct fpm_plan {
   int32_t* bcell = nullptr;
   int32_t* bsums = nullptr;
   size_t bin_bytes = 0;
+  // the reverse sweep in the binned order (fpm_plan_set_adjoint_binning):
+  // sort period in positions (0: the lattice walk) and the sorted
+  // cotangents (lam_x, lam_p) in two buffers; the state uses bd / bp
+  int adj_every = 0;
+  int adj_req = 0;  // the period asked for, kept across tile changes
+  float* blx[2] = {nullptr, nullptr};
+  float* blp[2] = {nullptr, nullptr};
+  size_t adj_bin_bytes = 0;
   // optional per-kernel timing (fpm_plan_profile)
   bool profile = false;
   std::vector<cudaEvent_t> ev[kProfKinds];
@@ -219,8 +227,9 @@ void free_all(fpm_plan* p) {
                   p->lmesh,  p->lrho,   p->fpart,   p->phi};
   for (void* b : bufs)
     if (b) cudaFree(b);
-  void* bins[] = {p->bd[0], p->bd[1], p->bp[0], p->bp[1], p->blag[0],
-                  p->blag[1], p->bcell, p->bsums};
+  void* bins[] = {p->bd[0],   p->bd[1],  p->bp[0],  p->bp[1],
+                  p->blag[0], p->blag[1], p->bcell,  p->bsums,
+                  p->blx[0],  p->blx[1], p->blp[0], p->blp[1]};
   for (void* b : bins)
     if (b) cudaFree(b);
 }
@@ -1191,7 +1200,8 @@ extern "C" int fpm_nbody_run(fpm_plan* p, float* disp, float* mom,
   prof_mark(p, 2, st);
   FPM_TRY(launch_ok());
   if (p->tape && p->tape_floats < tape_needed(p)) return FPM_ERR_ARG;
-  if (p->bin_tile && !p->pgd_on) return nbody_binned(p, a, st);
+  if (p->bin_tile && p->bin_mode != FPM_BIN_WALK && !p->pgd_on)
+    return nbody_binned(p, a, st);
   if (chains_ok(p)) return nbody_chains(p, a, st);
   for (int it = 0; it <= p->max_steps; ++it) {
     FPM_TRY(force_meshes(p, st, it < p->max_steps, it,
@@ -1265,7 +1275,35 @@ extern "C" int fpm_nbody_set_pgd(fpm_plan* p, int enable, const double* params,
 
 namespace {
 
+void free_adj_bins(fpm_plan* p) {
+  void* bins[] = {p->blx[0], p->blx[1], p->blp[0], p->blp[1]};
+  for (void* b : bins)
+    if (b) cudaFree(b);
+  p->blx[0] = p->blx[1] = p->blp[0] = p->blp[1] = nullptr;
+  p->device_bytes -= p->adj_bin_bytes;
+  p->adj_bin_bytes = 0;
+  p->adj_every = 0;
+}
+
+int alloc_adj_bins(fpm_plan* p) {
+  bool ok = true;
+  size_t tot = 0;
+  for (int b = 0; b < 2; ++b) {
+    p->blx[b] = dalloc<float>(3 * p->total_np, tot, ok);
+    p->blp[b] = dalloc<float>(3 * p->total_np, tot, ok);
+  }
+  p->adj_bin_bytes = tot;
+  p->device_bytes += tot;
+  if (!ok) {
+    cudaGetLastError();
+    free_adj_bins(p);
+    return FPM_ERR_OOM;
+  }
+  return FPM_OK;
+}
+
 void free_bins(fpm_plan* p) {
+  free_adj_bins(p);
   void* bins[] = {p->bd[0], p->bd[1], p->bp[0], p->bp[1], p->blag[0],
                   p->blag[1], p->bcell, p->bsums};
   for (void* b : bins)
@@ -1282,7 +1320,8 @@ void free_bins(fpm_plan* p) {
 extern "C" int fpm_plan_set_binning(fpm_plan* p, int tile, int sort_every,
                                     int mode) {
   if (!p || tile < 0 || sort_every < 1 ||
-      (mode != FPM_BIN_TILES && mode != FPM_BIN_CHUNKS))
+      (mode != FPM_BIN_TILES && mode != FPM_BIN_CHUNKS &&
+       mode != FPM_BIN_WALK))
     return FPM_ERR_ARG;
   if (tile == 0) {
     if (p->bin_tile) {
@@ -1306,7 +1345,11 @@ extern "C" int fpm_plan_set_binning(fpm_plan* p, int tile, int sort_every,
     return FPM_OK;
   }
   if (cudaDeviceSynchronize() != cudaSuccess) return FPM_ERR_CUDA;
+  // the old tile's buffers go first; until the new ones exist the plan
+  // takes the lattice walk (also when their allocation fails below)
   free_bins(p);
+  p->bin_tile = 0;
+  p->sched_gen++;
   std::vector<SimDev> sims = p->sims;
   int64_t tiles = 0;
   for (SimDev& S : sims) {
@@ -1349,6 +1392,32 @@ extern "C" int fpm_plan_set_binning(fpm_plan* p, int tile, int sort_every,
   p->bin_every = sort_every;
   p->bin_mode = mode;
   p->sched_gen++;
+  // a reverse sweep in the binned order asked for before keeps it, if its
+  // buffers fit (else it takes the lattice walk)
+  if (p->adj_req > 0 && alloc_adj_bins(p) == FPM_OK) p->adj_every = p->adj_req;
+  return FPM_OK;
+}
+
+extern "C" int fpm_plan_set_adjoint_binning(fpm_plan* p, int sort_every) {
+  if (!p || sort_every < 0) return FPM_ERR_ARG;
+  if (!(p->flags & FPM_PLAN_ADJOINT)) return FPM_ERR_STATE;
+  if (sort_every == 0) {
+    p->adj_req = 0;
+    if (p->adj_bin_bytes) {
+      if (cudaDeviceSynchronize() != cudaSuccess) return FPM_ERR_CUDA;
+      free_adj_bins(p);
+      p->sched_gen++;
+    }
+    return FPM_OK;
+  }
+  if (!p->bin_tile) return FPM_ERR_STATE;  // the order comes from the tiles
+  if (!p->adj_bin_bytes) {
+    if (cudaDeviceSynchronize() != cudaSuccess) return FPM_ERR_CUDA;
+    FPM_TRY(alloc_adj_bins(p));
+  }
+  p->adj_req = sort_every;
+  if (p->adj_every != sort_every) p->sched_gen++;
+  p->adj_every = sort_every;
   return FPM_OK;
 }
 
@@ -1517,6 +1586,81 @@ static int adjoint_step(fpm_plan* p, AdjArgs& a, int it, cudaStream_t st) {
   return FPM_OK;
 }
 
+// Sort of the reverse sweep's particle arrays of run k from src (lag NULL:
+// the caller's Lagrangian order) into the plan's buffer set dst.
+static int adj_sort_run(fpm_plan* p, size_t k, float* const src[4],
+                        const uint32_t* lag, int dst, cudaStream_t st) {
+  const Run& r = p->runs[k];
+  BinPayload pay;
+  pay.n = 4;
+  for (int q = 0; q < 4; ++q) pay.src[q] = src[q];
+  pay.dst[0] = p->bd[dst];
+  pay.dst[1] = p->bp[dst];
+  pay.dst[2] = p->blx[dst];
+  pay.dst[3] = p->blp[dst];
+  return launch_bin_sort(p->bin_tile, bin_run(p, r), pay, lag, p->bcell,
+                         p->bsums + r.bsum_off, p->blag[dst], st);
+}
+
+// The reverse sweep of a potential-tape plan in the binned order: the
+// caller's Lagrangian (d, p, lam_x, lam_p) are sorted by the cell of the
+// final position, every position runs k_adj_position over the sorted
+// slots, the particles are re-sorted by their current cell every
+// adj_every positions, and after position 0 they go back to the caller's
+// arrays in Lagrangian order for the last gather (a.it = -1).
+static int adjoint_binned(fpm_plan* p, AdjArgs a, cudaStream_t st) {
+  float* user[4] = {a.disp, a.mom, a.lam_x, a.lam_p};
+  for (size_t k = 0; k < p->runs.size(); ++k)
+    FPM_TRY(adj_sort_run(p, k, user, nullptr, 0, st));
+  int cur = 0;
+  const size_t lbytes = sizeof(float) * 4 * p->total_m;
+  for (int it = p->max_steps; it >= 0; --it) {
+    a.it = it;
+    a.disp = p->bd[cur];
+    a.mom = p->bp[cur];
+    a.lam_x = p->blx[cur];
+    a.lam_p = p->blp[cur];
+    a.lag = p->blag[cur];
+    prof_mark(p, 9, st);
+    prof_mark(p, 1, st);
+    stencil_grad(p, tape_phi(p, it), p->d_nsteps, it, 0, st);
+    prof_mark(p, 1, st);
+    FPM_TRY(launch_ok());
+    if (!p->all_xpass) FPM_CUDA(cudaMemsetAsync(p->lmesh, 0, lbytes, st));
+    prof_mark(p, 6, st);
+    launch_adj_position_sorted(p->d_sims, p->nsims, p->ch_p, a, st);
+    prof_mark(p, 6, st);
+    FPM_TRY(launch_ok());
+    FPM_TRY(adjoint_density(p, it, plan_green(p), st));
+    prof_mark(p, 9, st);
+    if (it > 0 && (p->max_steps - it + 1) % p->adj_every == 0) {
+      prof_mark(p, 10, st);
+      float* src[4] = {p->bd[cur], p->bp[cur], p->blx[cur], p->blp[cur]};
+      for (size_t k = 0; k < p->runs.size(); ++k)
+        FPM_TRY(adj_sort_run(p, k, src, p->blag[cur], 1 - cur, st));
+      prof_mark(p, 10, st);
+      cur = 1 - cur;
+    }
+  }
+  BinPayload pay;
+  pay.n = 4;
+  pay.src[0] = p->bd[cur];
+  pay.src[1] = p->bp[cur];
+  pay.src[2] = p->blx[cur];
+  pay.src[3] = p->blp[cur];
+  for (int q = 0; q < 4; ++q) pay.dst[q] = user[q];
+  for (size_t k = 0; k < p->runs.size(); ++k)
+    FPM_TRY(launch_bin_unsort(bin_run(p, p->runs[k]), pay, p->blag[cur], st));
+  a.disp = user[0];
+  a.mom = user[1];
+  a.lam_x = user[2];
+  a.lam_p = user[3];
+  a.lag = nullptr;
+  a.it = -1;
+  launch_adj_drift_paint(p->d_sims, p->nsims, traverse_chunks(p), a, st);
+  return launch_ok();
+}
+
 extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
                                  const float* force, float* lam_x,
                                  float* lam_p, const float* lam_f,
@@ -1556,6 +1700,7 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
   a.ckpt = ckpt;
   a.ckpt_every = ckpt ? ckpt_every : 1;
   a.status = p->d_status;
+  a.lag = nullptr;
   a.total_np = p->total_np;
   a.max_steps = p->max_steps;
   {
@@ -1564,6 +1709,8 @@ extern "C" int fpm_nbody_adjoint(fpm_plan* p, float* disp, float* mom,
       if (S.wi >= 16) long_np += S.np;
     a.long_walk = 2 * long_np > p->total_np ? 1 : 0;
   }
+  if (p->tape && p->adj_every > 0 && p->bin_tile && !p->pgd_on)
+    return adjoint_binned(p, a, st);
   for (int it = p->max_steps; it >= 0; --it) {
     a.it = it;
     prof_mark(p, 9, st);

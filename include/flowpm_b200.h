@@ -241,15 +241,35 @@ int fpm_pgd(fpm_plan* plan, float* disp, const double* params, void* stream);
  * FPM_BIN_CHUNKS steps the sorted particles in equal chunks, painting into
  * the density directly with warp-summed deposits of neighbouring lanes;
  * FPM_BIN_TILES gives each tile to one block, which paints into a
- * shared-memory copy of the tile.  The caller's arrays stay in Lagrangian
+ * shared-memory copy of the tile; FPM_BIN_WALK keeps the forward on the
+ * lattice walk and only provides the tiles and buffers for the reverse
+ * sweep's binned order (fpm_plan_set_adjoint_binning).  The caller's
+ * arrays stay in Lagrangian
  * order; the results equal the lattice walk's up to the order of the
  * density's FP32 sums.  tile 0 returns to the lattice walk.  Allocates 56
  * bytes per particle and 4 per force-mesh cell (freed by tile 0 or
  * fpm_plan_destroy), synchronising the device; every force mesh must divide
  * into tiles (else FPM_ERR_UNSUPPORTED).  Plans with PGD switched on keep
  * the lattice walk.  Captured graphs of the plan must be captured again. */
-enum { FPM_BIN_TILES = 0, FPM_BIN_CHUNKS = 1 };
+enum { FPM_BIN_TILES = 0, FPM_BIN_CHUNKS = 1, FPM_BIN_WALK = 2 };
 int fpm_plan_set_binning(fpm_plan* plan, int tile, int sort_every, int mode);
+
+/* The reverse sweep (fpm_nbody_adjoint) of a plan with a potential tape in
+ * the same binned order (no counterpart in the reference, whose gradient
+ * is TensorFlow's tape over the scatter / gather ops above): the caller's
+ * Lagrangian (disp, mom, lam_x, lam_p) are sorted by the cell of the final
+ * position, each position's fused reverse drift and force VJP runs over
+ * the sorted particles, which are re-sorted by their current cell every
+ * sort_every positions, and the results go back to the caller's arrays in
+ * Lagrangian order.  They equal the lattice walk's up to the order of the
+ * FP32 sums into the adjoint meshes.  Needs an adjoint plan
+ * (FPM_PLAN_ADJOINT) with binning on (fpm_plan_set_binning), else
+ * FPM_ERR_STATE; without a tape, or with PGD on, the reverse sweep keeps
+ * the lattice walk.  Allocates 48 bytes per particle (freed by sort_every
+ * 0, by tile 0 or by fpm_plan_destroy), synchronising the device; the
+ * setting survives a change of tile when the buffers still fit.  Captured
+ * graphs of the plan must be captured again. */
+int fpm_plan_set_adjoint_binning(fpm_plan* plan, int sort_every);
 
 /* Autotuner of the forward step's particle traversal.  No counterpart in
  * the reference (TensorFlow picks its own kernels).  Times, on the plan's

@@ -34,12 +34,15 @@ def binned(fpm):
   """Sets binning on cached plans; resets every plan it touched."""
   touched = []
 
-  def set_(dims, tile, every, flags=0, mode=1):
+  def set_(dims, tile, every, flags=0, mode=1, adj_every=0):
     p = _plan(dims, flags)
     p.set_binning(tile, every, mode)
+    p.set_adjoint_binning(adj_every) if flags else None
     touched.append(p)
   yield set_
   for p in touched:
+    if p.adjoint_binning:
+      p.set_adjoint_binning(0)
     p.set_binning(0)
 
 
@@ -157,6 +160,65 @@ def test_binned_forward_gradient(fpm, binned, store):
     binned([(16, 16, 16, 1)], 8, 2, flags=_lib.FPM_PLAN_ADJOINT, mode=mode)
     g1 = grad()
     assert rel_l2(g1, g0) < 1e-4
+
+
+@pytest.mark.parametrize('nc,adj_every,mode', [(16, 1, 1), (16, 3, 2),
+                                                (32, 2, 1), (32, 1, 2)])
+def test_binned_reverse_sweep(fpm, binned, nc, adj_every, mode):
+  """The potential-tape reverse sweep over the binned particle order
+  (fpm_plan_set_adjoint_binning: sorted state and cotangents, re-sorted
+  every adj_every positions, results back in Lagrangian order) gives the
+  lattice walk's gradient, with checkpoints and with the cotangent of the
+  final force (the loss reads F); the forward binned too (mode 1) or on
+  the lattice walk (mode 2, FPM_BIN_WALK)."""
+  from flowpm_b200 import _lib
+  rng = np.random.default_rng(nc + adj_every)
+  dims = [nc] * 3
+  lin = rng.standard_normal([1] + dims) * 0.6
+  stages = np.linspace(0.1, 1.0, 8)
+  target = rng.standard_normal([1] + dims) + 1.0
+  c = fpm.cosmology.Planck15()
+
+  def grad():
+    x = torch.tensor(lin, dtype=torch.float32, device='cuda',
+                     requires_grad=True)
+    st = fpm.nbody(c, fpm.lpt_init(c, x, 0.1, order=2), stages, dims,
+                   checkpoint_every=3, store_potential=True)
+    rho = fpm.cic_paint(torch.zeros([1] + dims, device='cuda'), st[0])
+    loss = ((rho - torch.tensor(target, dtype=torch.float32,
+                                device='cuda'))**2).sum()
+    loss = loss + 1e-3 * (st[2]**2).sum() + 1e-2 * (st[1]**2).sum()
+    (g,) = torch.autograd.grad(loss, x)
+    return host(g)
+
+  g0 = grad()
+  binned([tuple(dims) + (1,)], 8, 2, flags=_lib.FPM_PLAN_ADJOINT,
+         mode=mode, adj_every=adj_every)
+  g1 = grad()
+  assert np.isfinite(g1).all()
+  assert rel_l2(g1, g0) < 1e-4, rel_l2(g1, g0)
+
+
+def test_adjoint_binning_needs_binning(fpm):
+  from flowpm_b200 import _lib
+  from flowpm_b200._plans import Plan
+  p = Plan([(16, 16, 16, 1)], flags=_lib.FPM_PLAN_ADJOINT)
+  q = Plan([(16, 16, 16, 1)])
+  try:
+    with pytest.raises(_lib.FlowPMError) as e:
+      p.set_adjoint_binning(2)  # binning is off
+    assert e.value.code == _lib.FPM_ERR_STATE
+    q.set_binning(8, 1)
+    with pytest.raises(_lib.FlowPMError) as e:
+      q.set_adjoint_binning(2)  # not an adjoint plan
+    assert e.value.code == _lib.FPM_ERR_STATE
+    p.set_binning(8, 1)
+    p.set_adjoint_binning(2)
+    p.set_binning(16, 1)  # kept across a change of tile
+    p.set_adjoint_binning(0)
+  finally:
+    p.close()
+    q.close()
 
 
 def test_binning_refused_when_tiles_do_not_fit(fpm):
