@@ -64,6 +64,19 @@ REPLICA_SEED_BASE = 1000
 # the FP64 oracle (python tests/c4_gradient_check.py export / check); filled
 # in from its summary.
 GRAD_CHECK_C4 = None
+# Error of a simulation at the C5 spacing against the oracle, from
+# python tests/c5_fp64_check.py (256^3, box 500 Mpc/h, Planck15, seed 5120,
+# 30 steps; the oracle cannot run 512^3 in reasonable time on the host).
+FP64_CHECK_C5 = {
+    'workload': 'one C5 simulation at 256^3, box 500 Mpc/h (C5 spacing), '
+                'Planck15, seed 5120, 2LPT at a0 = 0.1, 30 KDK steps',
+    'how': 'python tests/c5_fp64_check.py (GPU run, oracle on 16 host '
+           'cores: 219 s FP32, 326 s FP64)',
+    'vs_oracle_fp32': {'density_rel_l2': 1.07e-05, 'pk_max_rel': 1.53e-06},
+    'fp64_error': {'density_rel_l2': 5.62e-06, 'pk_max_rel': 1.69e-06,
+                   'oracle_fp32_density_rel_l2': 1.11e-05,
+                   'oracle_fp32_pk_max_rel': 1.06e-06},
+}
 
 
 def parse():
@@ -576,6 +589,7 @@ def measure_batched(fpm, flush, reps):
     _lib.call('fpm_lattice_shift', _lib.ptr(d), _lib.ptr(x), 1, n, n, n, 1,
               st)
     err = max(err, float((res[0, 0] - x).abs().max()))
+  fp64 = c3_fp64_error(sims, d0s, p0s, runner.results())
   tb = _timed(batched, reps, flush)
   tp = _timed(plain, reps, flush)
   # Amdahl bound of the mix: the four 128^3 simulations hold 78 % of the
@@ -605,8 +619,46 @@ def measure_batched(fpm, flush, reps):
       'particle_updates_per_s': float(
           sum(n**3 * T for n, _, _, T, _ in sims)) / (tb * 1e-3),
       'max_abs_diff_batched_vs_plain': err,
+      'fp64_error': fp64,
       'traversal': list(choice),
   }
+
+
+def c3_fp64_error(sims, d0s, p0s, results):
+  """Final-density error of the batched results against the oracle in
+  float64 (and float32, the reference's arithmetic) run from the same
+  initial states with each simulation's own cosmology and step count, for
+  the first 32^3 and the first 64^3 simulation of the mix (the 128^3 size
+  is C2's, whose error the headline line's `parity` states)."""
+  from oracle import background as obg
+  from oracle import pm as opm
+  torch.set_num_threads(os.cpu_count() or 1)
+  out = {}
+  for size in (32, 64):
+    i = next(k for k, s in enumerate(sims) if s[0] == size)
+    n, box, c, T, seed = sims[i]
+    q = torch.stack(torch.meshgrid(*[torch.arange(n, dtype=torch.float64)] *
+                                   3, indexing='ij'), -1).reshape(-1, 3)
+    d0, p0 = d0s[i].double().cpu(), p0s[i].double().cpu()
+    x_gpu = results[i][0].double().cpu()  # (1, Np, 3) final positions
+    params = dict(Omega_c=c.Omega_c, sigma8=c.sigma8)
+    stages = np.linspace(A0, 1.0, T + 1)
+    rhos = {}
+    for name, dt, npdt in (('fp64', torch.float64, np.float64),
+                           ('fp32', torch.float32, np.float32)):
+      b = obg.Background(params, dtype=npdt)
+      st = torch.stack([q + d0, p0, torch.zeros_like(d0)])[:, None].to(dt)
+      st = opm.nbody(b, st, stages, n)
+      rhos[name] = opm.cic_paint(torch.zeros((1, n, n, n), dtype=dt),
+                                 st[0]).double()
+    rg = opm.cic_paint(torch.zeros((1, n, n, n), dtype=torch.float64),
+                       x_gpu)
+    rel = lambda a, b: float((a - b).norm() / b.norm())
+    out['%d^3' % n] = {'steps': T, 'density_rel_l2': rel(rg, rhos['fp64']),
+                       'oracle_fp32_density_rel_l2': rel(rhos['fp32'],
+                                                         rhos['fp64']),
+                       'vs_oracle_fp32': rel(rg, rhos['fp32'])}
+  return out
 
 
 def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
@@ -890,6 +942,7 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
       'forward_adjoint_ms': t_best,
       'sims_per_s_forward_adjoint': 2 / (t_best * 1e-3),
       'rebuilt': rebuilt,
+      'fp64_check': FP64_CHECK_C5 if n == 512 else None,
       'kernel_roofline': roof,
       'peak_gbs': peak,
       'peak_kind': peak_kind,
