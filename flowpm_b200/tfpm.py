@@ -44,19 +44,46 @@ def _check_kvec(kvec, nc):
         'only the default k grid fftk(nc, symmetric=False) is supported')
 
 
-def linear_amplitude(nc, boxsize, pk):
-  """Half-spectrum amplitude sqrt(P(|k|) / V), (nx, ny, nz//2 + 1) float32,
-  with |k| = sqrt(sum_d (k_d / L_d * n_d)^2) as in flowpm/tfpm.py:55-56.
+def _axis_kvec(kvec, nc):
+  """A caller's k grid as three per-axis vectors: each entry of ``kvec``
+  must broadcast along one axis only (the shapes fftk returns, (nx, 1, 1),
+  (1, ny, 1), (1, 1, nz)).  The field is built on the half spectrum, so
+  the grid must give every mode and its mirror -k the same |k| (true of
+  fftk's grid and of any rescaling of it)."""
+  if len(kvec) != 3:
+    raise ValueError('kvec must hold three arrays, one per axis')
+  out = []
+  for d, k in enumerate(kvec):
+    k = np.asarray(k, dtype=np.float64)
+    shape = [1, 1, 1]
+    shape[d] = nc[d]
+    if k.ndim != 3 or list(k.shape) != shape:
+      raise NotImplementedError(
+          'kvec[%d] must have shape %s (per-axis k vectors)' % (d, shape))
+    k = k.ravel()
+    if not np.array_equal(k * k, (k * k)[(-np.arange(nc[d])) % nc[d]]):
+      raise NotImplementedError(
+          'kvec[%d] must satisfy |k[i]| = |k[-i]| (half-spectrum field)' % d)
+    out.append(k)
+  return out
 
-  For cubic meshes in cubic boxes P is evaluated once per distinct
-  i^2 + j^2 + l^2; otherwise on every mode."""
+
+def linear_amplitude(nc, boxsize, pk, kvec=None):
+  """Half-spectrum amplitude sqrt(P(|k|) / V), (nx, ny, nz//2 + 1) float32,
+  with |k| = sqrt(sum_d (k_d / L_d * n_d)^2) as in flowpm/tfpm.py:55-56,
+  k_d from ``kvec`` (per-axis vectors, default fftk(nc, symmetric=False)).
+
+  For the default grid of a cubic mesh in a cubic box P is evaluated once
+  per distinct i^2 + j^2 + l^2; otherwise on every mode."""
   nc, boxsize = _nc3(nc), _box3(boxsize)
-  kvec = fftk(nc, symmetric=False)
+  custom = kvec is not None
+  kvec = _axis_kvec(kvec, nc) if custom else fftk(nc, symmetric=False)
   nzh = nc[2] // 2 + 1
   vol = boxsize[0] * boxsize[1] * boxsize[2]
-  ax = [(kk.ravel() / boxsize[i] * nc[i])**2 for i, kk in enumerate(kvec)]
+  ax = [(np.ravel(kk) / boxsize[i] * nc[i])**2 for i, kk in enumerate(kvec)]
   ax[2] = ax[2][:nzh]
-  if nc[0] == nc[1] == nc[2] and boxsize[0] == boxsize[1] == boxsize[2]:
+  if (not custom and nc[0] == nc[1] == nc[2] and
+      boxsize[0] == boxsize[1] == boxsize[2]):
     f = np.rint(np.fft.fftfreq(nc[0]) * nc[0]).astype(np.int64)
     sq = f * f
     key = (sq[:, None, None] + sq[None, :, None] +
@@ -85,10 +112,9 @@ def linear_field(nc, boxsize, pk, kvec=None, batch_size=1, seed=None,
   ``white`` (batch, nx, ny, nz) replaces the generated noise when given.
   Returns (batch, nx, ny, nz) float32 on the current CUDA device."""
   nc = _nc3(nc)
-  _check_kvec(kvec, nc)
   if dtype not in (torch.float32, np.float32):
     raise NotImplementedError('linear_field computes in float32')
-  amp = as_cuda(linear_amplitude(nc, boxsize, pk))
+  amp = as_cuda(linear_amplitude(nc, boxsize, pk, kvec))
   amp = amp.reshape(1, -1).expand(batch_size, -1).contiguous()
   plan = get_plan([tuple(nc) + (1,)] * batch_size, flags=_lib.FPM_PLAN_LPT)
   out = torch.empty([batch_size] + nc, dtype=torch.float32, device='cuda')

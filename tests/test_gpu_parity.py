@@ -139,6 +139,16 @@ def test_linear_field_seeded(fpm):
   assert_allclose(host(a), ref.numpy(), atol=1e-5 * float(ref.abs().max()))
 
 
+def test_linear_field_caller_kvec(fpm):
+  """linear_field on a caller's k grid (fftk's, doubled): |k| doubles, so
+  the field equals the default grid's with P(2k), on the same noise."""
+  pk = pk_table()
+  kv = [2.0 * k for k in fpm.kernels.fftk([32] * 3, symmetric=False)]
+  a = fpm.linear_field(32, 100., pk, kvec=kv, seed=4)
+  b = fpm.linear_field(32, 100., lambda k: pk(2.0 * np.asarray(k)), seed=4)
+  assert_allclose(host(a), host(b), atol=1e-5 * float(b.abs().max()))
+
+
 @pytest.mark.parametrize('nc,order', [(16, 1), (16, 2), (32, 2)])
 def test_lpt_init_golden(fpm, nc, order):
   z = golden('lpt')

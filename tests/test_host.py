@@ -123,6 +123,29 @@ def test_linear_amplitude(fpm, nc, box):
   assert_allclose(amp, ref[:, :, :n3[2] // 2 + 1], rtol=1e-6)
 
 
+def test_linear_amplitude_caller_kvec(fpm):
+  """A caller's per-axis k grid (here fftk's, rescaled per axis) gives the
+  amplitude of the reference formula on that grid; grids whose |k| is not
+  mirror-symmetric, or not per-axis, are refused."""
+  pk = pk_table()
+  n3, b3 = [8, 6, 10], [40., 30., 50.]
+  kv = [k * s for k, s in zip(opm.fftk(n3, symmetric=False), (1.5, 0.7, 2.))]
+  amp = fpm.tfpm.linear_amplitude(n3, b3, pk, kvec=kv)
+  km = sum((kk / b3[i] * n3[i])**2 for i, kk in enumerate(kv))**0.5
+  ref = (pk(km) / (b3[0] * b3[1] * b3[2]))**0.5
+  assert_allclose(amp, ref[:, :, :n3[2] // 2 + 1], rtol=1e-6)
+  default = fpm.tfpm.linear_amplitude(16, 50., pk)
+  same = fpm.tfpm.linear_amplitude(16, 50., pk,
+                                   kvec=opm.fftk([16] * 3, symmetric=False))
+  assert_allclose(same, default, rtol=1e-6)
+  skew = [k.copy() for k in kv]
+  skew[1] = skew[1] + 0.1
+  with pytest.raises(NotImplementedError):
+    fpm.tfpm.linear_amplitude(n3, b3, pk, kvec=skew)
+  with pytest.raises(NotImplementedError):
+    fpm.tfpm.linear_amplitude(n3, b3, pk, kvec=[np.ravel(k) for k in kv])
+
+
 # --------------------------------------------------------------------------
 # C ABI
 # --------------------------------------------------------------------------
