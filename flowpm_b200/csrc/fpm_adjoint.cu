@@ -419,8 +419,9 @@ k_adj_position_sorted(const SimDev* __restrict__ sims, int nsims,
       if (i >= end) break;
       const uint32_t l = a.lag[i];
       int qi, qj, qk;
-      lattice_ijk(S, l, qi, qj, qk);
-      adj_position_one(S, a, c, i, S.p_off + l, qi, qj, qk);
+      unpack_site(l, S.qkb, S.qjb, qi, qj, qk);
+      adj_position_one(S, a, c, i, S.p_off + site_local(S, qi, qj, qk), qi,
+                       qj, qk);
     }
   }
 }

@@ -32,7 +32,7 @@ struct AdjArgs {
   const float* ckpt;      // checkpoint slots (d, p) or null
   int ckpt_every;
   int32_t* status;
-  const uint32_t* lag;    // binned order: Lagrangian index of each slot
+  const uint32_t* lag;    // binned order: packed lattice site of each slot
   int64_t total_np;
   int max_steps;
   int it;
@@ -50,8 +50,9 @@ void launch_adj_position(const SimDev* sims, int nsims, int64_t nchunks,
                          const AdjArgs& a, cudaStream_t st);
 // launch_adj_position over particles kept sorted by cell (the binned order
 // of fpm_bin.cu): the particle chunks [0, nchunks) of the plan, slot i of
-// disp, mom, lam_x and lam_p holding Lagrangian particle a.lag[i] of its
-// simulation; checkpoints and lam_f are read in Lagrangian order.
+// disp, mom, lam_x and lam_p holding the particle of packed lattice site
+// a.lag[i] (pack_site) of its simulation; checkpoints and lam_f are read in
+// Lagrangian order.
 void launch_adj_position_sorted(const SimDev* sims, int nsims,
                                 int64_t nchunks, const AdjArgs& a,
                                 cudaStream_t st);

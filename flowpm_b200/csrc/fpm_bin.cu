@@ -39,89 +39,171 @@ __device__ __forceinline__ unsigned cell_key(const BinRun& R, int cx, int cy,
          (lx * T + ly) * T + lz;
 }
 
-// Run-relative cell key (simulation r of the run: + r * ncell) of the
-// particle in slot t of the run, and its Lagrangian index.
+// Cell key of slot t of simulation r of the run (run-relative: + r *
+// ncell) and its packed lattice site: from the carried index when lag is
+// set, else t is the Lagrangian index itself.
 template <int T>
-__device__ __forceinline__ uint64_t particle_key(const BinRun& R,
-                                                 const float* __restrict__ d,
+__device__ __forceinline__ uint32_t particle_key(const BinRun& R,
+                                                 const float3 dv,
                                                  const uint32_t* __restrict__ lag,
-                                                 int64_t t, uint32_t& l) {
-  const int64_t r = t / R.np;
-  l = lag ? lag[R.p0 + t] : (uint32_t)(t - r * R.np);
-  const unsigned tt = l / (unsigned)R.nz;
-  const int k = (int)(l - tt * (unsigned)R.nz);
-  const int i = (int)(tt / (unsigned)R.ny);
-  const int j = (int)(tt - (unsigned)i * (unsigned)R.ny);
-  const float3 dv = ld3(d, R.p0 + t);
+                                                 int r, int64_t slot,
+                                                 uint32_t t, uint32_t& l) {
+  int i, j, k;
+  if (lag) {
+    l = lag[slot];
+    unpack_site(l, R.qkb, R.qjb, i, j, k);
+  } else {
+    const unsigned tt = t / (unsigned)R.nz;
+    k = (int)(t - tt * (unsigned)R.nz);
+    i = (int)(tt / (unsigned)R.ny);
+    j = (int)(tt - (unsigned)i * (unsigned)R.ny);
+    l = pack_site(i, j, k, R.qkb, R.qjb);
+  }
   const float b = (float)R.bf;
   const float x = __fmul_rn(__fadd_rn(index_float(i), dv.x), b);
   const float y = __fmul_rn(__fadd_rn(index_float(j), dv.y), b);
   const float z = __fmul_rn(__fadd_rn(index_float(k), dv.z), b);
   const int cx = cic_axis(x, R.mx).i0, cy = cic_axis(y, R.my).i0,
             cz = cic_axis(z, R.mz).i0;
-  return (uint64_t)r * (uint64_t)R.ncell + cell_key<T>(R, cx, cy, cz);
+  return (uint32_t)r * (uint32_t)R.ncell + cell_key<T>(R, cx, cy, cz);
 }
 
-// cnt[m0 + key] += 1 for every particle of the run (warp-aggregated: lanes
-// with equal keys add once).
+// Lanes of a warp with equal keys in a row form a run (a sorted input
+// makes the particles of a cell contiguous); the run's first lane (its
+// head) adds or claims for the whole run.  Returns the mask of heads;
+// lanes past the end carry keys of their own (kSentinel - lane).
+constexpr uint32_t kSentinel = 0xffffffffu;
+__device__ __forceinline__ unsigned run_heads(uint32_t key, int lane) {
+  const uint32_t up = __shfl_up_sync(0xffffffffu, key, 1);
+  return __ballot_sync(0xffffffffu, lane == 0 || up != key);
+}
+// Lanes from this head to the next head.
+__device__ __forceinline__ int run_length(unsigned heads, int lane) {
+  const unsigned above = heads & ~((2u << lane) - 1u);
+  return (above ? __ffs(above) - 1 : 32) - lane;
+}
+// The head of this lane's run.
+__device__ __forceinline__ int run_head(unsigned heads, int lane) {
+  return 31 - __clz(heads & ((2u << lane) - 1u));
+}
+
+// Chunks of kChunk slots per simulation: the sort kernels walk chunks, so
+// that the simulation of a slot is known per chunk.
+__device__ __forceinline__ int64_t sort_chunks_per_sim(const BinRun& R) {
+  return (R.np + kChunk - 1) / kChunk;
+}
+
+// cnt[m0 + key] += 1 for every particle of the run, one atomic per run of
+// equal keys.
 template <int T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kThreads)
 k_bin_count(BinRun R, const float* __restrict__ d,
             const uint32_t* __restrict__ lag, int32_t* __restrict__ cnt) {
-  const int64_t n = (int64_t)R.count * R.np;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t l;
-    const uint64_t key = particle_key<T>(R, d, lag, t, l);
-    const unsigned m = __match_any_sync(__activemask(), key);
-    if ((threadIdx.x & 31) == __ffs(m) - 1)
-      atomicAdd(cnt + R.m0 + key, (int32_t)__popc(m));
+  const int lane = threadIdx.x & 31;
+  const int64_t cps = sort_chunks_per_sim(R);
+  const int64_t nch = cps * R.count;
+  for (int64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    const int r = (int)(ch / cps);
+    const int64_t t0 = (ch - (int64_t)r * cps) * kChunk;
+#pragma unroll
+    for (int item = 0; item < kItems; ++item) {
+      const int64_t t = t0 + item * kThreads + threadIdx.x;
+      const bool valid = t < R.np;
+      uint32_t key = kSentinel - lane, l;
+      if (valid) {
+        const int64_t slot = R.p0 + (int64_t)r * R.np + t;
+        key = particle_key<T>(R, ld3(d, slot), lag, r, slot, (uint32_t)t, l);
+      }
+      const unsigned heads = run_heads(key, lane);
+      if (valid && ((heads >> lane) & 1u))
+        atomicAdd(cnt + R.m0 + key, (int32_t)run_length(heads, lane));
+    }
   }
 }
 
-// Scatter: slot = off[key]++ (warp-aggregated, lanes of equal keys keep
-// their order); writes the NP float3 arrays of the payload (the first is
-// the displacement the keys come from) and the Lagrangian index to the
-// output arrays.
+// Scatter: the head of each run claims the run's slots with one atomic on
+// off[key] (lanes of a run keep their order), then every lane writes the
+// NP float3 arrays of the payload (the first is the displacement the keys
+// come from) and its packed lattice site.  The kItems claims of a thread
+// are issued before any of them is used, so their latencies overlap.
 template <int T, int NP>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kThreads)
 k_bin_scatter(BinRun R, BinPayload pay, const uint32_t* __restrict__ lag,
               int32_t* __restrict__ off, uint32_t* __restrict__ lag_out) {
-  const int64_t n = (int64_t)R.count * R.np;
   const int lane = threadIdx.x & 31;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t l;
-    const uint64_t key = particle_key<T>(R, pay.src[0], lag, t, l);
-    const unsigned m = __match_any_sync(__activemask(), key);
-    const int leader = __ffs(m) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(off + R.m0 + key, (int32_t)__popc(m));
-    base = __shfl_sync(m, base, leader);
-    const int64_t dst = base + __popc(m & ((1u << lane) - 1));
+  const int64_t cps = sort_chunks_per_sim(R);
+  const int64_t nch = cps * R.count;
+  for (int64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    const int r = (int)(ch / cps);
+    const int64_t t0 = (ch - (int64_t)r * cps) * kChunk;
+    const int64_t s0 = R.p0 + (int64_t)r * R.np;
+    uint32_t l[kItems];
+    int base[kItems];
+    unsigned heads[kItems];
+    float3 dv[kItems];
 #pragma unroll
-    for (int q = 0; q < NP; ++q) st3(pay.dst[q], dst, ld3(pay.src[q], R.p0 + t));
-    lag_out[dst] = l;
+    for (int item = 0; item < kItems; ++item) {
+      const int64_t t = t0 + item * kThreads + threadIdx.x;
+      const bool valid = t < R.np;
+      uint32_t key = kSentinel - lane;
+      l[item] = 0;
+      dv[item] = make_float3(0.f, 0.f, 0.f);
+      if (valid) {
+        dv[item] = ld3(pay.src[0], s0 + t);
+        key = particle_key<T>(R, dv[item], lag, r, s0 + t, (uint32_t)t,
+                              l[item]);
+      }
+      heads[item] = run_heads(key, lane);
+      base[item] = 0;
+      if (valid && ((heads[item] >> lane) & 1u))
+        base[item] = atomicAdd(off + R.m0 + key,
+                               (int32_t)run_length(heads[item], lane));
+    }
+#pragma unroll
+    for (int item = 0; item < kItems; ++item) {
+      const int64_t t = t0 + item * kThreads + threadIdx.x;
+      const int h = run_head(heads[item], lane);
+      const int b = __shfl_sync(0xffffffffu, base[item], h);
+      if (t >= R.np) continue;
+      const int64_t dst = (int64_t)b + (lane - h);
+      st3(pay.dst[0], dst, dv[item]);
+#pragma unroll
+      for (int q = 1; q < NP; ++q)
+        st3(pay.dst[q], dst, ld3(pay.src[q], s0 + t));
+      lag_out[dst] = l[item];
+    }
   }
 }
 
-// Back to Lagrangian order: slot p0 + t, holding lattice site lag of
-// simulation r = t / np of the run, goes to p0 + r np + lag.
+// Back to Lagrangian order: the slot of simulation r holding packed site
+// (i, j, k) goes to p0 + r np + (i ny + j) nz + k.
 template <int NP>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kThreads)
 k_bin_unsort(BinRun R, BinPayload pay, const uint32_t* __restrict__ lag) {
-  const int64_t n = (int64_t)R.count * R.np;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = t / R.np;
-    const int64_t g = R.p0 + r * R.np + lag[R.p0 + t];
+  const int64_t cps = sort_chunks_per_sim(R);
+  const int64_t nch = cps * R.count;
+  for (int64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    const int r = (int)(ch / cps);
+    const int64_t t0 = (ch - (int64_t)r * cps) * kChunk;
+    const int64_t s0 = R.p0 + (int64_t)r * R.np;
 #pragma unroll
-    for (int q = 0; q < NP; ++q) st3(pay.dst[q], g, ld3(pay.src[q], R.p0 + t));
+    for (int item = 0; item < kItems; ++item) {
+      const int64_t t = t0 + item * kThreads + threadIdx.x;
+      if (t >= R.np) continue;
+      int i, j, k;
+      unpack_site(lag[s0 + t], R.qkb, R.qjb, i, j, k);
+      const int64_t g =
+          s0 + (int64_t)(((unsigned)i * (unsigned)R.ny + (unsigned)j) *
+                             (unsigned)R.nz + (unsigned)k);
+#pragma unroll
+      for (int q = 0; q < NP; ++q) st3(pay.dst[q], g, ld3(pay.src[q], s0 + t));
+    }
   }
 }
 
-// Exclusive scan of v[0..n) in place (n a multiple of 4, v 16-byte
-// aligned), plus base: three passes over chunks of kScanChunk values.
+// Exclusive scan of the counts cnt[0..n) into out (n a multiple of 4, both
+// 16-byte aligned), plus base, zeroing cnt on the way: three passes over
+// chunks of kScanChunk values.
 constexpr int kScanThreads = 256, kScanPer = 16;
 constexpr int kScanChunk = kScanThreads * kScanPer;
 
@@ -203,14 +285,14 @@ k_scan_top(int32_t* sums, int nb, int32_t base) {
 // over the groups in block order: group (q, t) precedes (q, t + 1) and
 // (q + 1, 0).  The block scan runs once per q.
 __global__ void __launch_bounds__(kScanThreads)
-k_scan_apply(int32_t* __restrict__ v, int64_t n,
+k_scan_apply(int32_t* __restrict__ cnt, int32_t* __restrict__ out, int64_t n,
              const int32_t* __restrict__ sums) {
   const int64_t b0 = (int64_t)blockIdx.x * kScanChunk;
   int carry = sums[blockIdx.x];
 #pragma unroll
   for (int q = 0; q < kScanPer / 4; ++q) {
     const int64_t i = b0 + (q * kScanThreads + threadIdx.x) * 4;
-    int4 a = load_part(v, i, n);
+    int4 a = load_part(cnt, i, n);
     const int s = a.x + a.y + a.z + a.w;
     int total;
     const int e = block_excl_scan(s, total) + carry;
@@ -221,7 +303,9 @@ k_scan_apply(int32_t* __restrict__ v, int64_t n,
       o.y = e + a.x;
       o.z = o.y + a.y;
       o.w = o.z + a.z;
-      *reinterpret_cast<int4*>(v + i) = o;
+      *reinterpret_cast<int4*>(out + i) = o;
+      // the counts start from zero at the next sort
+      *reinterpret_cast<int4*>(cnt + i) = make_int4(0, 0, 0, 0);
     }
   }
 }
@@ -287,8 +371,8 @@ k_step_binned(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
     for (int i = begin + (int)threadIdx.x; i < end; i += blockDim.x) {
       const uint32_t l = b.blag[i];
       int qi, qj, qk;
-      lattice_ijk(S, l, qi, qj, qk);
-      const int64_t g = S.p_off + l;  // Lagrangian slot
+      unpack_site(l, S.qkb, S.qjb, qi, qj, qk);
+      const int64_t g = S.p_off + site_local(S, qi, qj, qk);  // Lagrangian
       float3 d = ld3(b.bd, i), p = ld3(b.bp, i);
       const float3 x = mesh_pos(S, qi, qj, qk, d);
       const Cic8 c0 = cic8(cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
@@ -407,8 +491,8 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
         p = ld3(b.bp, i);
       }
       int qi, qj, qk;
-      lattice_ijk(S, l, qi, qj, qk);
-      const int64_t g = S.p_off + l;  // Lagrangian slot
+      unpack_site(l, S.qkb, S.qjb, qi, qj, qk);
+      const int64_t g = S.p_off + site_local(S, qi, qj, qk);  // Lagrangian
       const float3 x = mesh_pos(S, qi, qj, qk, d);
       const Cic8 c0 = cic8(cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
                            cic_axis(x.z, S.mz), S.my, S.mz);
@@ -452,13 +536,30 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
         if (!finite3(xn.x, xn.y, xn.z))
           atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
       }
-      const Cic8 c1 = cic8(cic_axis(xn.x, S.mx), cic_axis(xn.y, S.my),
-                           cic_axis(xn.z, S.mz), S.my, S.mz);
+      const Axis nx1 = cic_axis(xn.x, S.mx), ny1 = cic_axis(xn.y, S.my),
+                 nz1 = cic_axis(xn.z, S.mz);
+      const Cic8 c1 = cic8(nx1, ny1, nz1, S.my, S.mz);
       // base cell of the deposit; a lane past the sim's end gets a key of
       // its own
       const unsigned key = valid ? c1.row[0] + c1.z0 : 0xffffffffu - lane;
       const unsigned up = __shfl_up_sync(0xffffffffu, key, 1);
       const bool head = lane == 0 || up != key;
+      if (b.count) {
+        // the sort after this step: one count per run of lanes in a cell
+        const unsigned hs = __ballot_sync(0xffffffffu, head);
+        if (valid && head) {
+          const int lt = b.tile_log2, tm = (1 << lt) - 1;
+          const unsigned tile =
+              ((unsigned)(nx1.i0 >> lt) * (unsigned)S.nty +
+               (unsigned)(ny1.i0 >> lt)) * (unsigned)S.ntz +
+              (unsigned)(nz1.i0 >> lt);
+          const unsigned local =
+              ((unsigned)((nx1.i0 & tm) << lt | (ny1.i0 & tm)) << lt) |
+              (unsigned)(nz1.i0 & tm);
+          atomicAdd(b.count + S.m_off + ((tile << (3 * lt)) | local),
+                    (int32_t)run_length(hs, lane));
+        }
+      }
       float w[8];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -470,9 +571,12 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
         // segmented sums over runs of contiguous lanes with equal keys (a
         // key can recur in a later run after the particles drifted since
         // their sort; each run deposits its own sum): lane + o is in this
-        // lane's run when no run starts in (lane, lane + o]
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
+        // lane's run when no run starts in (lane, lane + o]; the longest
+        // run of the warp bounds the rounds
+        const unsigned longest = __reduce_max_sync(
+            0xffffffffu, head ? (unsigned)run_length(heads, lane) : 1u);
+#pragma unroll 1
+        for (int o = 1; o < (int)longest; o <<= 1) {
           const bool same =
               lane + o < 32 &&
               ((unsigned long long)heads >> (lane + 1) & ((1ull << o) - 1)) == 0;
@@ -514,6 +618,25 @@ void launch_step_binned(int tile, const SimDev* sims, int nsims, int64_t ch0,
                0, st, sims, nsims, ch0, ch1, b);
 }
 
+namespace {
+int bits_for(int n) {  // bits of the largest index n - 1
+  int b = 0;
+  while ((1ll << b) < (long long)n) ++b;
+  return b;
+}
+}  // namespace
+
+bool bin_run_supported(int nx, int ny, int nz, int64_t ncell, int count,
+                       int* qkb, int* qjb) {
+  const int ib = bits_for(nx), jb = bits_for(ny), kb = bits_for(nz);
+  if (ib + jb + kb > 32 || jb + kb > 31) return false;
+  // keys below the sentinels kSentinel - lane of lanes past the end
+  if ((int64_t)count * ncell >= (int64_t)kSentinel - 64) return false;
+  *qkb = kb;
+  *qjb = jb;
+  return true;
+}
+
 bool bin_tile_supported(int tile, int mx, int my, int mz) {
   if (tile != 8 && tile != 16) return false;
   return mx % tile == 0 && my % tile == 0 && mz % tile == 0;
@@ -525,8 +648,10 @@ size_t bin_scan_blocks(int64_t ncells) {
 
 namespace {
 
-int64_t sort_blocks(int64_t n) {
-  int64_t blocks = (n + 255) / 256;
+// Blocks of the sort kernels: one per chunk of kChunk slots of a
+// simulation, at most 16 per SM (grid-stride beyond).
+int64_t sort_blocks(const BinRun& R) {
+  int64_t blocks = (R.np + kChunk - 1) / kChunk * R.count;
   const int64_t cap = (int64_t)kNumSMs * 16;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
@@ -538,32 +663,28 @@ void launch_scatter(int tile, unsigned blocks, const BinRun& R,
                     const BinPayload& pay, const uint32_t* lag, int32_t* cell,
                     uint32_t* lag_out, cudaStream_t st) {
   if (tile == 8)
-    k_bin_scatter<8, NP><<<blocks, 256, 0, st>>>(R, pay, lag, cell, lag_out);
+    k_bin_scatter<8, NP>
+        <<<blocks, kThreads, 0, st>>>(R, pay, lag, cell, lag_out);
   else
-    k_bin_scatter<16, NP><<<blocks, 256, 0, st>>>(R, pay, lag, cell, lag_out);
+    k_bin_scatter<16, NP>
+        <<<blocks, kThreads, 0, st>>>(R, pay, lag, cell, lag_out);
 }
 
 }  // namespace
 
-int launch_bin_sort(int tile, const BinRun& R, const BinPayload& pay,
-                    const uint32_t* lag, int32_t* cell, int32_t* sums,
-                    uint32_t* lag_out, cudaStream_t st) {
+int launch_bin_scan_scatter(int tile, const BinRun& R, const BinPayload& pay,
+                            const uint32_t* lag, int32_t* count,
+                            int32_t* cell, int32_t* sums, uint32_t* lag_out,
+                            cudaStream_t st) {
   if (pay.n != 2 && pay.n != 4) return FPM_ERR_ARG;
   const int64_t ncells = (int64_t)R.count * R.ncell;
-  const int64_t n = (int64_t)R.count * R.np;
-  if (cudaMemsetAsync(cell + R.m0, 0, sizeof(int32_t) * ncells, st) !=
-      cudaSuccess)
-    return FPM_ERR_CUDA;
-  const unsigned blocks = (unsigned)sort_blocks(n);
-  g_launches.fetch_add(5, std::memory_order_relaxed);
-  if (tile == 8)
-    k_bin_count<8><<<blocks, 256, 0, st>>>(R, pay.src[0], lag, cell);
-  else
-    k_bin_count<16><<<blocks, 256, 0, st>>>(R, pay.src[0], lag, cell);
+  const unsigned blocks = (unsigned)sort_blocks(R);
+  g_launches.fetch_add(4, std::memory_order_relaxed);
   const int nb = (int)bin_scan_blocks(ncells);
-  k_scan_sums<<<nb, kScanThreads, 0, st>>>(cell + R.m0, ncells, sums);
+  k_scan_sums<<<nb, kScanThreads, 0, st>>>(count + R.m0, ncells, sums);
   k_scan_top<<<1, 1024, 0, st>>>(sums, nb, (int32_t)R.p0);
-  k_scan_apply<<<nb, kScanThreads, 0, st>>>(cell + R.m0, ncells, sums);
+  k_scan_apply<<<nb, kScanThreads, 0, st>>>(count + R.m0, cell + R.m0, ncells,
+                                            sums);
   if (pay.n == 2)
     launch_scatter<2>(tile, blocks, R, pay, lag, cell, lag_out, st);
   else
@@ -571,10 +692,24 @@ int launch_bin_sort(int tile, const BinRun& R, const BinPayload& pay,
   return cudaGetLastError() == cudaSuccess ? FPM_OK : FPM_ERR_CUDA;
 }
 
+int launch_bin_sort(int tile, const BinRun& R, const BinPayload& pay,
+                    const uint32_t* lag, int32_t* count, int32_t* cell,
+                    int32_t* sums, uint32_t* lag_out, cudaStream_t st) {
+  if (pay.n != 2 && pay.n != 4) return FPM_ERR_ARG;
+  const unsigned blocks = (unsigned)sort_blocks(R);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (tile == 8)
+    k_bin_count<8><<<blocks, kThreads, 0, st>>>(R, pay.src[0], lag, count);
+  else
+    k_bin_count<16><<<blocks, kThreads, 0, st>>>(R, pay.src[0], lag, count);
+  return launch_bin_scan_scatter(tile, R, pay, lag, count, cell, sums,
+                                 lag_out, st);
+}
+
 int launch_bin_sort(int tile, const BinRun& R, const float* d,
-                    const float* p, const uint32_t* lag, int32_t* cell,
-                    int32_t* sums, float* d_out, float* p_out,
-                    uint32_t* lag_out, cudaStream_t st) {
+                    const float* p, const uint32_t* lag, int32_t* count,
+                    int32_t* cell, int32_t* sums, float* d_out, float* p_out,
+                    uint32_t* lag_out, bool counted, cudaStream_t st) {
   BinPayload pay;
   pay.n = 2;
   pay.src[0] = d;
@@ -583,15 +718,18 @@ int launch_bin_sort(int tile, const BinRun& R, const float* d,
   pay.dst[1] = p_out;
   pay.src[2] = pay.src[3] = nullptr;
   pay.dst[2] = pay.dst[3] = nullptr;
-  return launch_bin_sort(tile, R, pay, lag, cell, sums, lag_out, st);
+  if (counted)
+    return launch_bin_scan_scatter(tile, R, pay, lag, count, cell, sums,
+                                   lag_out, st);
+  return launch_bin_sort(tile, R, pay, lag, count, cell, sums, lag_out, st);
 }
 
 int launch_bin_unsort(const BinRun& R, const BinPayload& pay,
                       const uint32_t* lag, cudaStream_t st) {
   if (pay.n != 4) return FPM_ERR_ARG;
-  const unsigned blocks = (unsigned)sort_blocks((int64_t)R.count * R.np);
+  const unsigned blocks = (unsigned)sort_blocks(R);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_bin_unsort<4><<<blocks, 256, 0, st>>>(R, pay, lag);
+  k_bin_unsort<4><<<blocks, kThreads, 0, st>>>(R, pay, lag);
   return cudaGetLastError() == cudaSuccess ? FPM_OK : FPM_ERR_CUDA;
 }
 

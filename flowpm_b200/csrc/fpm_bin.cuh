@@ -14,8 +14,15 @@ struct BinRun {
   int nx, ny, nz, bf, mx, my, mz;
   int ntx, nty, ntz;       // tiles per axis
   int count;               // simulations
+  int qkb, qjb;            // bit widths of the packed lattice site
   int64_t np, ncell, p0, m0;
 };
+
+// Whether a run of `count` simulations of this shape can be binned: the
+// packed lattice site fits 32 bits and every run-relative cell key stays
+// below the sentinels the sort kernels keep for lanes past the end.
+bool bin_run_supported(int nx, int ny, int nz, int64_t ncell, int count,
+                       int* qkb, int* qjb);
 
 // Particle arrays a sort moves: n float3 arrays (2: displacement and
 // momentum; 4: displacement, momentum and the two cotangents of the
@@ -34,28 +41,32 @@ bool bin_tile_supported(int tile, int mx, int my, int mz);
 size_t bin_scan_blocks(int64_t ncells);
 
 // Counting sort of the run's particles by tile-major cell key: cell counts
-// into cell[m0 ..), their exclusive scan (plus p0: absolute slots), then the
-// scatter of (d, p, Lagrangian index) into the output arrays; afterwards
-// cell[c] holds the end slot of cell c.  lag NULL: the input is in
-// Lagrangian order (slot p0 + r np + t is lattice site t).  sums: at least
-// bin_scan_blocks(count * ncell) ints.
+// into count[m0 ..) (all zero on entry, and left zero), their exclusive
+// scan (plus p0: absolute slots) into cell[m0 ..), then the scatter of
+// (d, p, packed lattice site) into the output arrays; afterwards cell[c]
+// holds the end slot of cell c.  lag NULL: the input is in Lagrangian
+// order (slot p0 + r np + t is lattice site t); the index written is the
+// packed lattice site (pack_site).  counted: the counts are already in
+// count (a step kernel made them), only the scan and the scatter run.
+// sums: at least bin_scan_blocks(count * ncell) ints.
 int launch_bin_sort(int tile, const BinRun& R, const float* d,
-                    const float* p, const uint32_t* lag, int32_t* cell,
-                    int32_t* sums, float* d_out, float* p_out,
-                    uint32_t* lag_out, cudaStream_t st);
+                    const float* p, const uint32_t* lag, int32_t* count,
+                    int32_t* cell, int32_t* sums, float* d_out, float* p_out,
+                    uint32_t* lag_out, bool counted, cudaStream_t st);
 
 // The same sort of the payload's arrays.
 int launch_bin_sort(int tile, const BinRun& R, const BinPayload& pay,
-                    const uint32_t* lag, int32_t* cell, int32_t* sums,
-                    uint32_t* lag_out, cudaStream_t st);
+                    const uint32_t* lag, int32_t* count, int32_t* cell,
+                    int32_t* sums, uint32_t* lag_out, cudaStream_t st);
 
-// Sorted slots back to Lagrangian order (payload of 4 arrays): slot p0 + t
-// with Lagrangian index lag[p0 + t] goes to p0 + (t / np) np + lag.
+// Sorted slots back to Lagrangian order (payload of 4 arrays): the slot of
+// simulation r holding packed site (i, j, k) goes to p0 + r np +
+// (i ny + j) nz + k.
 int launch_bin_unsort(const BinRun& R, const BinPayload& pay,
                       const uint32_t* lag, cudaStream_t st);
 
 // State of the binned step: the sorted particles (updated in place), their
-// Lagrangian indices and the cells' end slots of the last sort.  The
+// packed lattice sites and the cells' end slots of the last sort.  The
 // StepArgs' disp, mom and force_out are the caller's Lagrangian arrays,
 // written at the last step (and ckpt / inter through the index).
 struct BinStepArgs {
@@ -64,6 +75,11 @@ struct BinStepArgs {
   float* bp;
   const uint32_t* blag;
   const int32_t* cell_end;
+  // k_step_sorted only: when set, the cells of the drifted particles are
+  // counted into count (keys tile-major in tiles of 2^tile_log2 cells, per
+  // simulation at its m_off) for the sort that follows the step
+  int32_t* count;
+  int tile_log2;
 };
 
 // The step over the tile chunks [ch0, ch1) (whole simulations), painting

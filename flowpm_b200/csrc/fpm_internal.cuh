@@ -57,6 +57,9 @@ struct SimDev {
   // the plan's tile enumeration
   int ntx, nty, ntz;
   int64_t ch_t;
+  // bit widths of the lattice site (i, j, k) packed into the carried
+  // index of the binned order: k in the low qkb bits, j in the next qjb
+  int qkb, qjb;
 };
 
 // Per-axis Fourier tables.  For an axis of n cells and index i,
@@ -347,6 +350,26 @@ __device__ __forceinline__ void lattice_ijk(const SimDev& S, int64_t local,
   k = (int)(l - t * (unsigned)S.nz);
   i = (int)(t / (unsigned)S.ny);
   j = (int)(t - (unsigned)i * (unsigned)S.ny);
+}
+
+// The carried index of the binned order: lattice site (i, j, k) packed as
+// (i << (kb + jb)) | (j << kb) | k, so that q comes back with shifts and
+// masks instead of two integer divisions.
+__device__ __forceinline__ void unpack_site(uint32_t l, int kb, int jb,
+                                            int& i, int& j, int& k) {
+  k = (int)(l & ((1u << kb) - 1u));
+  j = (int)((l >> kb) & ((1u << jb) - 1u));
+  i = (int)(l >> (kb + jb));
+}
+__device__ __forceinline__ uint32_t pack_site(int i, int j, int k, int kb,
+                                              int jb) {
+  return ((uint32_t)i << (kb + jb)) | ((uint32_t)j << kb) | (uint32_t)k;
+}
+// Lagrangian index (i*ny + j)*nz + k of a site inside its simulation.
+__device__ __forceinline__ int64_t site_local(const SimDev& S, int i, int j,
+                                              int k) {
+  return (int64_t)(((unsigned)i * (unsigned)S.ny + (unsigned)j) *
+                       (unsigned)S.nz + (unsigned)k);
 }
 
 // Position in force-mesh units: (q + d) * bf, as the reference's

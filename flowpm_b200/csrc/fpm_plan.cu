@@ -49,6 +49,7 @@ struct Run {
   // cuFFT plans of each smaller active count.
   std::vector<int> active;
   int64_t bsum_off = 0;    // this run's chunk sums in fpm_plan::bsums
+  int min_steps = 0;       // fewest leapfrog steps of the run's simulations
   std::map<int, cufftHandle> r2c_n, c2r3_n, r2c3_n, c2r1_n;
   cufftHandle r2c = 0, c2r3 = 0;     // force mesh
   cufftHandle r2c3 = 0, c2r1 = 0;    // force mesh, adjoint
@@ -145,6 +146,7 @@ struct fpm_plan {
   float* bp[2] = {nullptr, nullptr};
   uint32_t* blag[2] = {nullptr, nullptr};
   int32_t* bcell = nullptr;
+  int32_t* bcount = nullptr;  // per-cell counts, zero between sorts
   int32_t* bsums = nullptr;
   size_t bin_bytes = 0;
   // the reverse sweep in the binned order (fpm_plan_set_adjoint_binning):
@@ -228,7 +230,7 @@ void free_all(fpm_plan* p) {
   for (void* b : bufs)
     if (b) cudaFree(b);
   void* bins[] = {p->bd[0],   p->bd[1],  p->bp[0],  p->bp[1],
-                  p->blag[0], p->blag[1], p->bcell,  p->bsums,
+                  p->blag[0], p->blag[1], p->bcell,  p->bsums, p->bcount,
                   p->blx[0],  p->blx[1], p->blp[0], p->blp[1]};
   for (void* b : bins)
     if (b) cudaFree(b);
@@ -567,6 +569,9 @@ int update_schedule(fpm_plan* p, int max_steps, const int32_t* nsteps,
     bool prefix = true;
     for (int s = r.first + 1; s < r.first + r.count; ++s)
       if (nsteps[s] > nsteps[s - 1]) prefix = false;
+    r.min_steps = nsteps[r.first];
+    for (int s = r.first + 1; s < r.first + r.count; ++s)
+      r.min_steps = std::min(r.min_steps, (int)nsteps[s]);
     std::vector<int> act(max_steps + 1, r.count);
     if (prefix)
       for (int it = 0; it <= max_steps; ++it) {
@@ -1062,6 +1067,8 @@ BinRun bin_run(const fpm_plan* p, const Run& r) {
   R.nty = S.nty;
   R.ntz = S.ntz;
   R.count = r.count;
+  R.qkb = S.qkb;
+  R.qjb = S.qjb;
   R.np = S.np;
   R.ncell = (int64_t)S.mx * S.my * S.mz;
   R.p0 = S.p_off;
@@ -1072,11 +1079,17 @@ BinRun bin_run(const fpm_plan* p, const Run& r) {
 // Counting sort of run k's particles from (d, pm, lag) -- lag NULL: the
 // caller's Lagrangian order -- into the plan's sorted buffer dst.
 int bin_sort_run(fpm_plan* p, size_t k, const float* d, const float* pm,
-                 const uint32_t* lag, int dst, cudaStream_t st) {
+                 const uint32_t* lag, int dst, bool counted, cudaStream_t st) {
   const Run& r = p->runs[k];
-  return launch_bin_sort(p->bin_tile, bin_run(p, r), d, pm, lag, p->bcell,
-                         p->bsums + r.bsum_off, p->bd[dst], p->bp[dst],
-                         p->blag[dst], st);
+  return launch_bin_sort(p->bin_tile, bin_run(p, r), d, pm, lag, p->bcount,
+                         p->bcell, p->bsums + r.bsum_off, p->bd[dst],
+                         p->bp[dst], p->blag[dst], counted, st);
+}
+
+// Whether the step kernel of step it counts the cells for the sort that
+// follows it (k_step_sorted, every simulation of run k still drifting).
+bool fused_count(const fpm_plan* p, const Run& r, int it) {
+  return p->bin_mode == FPM_BIN_CHUNKS && it < r.min_steps;
 }
 
 int64_t run_part_chunk(const fpm_plan* p, size_t k) {
@@ -1089,13 +1102,16 @@ int64_t run_tile_chunk(const fpm_plan* p, size_t k) {
   return p->sims[p->runs[k].first].ch_t;
 }
 
-BinStepArgs bin_args(const fpm_plan* p, const StepArgs& a, int cur) {
+BinStepArgs bin_args(const fpm_plan* p, const StepArgs& a, int cur,
+                     bool count = false) {
   BinStepArgs b;
   b.a = a;
   b.bd = p->bd[cur];
   b.bp = p->bp[cur];
   b.blag = p->blag[cur];
   b.cell_end = p->bcell;
+  b.count = count ? p->bcount : nullptr;
+  b.tile_log2 = p->bin_tile == 16 ? 4 : 3;
   return b;
 }
 
@@ -1104,8 +1120,11 @@ BinStepArgs bin_args(const fpm_plan* p, const StepArgs& a, int cur) {
 // every bin_every steps the particles are sorted into the other buffer.
 // The last step writes the final d, p and F back in Lagrangian order.
 int nbody_binned(fpm_plan* p, StepArgs a, cudaStream_t st) {
+  // the counts are zero between sorts; a run interrupted by an error may
+  // have left some behind
+  FPM_CUDA(cudaMemsetAsync(p->bcount, 0, sizeof(int32_t) * p->total_m, st));
   for (size_t k = 0; k < p->runs.size(); ++k)
-    FPM_TRY(bin_sort_run(p, k, a.disp, a.mom, nullptr, 0, st));
+    FPM_TRY(bin_sort_run(p, k, a.disp, a.mom, nullptr, 0, false, st));
   if (chains_ok(p)) {
     const Green G = plan_green(p);
     FPM_CUDA(cudaEventRecord(p->ev_fork, st));
@@ -1124,16 +1143,18 @@ int nbody_binned(fpm_plan* p, StepArgs a, cudaStream_t st) {
                          p->tape ? tape_phi(p, it) : p->phi, tabs_of(p), G,
                          !stencil_path(p), rs);
         a.it = it;
+        const bool sort = it < p->max_steps && (it + 1) % p->bin_every == 0;
+        const bool counted = sort && fused_count(p, r, it);
         if (p->bin_mode == FPM_BIN_CHUNKS)
           launch_step_sorted(p->d_sims, p->nsims, run_part_chunk(p, k),
-                             run_part_chunk(p, k + 1), bin_args(p, a, cur),
-                             rs);
+                             run_part_chunk(p, k + 1),
+                             bin_args(p, a, cur, counted), rs);
         else
           launch_step_binned(p->bin_tile, p->d_sims, p->nsims, c0, c1,
                              bin_args(p, a, cur), rs);
-        if (it < p->max_steps && (it + 1) % p->bin_every == 0) {
+        if (sort) {
           FPM_TRY(bin_sort_run(p, k, p->bd[cur], p->bp[cur], p->blag[cur],
-                               1 - cur, rs));
+                               1 - cur, counted, rs));
           cur = 1 - cur;
         }
       }
@@ -1149,20 +1170,24 @@ int nbody_binned(fpm_plan* p, StepArgs a, cudaStream_t st) {
     FPM_TRY(force_meshes(p, st, it < p->max_steps, it,
                          p->tape ? tape_phi(p, it) : nullptr));
     a.it = it;
+    const bool sort = it < p->max_steps && (it + 1) % p->bin_every == 0;
+    // one launch steps every run: it counts only when every run may
+    bool counted = sort;
+    for (const Run& r : p->runs) counted = counted && fused_count(p, r, it);
     prof_mark(p, 0, st);
     if (p->bin_mode == FPM_BIN_CHUNKS)
-      launch_step_sorted(p->d_sims, p->nsims, 0, p->ch_p, bin_args(p, a, cur),
-                         st);
+      launch_step_sorted(p->d_sims, p->nsims, 0, p->ch_p,
+                         bin_args(p, a, cur, counted), st);
     else
       launch_step_binned(p->bin_tile, p->d_sims, p->nsims, 0, p->total_tiles,
                          bin_args(p, a, cur), st);
     prof_mark(p, 0, st);
     FPM_TRY(launch_ok());
-    if (it < p->max_steps && (it + 1) % p->bin_every == 0) {
+    if (sort) {
       prof_mark(p, 10, st);
       for (size_t k = 0; k < p->runs.size(); ++k)
         FPM_TRY(bin_sort_run(p, k, p->bd[cur], p->bp[cur], p->blag[cur],
-                             1 - cur, st));
+                             1 - cur, counted, st));
       prof_mark(p, 10, st);
       cur = 1 - cur;
     }
@@ -1304,13 +1329,13 @@ int alloc_adj_bins(fpm_plan* p) {
 
 void free_bins(fpm_plan* p) {
   free_adj_bins(p);
-  void* bins[] = {p->bd[0], p->bd[1], p->bp[0], p->bp[1], p->blag[0],
-                  p->blag[1], p->bcell, p->bsums};
+  void* bins[] = {p->bd[0],   p->bd[1], p->bp[0],  p->bp[1],    p->blag[0],
+                  p->blag[1], p->bcell, p->bsums, p->bcount};
   for (void* b : bins)
     if (b) cudaFree(b);
   p->bd[0] = p->bd[1] = p->bp[0] = p->bp[1] = nullptr;
   p->blag[0] = p->blag[1] = nullptr;
-  p->bcell = p->bsums = nullptr;
+  p->bcell = p->bsums = p->bcount = nullptr;
   p->device_bytes -= p->bin_bytes;
   p->bin_bytes = 0;
 }
@@ -1336,6 +1361,13 @@ extern "C" int fpm_plan_set_binning(fpm_plan* p, int tile, int sort_every,
   for (const SimDev& S : p->sims)
     if (!bin_tile_supported(tile, S.mx, S.my, S.mz) || S.m_off % 4 != 0)
       return FPM_ERR_UNSUPPORTED;
+  for (const Run& r : p->runs) {
+    const SimDev& S = p->sims[r.first];
+    int kb, jb;
+    if (!bin_run_supported(S.nx, S.ny, S.nz, (int64_t)S.mx * S.my * S.mz,
+                           r.count, &kb, &jb))
+      return FPM_ERR_UNSUPPORTED;
+  }
   if (tile == p->bin_tile) {
     if (sort_every != p->bin_every || mode != p->bin_mode) {
       p->bin_every = sort_every;
@@ -1358,6 +1390,8 @@ extern "C" int fpm_plan_set_binning(fpm_plan* p, int tile, int sort_every,
     S.ntz = S.mz / tile;
     S.ch_t = tiles;
     tiles += (int64_t)S.ntx * S.nty * S.ntz;
+    bin_run_supported(S.nx, S.ny, S.nz, (int64_t)S.mx * S.my * S.mz, 1,
+                      &S.qkb, &S.qjb);
   }
   int64_t nsum = 0;
   for (auto& r : p->runs) {
@@ -1373,6 +1407,7 @@ extern "C" int fpm_plan_set_binning(fpm_plan* p, int tile, int sort_every,
     p->blag[b] = dalloc<uint32_t>(p->total_np, tot, ok);
   }
   p->bcell = dalloc<int32_t>(p->total_m, tot, ok);
+  p->bcount = dalloc<int32_t>(p->total_m, tot, ok);
   p->bsums = dalloc<int32_t>(nsum, tot, ok);
   p->bin_bytes = tot;
   p->device_bytes += tot;
@@ -1382,7 +1417,8 @@ extern "C" int fpm_plan_set_binning(fpm_plan* p, int tile, int sort_every,
     return FPM_ERR_OOM;
   }
   if (cudaMemcpy(p->d_sims, sims.data(), sizeof(SimDev) * sims.size(),
-                 cudaMemcpyHostToDevice) != cudaSuccess) {
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(p->bcount, 0, sizeof(int32_t) * p->total_m) != cudaSuccess) {
     free_bins(p);
     return FPM_ERR_CUDA;
   }
@@ -1598,8 +1634,8 @@ static int adj_sort_run(fpm_plan* p, size_t k, float* const src[4],
   pay.dst[1] = p->bp[dst];
   pay.dst[2] = p->blx[dst];
   pay.dst[3] = p->blp[dst];
-  return launch_bin_sort(p->bin_tile, bin_run(p, r), pay, lag, p->bcell,
-                         p->bsums + r.bsum_off, p->blag[dst], st);
+  return launch_bin_sort(p->bin_tile, bin_run(p, r), pay, lag, p->bcount,
+                         p->bcell, p->bsums + r.bsum_off, p->blag[dst], st);
 }
 
 // The reverse sweep of a potential-tape plan in the binned order: the
@@ -1610,6 +1646,7 @@ static int adj_sort_run(fpm_plan* p, size_t k, float* const src[4],
 // arrays in Lagrangian order for the last gather (a.it = -1).
 static int adjoint_binned(fpm_plan* p, AdjArgs a, cudaStream_t st) {
   float* user[4] = {a.disp, a.mom, a.lam_x, a.lam_p};
+  FPM_CUDA(cudaMemsetAsync(p->bcount, 0, sizeof(int32_t) * p->total_m, st));
   for (size_t k = 0; k < p->runs.size(); ++k)
     FPM_TRY(adj_sort_run(p, k, user, nullptr, 0, st));
   int cur = 0;
