@@ -1131,7 +1131,11 @@ def main():
   peak, peak_kind = peaks()
   step_ms = kt['step'] / max(kn['step'], 1)
   # the binned step also reads each particle's Lagrangian index (4 B)
-  kbytes = (KERNEL_BYTES_PER_PART + (4 if tile else 0)) * npart
+  # the binned step also reads each particle's packed lattice site (4 B);
+  # re-sorted as they move (mode 3) it also writes it to the new slot
+  binned = tile and mode != 2
+  kbytes = (KERNEL_BYTES_PER_PART + (4 if binned else 0) +
+            (4 if binned and mode == 3 else 0)) * npart
   achieved = kbytes / (step_ms * 1e-3) / 1e9
   whole = STEP_BYTES_PER_PART * npart * N_STEPS * args.steps / (ms * 1e-3) / 1e9
   line = {
@@ -1163,15 +1167,18 @@ def main():
           },
       },
       'gpu_launches': int(n_launch),
-      'traversal': ('particles sorted by cell (keys in tiles of %d^3 '
+      'traversal': ('particles re-sorted by cell (keys in tiles of %d^3 '
+                    'cells) as they move, at every step' % tile
+                    if mode == 3 else
+                    'particles sorted by cell (keys in tiles of %d^3 '
                     'cells) every %d steps, %s' % (
                         tile, every, 'equal chunks' if mode == 1 else
                         'one block per tile, shared-memory paint'))
-                   if tile else 'lattice walk',
+                   if binned else 'lattice walk',
       'autotune': tuning,
       'roofline': {
-          'kernel': (('k_step_sorted' if mode == 1 else 'k_step_binned')
-                     if tile else 'k_step') +
+          'kernel': (('k_step_binned' if mode == 0 else 'k_step_sorted')
+                     if binned else 'k_step') +
                     ' (fused readout + kick + drift + CIC paint)',
           'bound': 'hbm',
           'achieved': achieved,

@@ -133,6 +133,7 @@ FPM_TUNE_CONFIGS = 8
 FPM_BIN_TILES = 0
 FPM_BIN_CHUNKS = 1
 FPM_BIN_WALK = 2
+FPM_BIN_FLOW = 3
 FPM_STATUS_NONFINITE_POS = 1
 FPM_STATUS_NONFINITE_MOM = 2
 

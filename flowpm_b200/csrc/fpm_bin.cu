@@ -39,6 +39,18 @@ __device__ __forceinline__ unsigned cell_key(const BinRun& R, int cx, int cy,
          (lx * T + ly) * T + lz;
 }
 
+// The same key from a simulation's tile counts, tiles of 2^lt cells.
+__device__ __forceinline__ unsigned cell_key_lt(const SimDev& S, int lt,
+                                                int cx, int cy, int cz) {
+  const int tm = (1 << lt) - 1;
+  const unsigned tile = ((unsigned)(cx >> lt) * (unsigned)S.nty +
+                         (unsigned)(cy >> lt)) * (unsigned)S.ntz +
+                        (unsigned)(cz >> lt);
+  const unsigned local =
+      ((unsigned)((cx & tm) << lt | (cy & tm)) << lt) | (unsigned)(cz & tm);
+  return (tile << (3 * lt)) | local;
+}
+
 // Cell key of slot t of simulation r of the run (run-relative: + r *
 // ncell) and its packed lattice site: from the carried index when lag is
 // set, else t is the Lagrangian index itself.
@@ -253,30 +265,40 @@ k_scan_sums(const int32_t* __restrict__ v, int64_t n, int32_t* sums) {
   if (threadIdx.x == 0) sums[blockIdx.x] = total;
 }
 
-// One block: exclusive scan of the nb chunk sums, plus base.
+// One block of 1024 threads: exclusive scan of the nb chunk sums, plus
+// base (each thread sums a run of ceil(nb / 1024) of them; a two-level
+// shuffle scan over the 32 warps combines the runs).
 __global__ void __launch_bounds__(1024)
 k_scan_top(int32_t* sums, int nb, int32_t base) {
-  __shared__ int part[1024];
+  __shared__ int wsum[32];
   const int per = (nb + 1023) / 1024;
   const int b0 = threadIdx.x * per;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int s = 0;
   for (int i = 0; i < per && b0 + i < nb; ++i) s += sums[b0 + i];
-  part[threadIdx.x] = s;
+  int x = s;  // inclusive scan over the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int acc = base;
-    for (int t = 0; t < 1024; ++t) {
-      const int x = part[t];
-      part[t] = acc;
-      acc += x;
+  if (w == 0) {
+    int t = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
     }
+    wsum[lane] = t;  // inclusive over warps
   }
   __syncthreads();
-  int acc = part[threadIdx.x];
+  int acc = base + (x - s) + (w > 0 ? wsum[w - 1] : 0);
   for (int i = 0; i < per && b0 + i < nb; ++i) {
-    const int x = sums[b0 + i];
+    const int v = sums[b0 + i];
     sums[b0 + i] = acc;
-    acc += x;
+    acc += v;
   }
 }
 
@@ -485,17 +507,36 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
       const bool valid = i < end;  // warp-uniform except in a sim's last chunk
       uint32_t l = 0;
       float3 d = make_float3(0.f, 0.f, 0.f), p = d;
+      int qi = 0, qj = 0, qk = 0;
       if (valid) {
-        l = b.blag[i];
         d = ld3(b.bd, i);
         p = ld3(b.bp, i);
+        if (b.blag) {
+          l = b.blag[i];
+          unpack_site(l, S.qkb, S.qjb, qi, qj, qk);
+        } else {  // Lagrangian order: slot i is lattice site i - p_off
+          lattice_ijk(S, i - S.p_off, qi, qj, qk);
+          l = pack_site(qi, qj, qk, S.qkb, S.qjb);
+        }
       }
-      int qi, qj, qk;
-      unpack_site(l, S.qkb, S.qjb, qi, qj, qk);
       const int64_t g = S.p_off + site_local(S, qi, qj, qk);  // Lagrangian
       const float3 x = mesh_pos(S, qi, qj, qk, d);
-      const Cic8 c0 = cic8(cic_axis(x.x, S.mx), cic_axis(x.y, S.my),
-                           cic_axis(x.z, S.mz), S.my, S.mz);
+      const Axis ax0 = cic_axis(x.x, S.mx), ay0 = cic_axis(x.y, S.my),
+                 az0 = cic_axis(x.z, S.mz);
+      const Cic8 c0 = cic8(ax0, ay0, az0, S.my, S.mz);
+      // re-sorted as it moves: the run of lanes in this cell claims its
+      // slots now; the claim's latency overlaps the readout
+      int claim_base = 0;
+      unsigned claim_heads = 0xffffffffu;
+      if (b.claim && !last) {
+        const unsigned k0 = valid ? c0.row[0] + c0.z0 : 0xffffffffu - lane;
+        claim_heads = run_heads(k0, lane);
+        if (valid && ((claim_heads >> lane) & 1u))
+          claim_base = atomicAdd(
+              b.claim + S.m_off +
+                  cell_key_lt(S, b.tile_log2, ax0.i0, ay0.i0, az0.i0),
+              (int32_t)run_length(claim_heads, lane));
+      }
       float3 f = valid ? readout_cic8(a.fmesh + 3 * S.m_off, mcells, c0)
                        : make_float3(0.f, 0.f, 0.f);
       // force = readout * factor / pm_nc_factor (flowpm/tfpm.py:218, :356)
@@ -530,12 +571,21 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
       p = axpy(p, ks, f);  // opening kick of step it
       d = axpy(d, dr, p);  // drift of step it
       const float3 xn = mesh_pos(S, qi, qj, qk, d);
-      if (valid) {
+      if (b.claim) {
+        const int h = run_head(claim_heads, lane);
+        const int base = __shfl_sync(0xffffffffu, claim_base, h);
+        if (valid) {
+          const int64_t o = (int64_t)base + (lane - h);
+          st3(b.op, o, p);
+          st3(b.od, o, d);
+          b.olag[o] = l;
+        }
+      } else if (valid) {
         st3(b.bp, i, p);
         st3(b.bd, i, d);
-        if (!finite3(xn.x, xn.y, xn.z))
-          atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
       }
+      if (valid && !finite3(xn.x, xn.y, xn.z))
+        atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
       const Axis nx1 = cic_axis(xn.x, S.mx), ny1 = cic_axis(xn.y, S.my),
                  nz1 = cic_axis(xn.z, S.mz);
       const Cic8 c1 = cic8(nx1, ny1, nz1, S.my, S.mz);
@@ -547,18 +597,10 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
       if (b.count) {
         // the sort after this step: one count per run of lanes in a cell
         const unsigned hs = __ballot_sync(0xffffffffu, head);
-        if (valid && head) {
-          const int lt = b.tile_log2, tm = (1 << lt) - 1;
-          const unsigned tile =
-              ((unsigned)(nx1.i0 >> lt) * (unsigned)S.nty +
-               (unsigned)(ny1.i0 >> lt)) * (unsigned)S.ntz +
-              (unsigned)(nz1.i0 >> lt);
-          const unsigned local =
-              ((unsigned)((nx1.i0 & tm) << lt | (ny1.i0 & tm)) << lt) |
-              (unsigned)(nz1.i0 & tm);
-          atomicAdd(b.count + S.m_off + ((tile << (3 * lt)) | local),
+        if (valid && head)
+          atomicAdd(b.count + S.m_off +
+                        cell_key_lt(S, b.tile_log2, nx1.i0, ny1.i0, nz1.i0),
                     (int32_t)run_length(hs, lane));
-        }
       }
       float w[8];
 #pragma unroll
@@ -672,19 +714,44 @@ void launch_scatter(int tile, unsigned blocks, const BinRun& R,
 
 }  // namespace
 
+#define FPM_RET(x)                 \
+  do {                             \
+    const int rc_ = (x);           \
+    if (rc_ != FPM_OK) return rc_; \
+  } while (0)
+
+int launch_bin_scan(const BinRun& R, int32_t* count, int32_t* cell,
+                    int32_t* sums, cudaStream_t st) {
+  const int64_t ncells = (int64_t)R.count * R.ncell;
+  const int nb = (int)bin_scan_blocks(ncells);
+  g_launches.fetch_add(3, std::memory_order_relaxed);
+  k_scan_sums<<<nb, kScanThreads, 0, st>>>(count + R.m0, ncells, sums);
+  k_scan_top<<<1, 1024, 0, st>>>(sums, nb, (int32_t)R.p0);
+  k_scan_apply<<<nb, kScanThreads, 0, st>>>(count + R.m0, cell + R.m0, ncells,
+                                            sums);
+  return cudaGetLastError() == cudaSuccess ? FPM_OK : FPM_ERR_CUDA;
+}
+
+int launch_bin_count_scan(int tile, const BinRun& R, const float* d,
+                          const uint32_t* lag, int32_t* count, int32_t* cell,
+                          int32_t* sums, cudaStream_t st) {
+  const unsigned blocks = (unsigned)sort_blocks(R);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (tile == 8)
+    k_bin_count<8><<<blocks, kThreads, 0, st>>>(R, d, lag, count);
+  else
+    k_bin_count<16><<<blocks, kThreads, 0, st>>>(R, d, lag, count);
+  return launch_bin_scan(R, count, cell, sums, st);
+}
+
 int launch_bin_scan_scatter(int tile, const BinRun& R, const BinPayload& pay,
                             const uint32_t* lag, int32_t* count,
                             int32_t* cell, int32_t* sums, uint32_t* lag_out,
                             cudaStream_t st) {
   if (pay.n != 2 && pay.n != 4) return FPM_ERR_ARG;
-  const int64_t ncells = (int64_t)R.count * R.ncell;
+  FPM_RET(launch_bin_scan(R, count, cell, sums, st));
   const unsigned blocks = (unsigned)sort_blocks(R);
-  g_launches.fetch_add(4, std::memory_order_relaxed);
-  const int nb = (int)bin_scan_blocks(ncells);
-  k_scan_sums<<<nb, kScanThreads, 0, st>>>(count + R.m0, ncells, sums);
-  k_scan_top<<<1, 1024, 0, st>>>(sums, nb, (int32_t)R.p0);
-  k_scan_apply<<<nb, kScanThreads, 0, st>>>(count + R.m0, cell + R.m0, ncells,
-                                            sums);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   if (pay.n == 2)
     launch_scatter<2>(tile, blocks, R, pay, lag, cell, lag_out, st);
   else

@@ -54,6 +54,17 @@ int launch_bin_sort(int tile, const BinRun& R, const float* d,
                     int32_t* cell, int32_t* sums, float* d_out, float* p_out,
                     uint32_t* lag_out, bool counted, cudaStream_t st);
 
+// The first half of a sort: counts of the cells of (d, lag) -- lag NULL:
+// Lagrangian order -- into count (zero on entry), scanned into cell (the
+// first slot of each cell, plus p0) with count left zero.
+int launch_bin_count_scan(int tile, const BinRun& R, const float* d,
+                          const uint32_t* lag, int32_t* count, int32_t* cell,
+                          int32_t* sums, cudaStream_t st);
+
+// The scan alone (counts already in count, left zero).
+int launch_bin_scan(const BinRun& R, int32_t* count, int32_t* cell,
+                    int32_t* sums, cudaStream_t st);
+
 // The same sort of the payload's arrays.
 int launch_bin_sort(int tile, const BinRun& R, const BinPayload& pay,
                     const uint32_t* lag, int32_t* count, int32_t* cell,
@@ -80,6 +91,15 @@ struct BinStepArgs {
   // simulation at its m_off) for the sort that follows the step
   int32_t* count;
   int tile_log2;
+  // k_step_sorted only, the particles re-sorted as they move (FPM_BIN_FLOW):
+  // with claim set, each particle claims claim[key of its cell at the start
+  // of the step]++ (the scan of the previous step's counts) and writes its
+  // updated (d, p, site) there in (od, op, olag) instead of in place; with
+  // blag NULL the input (bd, bp) is in Lagrangian order
+  int32_t* claim;
+  float* od;
+  float* op;
+  uint32_t* olag;
 };
 
 // The step over the tile chunks [ch0, ch1) (whole simulations), painting

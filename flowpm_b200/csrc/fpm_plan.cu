@@ -50,6 +50,7 @@ struct Run {
   std::vector<int> active;
   int64_t bsum_off = 0;    // this run's chunk sums in fpm_plan::bsums
   int min_steps = 0;       // fewest leapfrog steps of the run's simulations
+  int max_steps = 0;       // most leapfrog steps of the run's simulations
   std::map<int, cufftHandle> r2c_n, c2r3_n, r2c3_n, c2r1_n;
   cufftHandle r2c = 0, c2r3 = 0;     // force mesh
   cufftHandle r2c3 = 0, c2r1 = 0;    // force mesh, adjoint
@@ -569,9 +570,11 @@ int update_schedule(fpm_plan* p, int max_steps, const int32_t* nsteps,
     bool prefix = true;
     for (int s = r.first + 1; s < r.first + r.count; ++s)
       if (nsteps[s] > nsteps[s - 1]) prefix = false;
-    r.min_steps = nsteps[r.first];
-    for (int s = r.first + 1; s < r.first + r.count; ++s)
+    r.min_steps = r.max_steps = nsteps[r.first];
+    for (int s = r.first + 1; s < r.first + r.count; ++s) {
       r.min_steps = std::min(r.min_steps, (int)nsteps[s]);
+      r.max_steps = std::max(r.max_steps, (int)nsteps[s]);
+    }
     std::vector<int> act(max_steps + 1, r.count);
     if (prefix)
       for (int it = 0; it <= max_steps; ++it) {
@@ -1089,7 +1092,7 @@ int bin_sort_run(fpm_plan* p, size_t k, const float* d, const float* pm,
 // Whether the step kernel of step it counts the cells for the sort that
 // follows it (k_step_sorted, every simulation of run k still drifting).
 bool fused_count(const fpm_plan* p, const Run& r, int it) {
-  return p->bin_mode == FPM_BIN_CHUNKS && it < r.min_steps;
+  return p->bin_mode != FPM_BIN_TILES && it < r.min_steps;
 }
 
 int64_t run_part_chunk(const fpm_plan* p, size_t k) {
@@ -1112,7 +1115,106 @@ BinStepArgs bin_args(const fpm_plan* p, const StepArgs& a, int cur,
   b.cell_end = p->bcell;
   b.count = count ? p->bcount : nullptr;
   b.tile_log2 = p->bin_tile == 16 ? 4 : 3;
+  b.claim = nullptr;  // in place unless nbody_flow sets the claims
+  b.od = b.op = nullptr;
+  b.olag = nullptr;
   return b;
+}
+
+// Whether every run's simulations take the same number of steps (the
+// particles re-sorted as they move keep a simulation's slots only when
+// every one of them moves at every step).
+bool runs_uniform(const fpm_plan* p) {
+  for (const Run& r : p->runs)
+    if (r.min_steps != r.max_steps) return false;
+  return true;
+}
+
+// The leapfrog with the particles re-sorted as they move (FPM_BIN_FLOW):
+// the cells of the caller's Lagrangian state are counted and scanned into
+// first slots; then at every step each particle claims the next slot of
+// its cell at the start of the step and k_step_sorted writes it there in
+// the other buffer, counting the cells of the drifted particles for the
+// next step's scan.  The order a step sees is its previous step's, with no
+// sort pass; the last step writes the final d, p and F in Lagrangian order.
+int nbody_flow(fpm_plan* p, StepArgs a, cudaStream_t st) {
+  FPM_CUDA(cudaMemsetAsync(p->bcount, 0, sizeof(int32_t) * p->total_m, st));
+  auto args = [&](int cur, int it, const Run* r) {
+    // cur < 0: the caller's Lagrangian arrays
+    BinStepArgs b = bin_args(p, a, cur < 0 ? 0 : cur);
+    const int nxt = cur < 0 ? 0 : 1 - cur;
+    if (cur < 0) {
+      b.bd = a.disp;
+      b.bp = a.mom;
+      b.blag = nullptr;
+    }
+    const int T = r ? r->min_steps : p->max_steps;
+    if (it < T) {
+      b.claim = p->bcell;
+      b.count = p->bcount;
+      b.od = p->bd[nxt];
+      b.op = p->bp[nxt];
+      b.olag = p->blag[nxt];
+    }
+    b.a.it = it;
+    return b;
+  };
+  for (size_t k = 0; k < p->runs.size(); ++k) {
+    const Run& r = p->runs[k];
+    FPM_TRY(launch_bin_count_scan(p->bin_tile, bin_run(p, r), a.disp, nullptr,
+                                  p->bcount, p->bcell,
+                                  p->bsums + r.bsum_off, st));
+  }
+  if (chains_ok(p)) {
+    const Green G = plan_green(p);
+    FPM_CUDA(cudaEventRecord(p->ev_fork, st));
+    for (size_t k = 0; k < p->runs.size(); ++k) {
+      Run& r = p->runs[k];
+      const SimDev& S = p->sims[r.first];
+      cudaStream_t rs = k == 0 ? st : p->side[k - 1];
+      if (k > 0) FPM_CUDA(cudaStreamWaitEvent(rs, p->ev_fork, 0));
+      int cur = -1;
+      for (int it = 0; it <= r.min_steps; ++it) {
+        launch_fft_force(p->d_sims, r.first, r.count, S.mx, S.my, S.mz,
+                         p->rho, it < p->max_steps ? 1 : 0, p->dk, p->fk,
+                         p->fmesh, p->tape ? tape_phi(p, it) : p->phi,
+                         tabs_of(p), G, !stencil_path(p), rs);
+        launch_step_sorted(p->d_sims, p->nsims, run_part_chunk(p, k),
+                           run_part_chunk(p, k + 1), args(cur, it, &r), rs);
+        if (it < r.min_steps) {
+          FPM_TRY(launch_bin_scan(bin_run(p, r), p->bcount, p->bcell,
+                                  p->bsums + r.bsum_off, rs));
+          cur = cur < 0 ? 0 : 1 - cur;
+        }
+      }
+      if (k > 0) {
+        FPM_CUDA(cudaEventRecord(p->ev_join[k - 1], rs));
+        FPM_CUDA(cudaStreamWaitEvent(st, p->ev_join[k - 1], 0));
+      }
+    }
+    return launch_ok();
+  }
+  int cur = -1;
+  for (int it = 0; it <= p->max_steps; ++it) {
+    FPM_TRY(force_meshes(p, st, it < p->max_steps, it,
+                         p->tape ? tape_phi(p, it) : nullptr));
+    prof_mark(p, 0, st);
+    launch_step_sorted(p->d_sims, p->nsims, 0, p->ch_p,
+                       args(cur, it, nullptr), st);
+    prof_mark(p, 0, st);
+    FPM_TRY(launch_ok());
+    if (it < p->max_steps) {
+      prof_mark(p, 10, st);
+      for (size_t k = 0; k < p->runs.size(); ++k) {
+        const Run& r = p->runs[k];
+        FPM_TRY(launch_bin_scan(bin_run(p, r), p->bcount, p->bcell,
+                                p->bsums + r.bsum_off, st));
+      }
+      prof_mark(p, 10, st);
+      cur = cur < 0 ? 0 : 1 - cur;
+    }
+  }
+  return FPM_OK;
 }
 
 // The leapfrog on the binned step: the caller's Lagrangian state is sorted
@@ -1120,6 +1222,7 @@ BinStepArgs bin_args(const fpm_plan* p, const StepArgs& a, int cur,
 // every bin_every steps the particles are sorted into the other buffer.
 // The last step writes the final d, p and F back in Lagrangian order.
 int nbody_binned(fpm_plan* p, StepArgs a, cudaStream_t st) {
+  if (p->bin_mode == FPM_BIN_FLOW && runs_uniform(p)) return nbody_flow(p, a, st);
   // the counts are zero between sorts; a run interrupted by an error may
   // have left some behind
   FPM_CUDA(cudaMemsetAsync(p->bcount, 0, sizeof(int32_t) * p->total_m, st));
@@ -1145,7 +1248,7 @@ int nbody_binned(fpm_plan* p, StepArgs a, cudaStream_t st) {
         a.it = it;
         const bool sort = it < p->max_steps && (it + 1) % p->bin_every == 0;
         const bool counted = sort && fused_count(p, r, it);
-        if (p->bin_mode == FPM_BIN_CHUNKS)
+        if (p->bin_mode != FPM_BIN_TILES)
           launch_step_sorted(p->d_sims, p->nsims, run_part_chunk(p, k),
                              run_part_chunk(p, k + 1),
                              bin_args(p, a, cur, counted), rs);
@@ -1175,7 +1278,7 @@ int nbody_binned(fpm_plan* p, StepArgs a, cudaStream_t st) {
     bool counted = sort;
     for (const Run& r : p->runs) counted = counted && fused_count(p, r, it);
     prof_mark(p, 0, st);
-    if (p->bin_mode == FPM_BIN_CHUNKS)
+    if (p->bin_mode != FPM_BIN_TILES)
       launch_step_sorted(p->d_sims, p->nsims, 0, p->ch_p,
                          bin_args(p, a, cur, counted), st);
     else
@@ -1346,7 +1449,7 @@ extern "C" int fpm_plan_set_binning(fpm_plan* p, int tile, int sort_every,
                                     int mode) {
   if (!p || tile < 0 || sort_every < 1 ||
       (mode != FPM_BIN_TILES && mode != FPM_BIN_CHUNKS &&
-       mode != FPM_BIN_WALK))
+       mode != FPM_BIN_WALK && mode != FPM_BIN_FLOW))
     return FPM_ERR_ARG;
   if (tile == 0) {
     if (p->bin_tile) {
@@ -2242,12 +2345,13 @@ namespace {
 
 // (tile, sort period, mode) of each configuration fpm_plan_autotune times:
 // the lattice walk; the sorted particles in equal chunks (keys tile-major
-// in tiles of 8 or 16 cells) re-sorted every 1, 2 or 4 leapfrog steps; the
-// shared-memory tiles of 8 or 16 cells re-sorted every 4 steps.
+// in tiles of 16 cells) re-sorted every 2, 3, 4 or 6 leapfrog steps, or in
+// tiles of 8 every 4; re-sorted as they move, in tiles of 16; the
+// shared-memory tiles of 16 cells re-sorted every 4 steps.
 constexpr int kTune[FPM_TUNE_CONFIGS][3] = {
-    {0, 1, FPM_BIN_CHUNKS},  {8, 1, FPM_BIN_CHUNKS},  {8, 2, FPM_BIN_CHUNKS},
-    {8, 4, FPM_BIN_CHUNKS},  {16, 2, FPM_BIN_CHUNKS}, {16, 4, FPM_BIN_CHUNKS},
-    {8, 4, FPM_BIN_TILES},   {16, 4, FPM_BIN_TILES}};
+    {0, 1, FPM_BIN_CHUNKS},  {16, 2, FPM_BIN_CHUNKS}, {16, 3, FPM_BIN_CHUNKS},
+    {16, 4, FPM_BIN_CHUNKS}, {16, 6, FPM_BIN_CHUNKS}, {8, 4, FPM_BIN_CHUNKS},
+    {16, 1, FPM_BIN_FLOW},   {16, 4, FPM_BIN_TILES}};
 
 std::mutex g_tune_mu;
 // choice per (device, plan flags, step count, PGD, tape, dims...)

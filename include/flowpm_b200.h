@@ -241,7 +241,12 @@ int fpm_pgd(fpm_plan* plan, float* disp, const double* params, void* stream);
  * FPM_BIN_CHUNKS steps the sorted particles in equal chunks, painting into
  * the density directly with warp-summed deposits of neighbouring lanes;
  * FPM_BIN_TILES gives each tile to one block, which paints into a
- * shared-memory copy of the tile; FPM_BIN_WALK keeps the forward on the
+ * shared-memory copy of the tile; FPM_BIN_FLOW re-sorts the particles at
+ * every step without a sort pass: each step kernel writes every particle to
+ * the next free slot of its cell in the other buffer and counts the cells
+ * of the drifted particles for the next step (sort_every is ignored; runs
+ * whose simulations take different step counts fall back to
+ * FPM_BIN_CHUNKS); FPM_BIN_WALK keeps the forward on the
  * lattice walk and only provides the tiles and buffers for the reverse
  * sweep's binned order (fpm_plan_set_adjoint_binning).  The caller's
  * arrays stay in Lagrangian
@@ -251,7 +256,12 @@ int fpm_pgd(fpm_plan* plan, float* disp, const double* params, void* stream);
  * fpm_plan_destroy), synchronising the device; every force mesh must divide
  * into tiles (else FPM_ERR_UNSUPPORTED).  Plans with PGD switched on keep
  * the lattice walk.  Captured graphs of the plan must be captured again. */
-enum { FPM_BIN_TILES = 0, FPM_BIN_CHUNKS = 1, FPM_BIN_WALK = 2 };
+enum {
+  FPM_BIN_TILES = 0,
+  FPM_BIN_CHUNKS = 1,
+  FPM_BIN_WALK = 2,
+  FPM_BIN_FLOW = 3
+};
 int fpm_plan_set_binning(fpm_plan* plan, int tile, int sort_every, int mode);
 
 /* The reverse sweep (fpm_nbody_adjoint) of a plan with a potential tape in

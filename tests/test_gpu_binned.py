@@ -46,7 +46,7 @@ def binned(fpm):
     p.set_binning(0)
 
 
-MODES = [(8, 1, 1), (16, 3, 1), (8, 4, 0), (16, 2, 0)]
+MODES = [(8, 1, 1), (16, 3, 1), (8, 4, 0), (16, 2, 0), (16, 1, 3), (8, 1, 3)]
 
 
 @pytest.mark.parametrize('tile,every,mode', MODES)
@@ -80,7 +80,8 @@ def test_binned_c1_density(fpm, binned, capsys):
   zeros = lambda: torch.zeros((1, 32, 32, 32))
   walk = host(fpm.cic_paint(zeros(), fpm.nbody(c, s0, stages, 32)[0]))
   errs = {}
-  for tile, every, mode in ((8, 1, 1), (16, 2, 1), (8, 5, 0), (16, 2, 0)):
+  for tile, every, mode in ((8, 1, 1), (16, 2, 1), (8, 5, 0), (16, 2, 0),
+                            (16, 1, 3)):
     binned([(32, 32, 32, 1)], tile, every, mode=mode)
     rho = host(fpm.cic_paint(zeros(), fpm.nbody(c, s0, stages, 32)[0]))
     e = errs[(tile, every, mode)] = (rel_l2(rho, z['n32_rho']),
@@ -120,7 +121,9 @@ def test_binned_batch_uneven(fpm):
     r.load(states)
     r.run()
     ref = [host(s) for s in r.results()]
-    for tile, every, mode in ((8, 1, 1), (16, 2, 1), (8, 2, 0)):
+    # (16, 1, 3): the mix's runs take different step counts, so the flow
+    # mode falls back to re-sorting every step
+    for tile, every, mode in ((8, 1, 1), (16, 2, 1), (8, 2, 0), (16, 1, 3)):
       r.set_binning(tile, every, mode)
       r.load(states)
       r.run()
@@ -156,14 +159,15 @@ def test_binned_forward_gradient(fpm, binned, store):
 
   from flowpm_b200 import _lib
   g0 = grad()
-  for mode in (0, 1):
+  for mode in (0, 1, 3):
     binned([(16, 16, 16, 1)], 8, 2, flags=_lib.FPM_PLAN_ADJOINT, mode=mode)
     g1 = grad()
     assert rel_l2(g1, g0) < 1e-4
 
 
 @pytest.mark.parametrize('nc,adj_every,mode', [(16, 1, 1), (16, 3, 2),
-                                                (32, 2, 1), (32, 1, 2)])
+                                                (32, 2, 1), (32, 1, 2),
+                                                (32, 2, 3)])
 def test_binned_reverse_sweep(fpm, binned, nc, adj_every, mode):
   """The potential-tape reverse sweep over the binned particle order
   (fpm_plan_set_adjoint_binning: sorted state and cotangents, re-sorted
@@ -266,10 +270,10 @@ def test_autotune_picks_and_caches(fpm):
     assert torch.equal(d0, keep[0]) and torch.equal(p0, keep[1])
     assert all(v is not None and v > 0 for v in ms.values()), ms
     best = min(ms, key=lambda k: ms[k])
-    names = {'walk': (0, 1, 1), 'chunks8/1': (8, 1, 1), 'chunks8/2': (8, 2, 1),
-             'chunks8/4': (8, 4, 1), 'chunks16/2': (16, 2, 1),
-             'chunks16/4': (16, 4, 1), 'tiles8/4': (8, 4, 0),
-             'tiles16/4': (16, 4, 0)}
+    names = {'walk': (0, 1, 1), 'chunks16/2': (16, 2, 1),
+             'chunks16/3': (16, 3, 1), 'chunks16/4': (16, 4, 1),
+             'chunks16/6': (16, 6, 1), 'chunks8/4': (8, 4, 1),
+             'flow16': (16, 1, 3), 'tiles16/4': (16, 4, 0)}
     assert choice == names[best]
     outs = {}
     for plan in (p, q):  # p tuned, q the lattice walk
