@@ -49,9 +49,10 @@ WORKLOAD = ('C2: forward PM, 128^3 particles / 128^3 mesh, box 200 Mpc/h, '
 STEP_BYTES_PER_PART = 124
 KERNEL_BYTES_PER_PART = 64
 # DRAM bytes (read + write) of one step-kernel launch at 128^3, from one
-# ncu capture each, by tile (0: the lattice walk's k_step,
-# dram__bytes_read.sum + dram__bytes_write.sum = 84.1 + 8.3 MB).
-KSTEP_TRAFFIC_BYTES_128 = {0: 92.4e6}
+# ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum), by
+# traversal: the lattice walk's k_step 84.1 + 8.3 MB; k_step_sorted (keys
+# in tiles of 16 cells, equal chunks) 92.4 + 11.7 MB.
+KSTEP_TRAFFIC_BYTES_128 = {'walk': 92.4e6, (16, 1): 104.1e6}
 L2_FLUSH_BYTES = 256 << 20
 # sort periods (in positions) of the reverse sweep over the binned particle
 # order that C4 and C5 time beside the lattice walk's, and the cell tile of
@@ -1186,7 +1187,8 @@ def main():
           'peak_kind': peak_kind,
           'unit': 'GB/s',
           'frac': achieved / peak,
-          'traffic': KSTEP_TRAFFIC_BYTES_128.get(tile) if N_MESH == 128
+          'traffic': KSTEP_TRAFFIC_BYTES_128.get(
+              (tile, mode) if binned else 'walk') if N_MESH == 128
                      else None,
           'algorithmic_bytes_per_launch': kbytes,
           'avg_launch_ms': step_ms,

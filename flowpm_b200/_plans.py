@@ -73,8 +73,8 @@ class Plan(object):
     for g in self._graphs.values():
       _lib.lib.fpm_graph_destroy(g)
     self._graphs = {}
-    names = ['walk', 'chunks16/2', 'chunks16/3', 'chunks16/4', 'chunks16/6',
-             'chunks8/4', 'flow16', 'tiles16/4']
+    names = ['walk', 'chunks16/4', 'chunks16/6', 'chunks16/10', 'chunks16/16',
+             'chunks8/10', 'flow16', 'tiles16/4']
     return self.binning, {n: (float(t) if t >= 0 else None)
                           for n, t in zip(names, ms)}
 

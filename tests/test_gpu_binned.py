@@ -270,9 +270,9 @@ def test_autotune_picks_and_caches(fpm):
     assert torch.equal(d0, keep[0]) and torch.equal(p0, keep[1])
     assert all(v is not None and v > 0 for v in ms.values()), ms
     best = min(ms, key=lambda k: ms[k])
-    names = {'walk': (0, 1, 1), 'chunks16/2': (16, 2, 1),
-             'chunks16/3': (16, 3, 1), 'chunks16/4': (16, 4, 1),
-             'chunks16/6': (16, 6, 1), 'chunks8/4': (8, 4, 1),
+    names = {'walk': (0, 1, 1), 'chunks16/4': (16, 4, 1),
+             'chunks16/6': (16, 6, 1), 'chunks16/10': (16, 10, 1),
+             'chunks16/16': (16, 16, 1), 'chunks8/10': (8, 10, 1),
              'flow16': (16, 1, 3), 'tiles16/4': (16, 4, 0)}
     assert choice == names[best]
     outs = {}
