@@ -57,7 +57,7 @@ L2_FLUSH_BYTES = 256 << 20
 # sort periods (in positions) of the reverse sweep over the binned particle
 # order that C4 and C5 time beside the lattice walk's, and the cell tile of
 # the keys when the forward keeps the lattice walk
-ADJ_SORT_PERIODS = (1, 2, 4)
+ADJ_SORT_PERIODS = (4, 8, 1 << 20)  # 1 << 20: sorted once, at the start
 ADJ_TILE = 16
 # seed of replica r's linear field: replicas.replica_seed(1000, r)
 REPLICA_SEED_BASE = 1000
@@ -383,6 +383,12 @@ def _timed(fn, reps, flush):
   return float(np.median(ts))
 
 
+def _sorted_name(k):
+  """Method name of the reverse sweep in the binned order, re-sorted every
+  k positions."""
+  return 'potential_tape_sorted' + ('_once' if k >= 1 << 20 else str(k))
+
+
 def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5):
   """Config C4: 128^3, 20 steps, chi^2 of the final CIC density against
   (that density + N(0, 1) noise); gradient with respect to the initial
@@ -469,14 +475,13 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5):
   # the reverse sweep over the binned particle order (re-sorted every k
   # positions) takes its cell tiles from the forward's binning, or, when
   # the forward keeps the lattice walk, from tiles set for it alone
-  sorted_k = ADJ_SORT_PERIODS
-  methods = ['potential_tape', 'rebuilt'] + [
-      'potential_tape_sorted%d' % k for k in sorted_k]
+  sorted_k = {_sorted_name(k): k for k in ADJ_SORT_PERIODS}
+  methods = ['potential_tape', 'rebuilt'] + list(sorted_k)
   for method in methods:
-    if method.startswith('potential_tape_sorted'):
+    if method in sorted_k:
       if not plan.binning[0]:
         plan.set_binning(ADJ_TILE, 1, _lib.FPM_BIN_WALK)
-      plan.set_adjoint_binning(int(method[len('potential_tape_sorted'):]))
+      plan.set_adjoint_binning(sorted_k[method])
     capture('rebuilt' if method == 'rebuilt' else 'potential_tape')
     if method == 'potential_tape':
       forward()
@@ -499,17 +504,16 @@ def measure_fwd_adjoint(fpm, flush, reps, n=128, steps=20, ckpt=5):
   plan.set_binning(0)
   b = grads['rebuilt'].double()
   rel = lambda m: float((grads[m].double() - b).norm() / b.norm())
-  tape = ['potential_tape'] + ['potential_tape_sorted%d' % k
-                               for k in sorted_k]
+  tape = ['potential_tape'] + list(sorted_k)
   best = max(tape, key=lambda m: out[m]['value'])
   out['method'] = best
   out['value'] = out[best]['value']
   out['ms_per_step'] = out[best]['ms_per_step']
   out['potential_tape_gb'] = phi_tape.numel() * 4 / 1e9
   out['lam_x_rel_l2_tape_vs_rebuilt'] = rel('potential_tape')
-  for k in sorted_k:
-    out['lam_x_rel_l2_sorted%d_vs_rebuilt' % k] = rel(
-        'potential_tape_sorted%d' % k)
+  for name in sorted_k:
+    out['lam_x_rel_l2_%s_vs_rebuilt' % name[len('potential_tape_'):]] = rel(
+        name)
   return out
 
 
@@ -829,7 +833,8 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
           kk[name] = {'avg_launch_ms': tot.value / cnt.value,
                       'launches': cnt.value}
       _lib.call('fpm_plan_profile', plan.handle, 0)
-      sorted_adj[k] = {'value': 2.0 * np_ * steps / (t_k * 1e-3),
+      sorted_adj[k] = {'sort_every': k,
+                       'value': 2.0 * np_ * steps / (t_k * 1e-3),
                        'forward_adjoint_ms': t_k, 'kernels': kk}
     plan.set_adjoint_binning(0)
   kb, pk = fpm.power_spectrum(rho, kmin=0.01, dk=0.01, boxsize=[box] * 3)
@@ -916,7 +921,7 @@ def measure_large(fpm, flush, reps=2, n=512, steps=30, ckpt=5, tape=True):
   method, t_best = 'potential_tape' if tape else 'rebuilt', t_all
   for k, v in (sorted_adj or {}).items():
     if k != 'error' and v['forward_adjoint_ms'] < t_best:
-      method, t_best = 'potential_tape_sorted%d' % k, v['forward_adjoint_ms']
+      method, t_best = _sorted_name(k), v['forward_adjoint_ms']
   if sorted_adj:
     for v in sorted_adj.values():
       a = v.get('kernels', {}).get('adj_drift_vjp') if isinstance(

@@ -74,7 +74,7 @@ class Plan(object):
       _lib.lib.fpm_graph_destroy(g)
     self._graphs = {}
     names = ['walk', 'chunks16/4', 'chunks16/6', 'chunks16/10', 'chunks16/16',
-             'chunks8/10', 'flow16', 'tiles16/4']
+             'chunks16/once', 'flow16', 'tiles16/4']
     return self.binning, {n: (float(t) if t >= 0 else None)
                           for n, t in zip(names, ms)}
 

@@ -2346,11 +2346,12 @@ namespace {
 // (tile, sort period, mode) of each configuration fpm_plan_autotune times:
 // the lattice walk; the sorted particles in equal chunks (keys tile-major
 // in tiles of 16 cells) re-sorted every 4, 6, 10 or 16 leapfrog steps, or
-// in tiles of 8 every 10; re-sorted as they move, in tiles of 16; the
+// sorted once at the start; re-sorted as they move, in tiles of 16; the
 // shared-memory tiles of 16 cells re-sorted every 4 steps.
 constexpr int kTune[FPM_TUNE_CONFIGS][3] = {
     {0, 1, FPM_BIN_CHUNKS},  {16, 4, FPM_BIN_CHUNKS}, {16, 6, FPM_BIN_CHUNKS},
-    {16, 10, FPM_BIN_CHUNKS}, {16, 16, FPM_BIN_CHUNKS}, {8, 10, FPM_BIN_CHUNKS},
+    {16, 10, FPM_BIN_CHUNKS}, {16, 16, FPM_BIN_CHUNKS},
+    {16, 1 << 20, FPM_BIN_CHUNKS},
     {16, 1, FPM_BIN_FLOW},   {16, 4, FPM_BIN_TILES}};
 
 std::mutex g_tune_mu;

@@ -236,7 +236,8 @@ int fpm_pgd(fpm_plan* plan, float* disp, const double* params, void* stream);
  * the reference's tf.scatter_nd / tf.gather_nd, flowpm/utils.py:87-89,
  * :207-209, which is arbitrary): with tile 8 or 16, fpm_nbody_run keeps the
  * particle state sorted by force-mesh cell, cell keys tile-major in tiles
- * of tile^3 cells, and re-sorts it every sort_every leapfrog steps
+ * of tile^3 cells, and re-sorts it every sort_every leapfrog steps (a
+ * period longer than the run sorts once, at the start)
  * (counting sort carrying each particle's Lagrangian index).  mode
  * FPM_BIN_CHUNKS steps the sorted particles in equal chunks, painting into
  * the density directly with warp-summed deposits of neighbouring lanes;

@@ -272,7 +272,7 @@ def test_autotune_picks_and_caches(fpm):
     best = min(ms, key=lambda k: ms[k])
     names = {'walk': (0, 1, 1), 'chunks16/4': (16, 4, 1),
              'chunks16/6': (16, 6, 1), 'chunks16/10': (16, 10, 1),
-             'chunks16/16': (16, 16, 1), 'chunks8/10': (8, 10, 1),
+             'chunks16/16': (16, 16, 1), 'chunks16/once': (16, 1 << 20, 1),
              'flow16': (16, 1, 3), 'tiles16/4': (16, 4, 0)}
     assert choice == names[best]
     outs = {}
