@@ -23,6 +23,24 @@
 // checkpoints, intermediate states) are written through the carried index.
 #include "fpm_bin.cuh"
 
+// Lanes of k_step_sorted that deposit into the same base cell sum their
+// weights with a segmented shuffle reduction and deposit once (1), or each
+// lane deposits its own (0).
+#ifndef FPM_SORTED_SEGSUM
+#define FPM_SORTED_SEGSUM 1
+#endif
+// k_step_sorted paints through a shared-memory box of cells around its
+// chunk (1) or straight into the density (0).  Measured on B200 (particles
+// re-sorted every 16 steps; step kernels per 40-step simulation): 4.12 ms
+// with the box against 2.99 ms without at 128^3, 28.9 against 20.7 ms at
+// 256^3 -- the shared-memory atomics, the barriers and the flush of each
+// chunk cost more than the L2 reductions they save, once runs of lanes in
+// one cell already deposit once (the segmented sums; without them the
+// step takes 3.46 ms at 128^3).
+#ifndef FPM_SORTED_BOX
+#define FPM_SORTED_BOX 0
+#endif
+
 namespace fpm {
 
 namespace {
@@ -344,6 +362,16 @@ __device__ __forceinline__ int rel_cell(int c, int o, int m) {
   return r + T / 2;
 }
 
+// Offset of periodic cell c from a box origin o on an axis of m cells: the
+// representative of c - o (mod m) in (-m/2, m/2], so a box no larger than
+// the mesh sees every cell at most once; the caller tests 0 <= r < size.
+__device__ __forceinline__ int box_rel(int c, int o, int m) {
+  int r = c - o;
+  if (r > (m >> 1)) r -= m;
+  else if (r <= -(m >> 1)) r += m;
+  return r;
+}
+
 // The binned leapfrog step: one tile of T^3 force-mesh cells per block
 // iteration.  Per particle the arithmetic is k_step's (readout, closing
 // kick, opening kick, drift, paint), in the same order and rounding.  The
@@ -479,9 +507,19 @@ k_step_binned(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
 // (5 steps) and only the run's first lane issues the reductions.  The sums
 // of a run are formed in a different order than one deposit at a time
 // (FP32 rounding, as any order of the reference's scatter).
+template <bool BOX>
 __global__ void __launch_bounds__(kThreads, FPM_STEP_MINBLOCKS)
 k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
               int64_t nchunks, BinStepArgs b) {
+  // BOX: the paint goes into a shared-memory box of cells around the
+  // chunk (BX x-planes from the first particle's cell less two, and the
+  // y and z extent of its 16^3 tile with a margin: z from four before, so
+  // the box flushes as aligned float4), then into rho with one 16-byte
+  // vector reduction per non-zero group of four; deposits outside the box
+  // go to rho directly.
+  constexpr int BX = 8, BY = 20, BZ = 24, BN = BX * BY * BZ;
+  __shared__ __align__(16) float box[BOX ? BN : 4];
+  __shared__ int box_org[3];
   pdl_wait();  // the force meshes of the solve before
   const StepArgs& a = b.a;
   const int lane = threadIdx.x & 31;
@@ -501,6 +539,27 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
     float* m = a.rho + S.m_off;
     const int64_t first = S.p_off + (ch - S.ch_p) * kChunk;
     const int64_t end = S.p_off + S.np;
+    int bx0 = 0, by0 = 0, bz0 = 0;
+    if (BOX && !last) {  // uniform over the block
+      if (threadIdx.x == 0) {
+        int fi, fj, fk;
+        if (b.blag) {
+          unpack_site(b.blag[first], S.qkb, S.qjb, fi, fj, fk);
+        } else {
+          lattice_ijk(S, first - S.p_off, fi, fj, fk);
+        }
+        const float3 fx = mesh_pos(S, fi, fj, fk, ld3(b.bd, first));
+        box_org[0] = cic_axis(fx.x, S.mx).i0 - 2;
+        box_org[1] = (cic_axis(fx.y, S.my).i0 & ~15) - 2;
+        box_org[2] = (cic_axis(fx.z, S.mz).i0 & ~15) - 4;
+      }
+      for (int q = threadIdx.x; q < BN / 4; q += kThreads)
+        reinterpret_cast<float4*>(box)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncthreads();
+      bx0 = box_org[0];
+      by0 = box_org[1];
+      bz0 = box_org[2];
+    }
 #pragma unroll 1
     for (int item = 0; item < kItems; ++item) {
       const int64_t i = first + item * kThreads + threadIdx.x;
@@ -608,7 +667,8 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
         w[2 * q] = __fmul_rn(c1.wxy[q], c1.wz0);
         w[2 * q + 1] = __fmul_rn(c1.wxy[q], c1.wz1);
       }
-      const unsigned heads = __ballot_sync(0xffffffffu, head);
+      const unsigned heads =
+          FPM_SORTED_SEGSUM ? __ballot_sync(0xffffffffu, head) : 0xffffffffu;
       if (heads != 0xffffffffu) {
         // segmented sums over runs of contiguous lanes with equal keys (a
         // key can recur in a later run after the particles drifted since
@@ -629,13 +689,50 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
           }
         }
       }
-      if (valid && head) {
+      if (valid && (head || !FPM_SORTED_SEGSUM)) {
+        if (BOX) {
+          const int rx0 = box_rel(nx1.i0, bx0, S.mx),
+                    rx1 = box_rel(nx1.i1, bx0, S.mx),
+                    ry0 = box_rel(ny1.i0, by0, S.my),
+                    ry1 = box_rel(ny1.i1, by0, S.my),
+                    rz0 = box_rel(nz1.i0, bz0, S.mz),
+                    rz1 = box_rel(nz1.i1, bz0, S.mz);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          red_add(m + c1.row[q] + c1.z0, w[2 * q]);
-          red_add(m + c1.row[q] + c1.z1, w[2 * q + 1]);
+          for (int q = 0; q < 4; ++q) {
+            const int rx = (q & 1) ? rx1 : rx0, ry = (q >> 1) ? ry1 : ry0;
+            const bool in = (unsigned)rx < (unsigned)BX &&
+                            (unsigned)ry < (unsigned)BY;
+            float* t = box + (rx * BY + ry) * BZ;
+            if (in && (unsigned)rz0 < (unsigned)BZ)
+              atomicAdd(t + rz0, w[2 * q]);
+            else
+              red_add(m + c1.row[q] + c1.z0, w[2 * q]);
+            if (in && (unsigned)rz1 < (unsigned)BZ)
+              atomicAdd(t + rz1, w[2 * q + 1]);
+            else
+              red_add(m + c1.row[q] + c1.z1, w[2 * q + 1]);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            red_add(m + c1.row[q] + c1.z0, w[2 * q]);
+            red_add(m + c1.row[q] + c1.z1, w[2 * q + 1]);
+          }
         }
       }
+    }
+    if (BOX && !last) {  // flush the box
+      __syncthreads();
+      for (int q = threadIdx.x; q < BN / 4; q += kThreads) {
+        const float4 v = reinterpret_cast<const float4*>(box)[q];
+        if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+        const int zg = q % (BZ / 4), row = q / (BZ / 4);
+        const int cy = wrap_near(by0 + row % BY, S.my);
+        const int cx = wrap_near(bx0 + row / BY, S.mx);
+        const int cz = wrap_near(bz0 + 4 * zg, S.mz);
+        red_add_f4(m + ((int64_t)cx * S.my + cy) * S.mz + cz, v);
+      }
+      __syncthreads();  // the next chunk zeroes the box
     }
   }
 }
@@ -645,8 +742,13 @@ k_step_sorted(const SimDev* __restrict__ sims, int nsims, int64_t ch0,
 void launch_step_sorted(const SimDev* sims, int nsims, int64_t ch0,
                         int64_t ch1, const BinStepArgs& b, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  launch_pdl(k_step_sorted, dim3(grid_for(ch1 - ch0)), dim3(kThreads), 0, st,
-             sims, nsims, ch0, ch1, b);
+  // the shared-memory box follows tiles of 16 cells
+  if (FPM_SORTED_BOX && b.tile_log2 == 4)
+    launch_pdl(k_step_sorted<true>, dim3(grid_for(ch1 - ch0)), dim3(kThreads),
+               0, st, sims, nsims, ch0, ch1, b);
+  else
+    launch_pdl(k_step_sorted<false>, dim3(grid_for(ch1 - ch0)),
+               dim3(kThreads), 0, st, sims, nsims, ch0, ch1, b);
 }
 
 void launch_step_binned(int tile, const SimDev* sims, int nsims, int64_t ch0,
