@@ -274,17 +274,26 @@ __device__ __forceinline__ bool adj_pos_setup(const SimDev& S, int s,
 
 // One particle of k_adj_position: its state in slot `slot` of the
 // per-particle arrays, its lattice site (i, j, k), and g its Lagrangian
-// slot in the checkpoints and lam_f.
+// slot in the checkpoints and lam_f.  AGG (particles sorted by cell, every
+// lane of the warp calling together, `valid` false past the end): lanes
+// whose force-VJP scatter starts from the same base cell sum their
+// deposits with segmented shuffles, corner by corner, and the run's first
+// lane deposits the sums once.
+template <bool AGG>
 __device__ __forceinline__ void adj_position_one(const SimDev& S,
                                                  const AdjArgs& a,
                                                  const AdjPos& c, int64_t slot,
                                                  int64_t g, int i, int j,
-                                                 int k) {
-  float3 d = ld3(a.disp, slot);
-  float3 lx = ld3(a.lam_x, slot);
-  float3 lp = ld3(a.lam_p, slot);
-  // rec: p_half of step it (left by the position after); else p_T
-  const float3 ph = ld3(a.mom, slot);
+                                                 int k, bool valid = true) {
+  const int lane = threadIdx.x & 31;
+  float3 d = make_float3(0.f, 0.f, 0.f), lx = d, lp = d, ph = d;
+  if (!AGG || valid) {
+    d = ld3(a.disp, slot);
+    lx = ld3(a.lam_x, slot);
+    lp = ld3(a.lam_p, slot);
+    // rec: p_half of step it (left by the position after); else p_T
+    ph = ld3(a.mom, slot);
+  }
   if (c.rec) {  // reverse drift from x_{it+1} (k_adj_drift_paint)
     const float3 gg = gather_grad(c.lr, S.mx, S.my, S.mz,
                                   mesh_pos(S, i, j, k, d));
@@ -298,19 +307,22 @@ __device__ __forceinline__ void adj_position_one(const SimDev& S,
     lp.x += c.dr * lx.x;
     lp.y += c.dr * lx.y;
     lp.z += c.dr * lx.z;
-    st3(a.disp, slot, d);
-    st3(a.lam_p, slot, lp);
+    if (!AGG || valid) {
+      st3(a.disp, slot, d);
+      st3(a.lam_p, slot, lp);
+    }
   }
   // force VJP at x_it (k_adj_vjp)
   float3 v = make_float3(c.cv * lp.x, c.cv * lp.y, c.cv * lp.z);
-  if (c.last && a.lam_f) {
+  if (c.last && a.lam_f && (!AGG || valid)) {
     const float3 lf = ld3(a.lam_f, g);
     v.x += lf.x;
     v.y += lf.y;
     v.z += lf.z;
   }
   const float3 y = mesh_pos(S, i, j, k, d);
-  if (!finite3(y.x, y.y, y.z)) atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
+  if ((!AGG || valid) && !finite3(y.x, y.y, y.z))
+    atomicOr(a.status, FPM_STATUS_NONFINITE_POS);
   const Axis ax = cic_axis(y.x, S.mx), ay = cic_axis(y.y, S.my),
              az = cic_axis(y.z, S.mz);
   const DAxis dx = cic_daxis(y.x), dy = cic_daxis(y.y), dz = cic_daxis(y.z);
@@ -320,6 +332,17 @@ __device__ __forceinline__ void adj_position_one(const SimDev& S,
   // 32-bit offsets inside the simulation's mesh (< 2^31 cells)
   const unsigned my = S.my, mz = S.mz;
   const unsigned rx0 = (unsigned)ax.i0 * my, rx1 = (unsigned)ax.i1 * my;
+  unsigned heads = 0xffffffffu, longest = 1;
+  if (AGG) {
+    const unsigned key = valid ? (rx0 + (unsigned)ay.i0) * mz +
+                                     (unsigned)az.i0
+                               : 0xffffffffu - lane;
+    heads = run_heads(key, lane);
+    if (heads != 0xffffffffu)
+      longest = __reduce_max_sync(
+          0xffffffffu,
+          (heads >> lane) & 1u ? (unsigned)run_length(heads, lane) : 1u);
+  }
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
     const int cx = conn_x(q), cy = conn_y(q), cz = conn_z(q);
@@ -334,12 +357,33 @@ __device__ __forceinline__ void adj_position_one(const SimDev& S,
     r2 = __fadd_rn(r2, __fmul_rn(a2, wc));
     grad_acc(ax, ay, az, dx, dy, dz, cx, cy, cz,
              v.x * a0 + v.y * a1 + v.z * a2, acc);
+    float t0 = u0 * wc, t1 = u1 * wc, t2 = u2 * wc;
+    if (AGG) {
+      // segmented sums over the runs: lane + o is in this lane's run when
+      // no run starts in (lane, lane + o]
+#pragma unroll 1
+      for (int off = 1; off < (int)longest; off <<= 1) {
+        const bool same =
+            lane + off < 32 &&
+            ((unsigned long long)heads >> (lane + 1) & ((1ull << off) - 1)) ==
+                0;
+        const float s0 = __shfl_down_sync(0xffffffffu, t0, off);
+        const float s1 = __shfl_down_sync(0xffffffffu, t1, off);
+        const float s2 = __shfl_down_sync(0xffffffffu, t2, off);
+        if (same) {
+          t0 = __fadd_rn(t0, s0);
+          t1 = __fadd_rn(t1, s1);
+          t2 = __fadd_rn(t2, s2);
+        }
+      }
+      if (!valid || !((heads >> lane) & 1u)) continue;
+    }
     if (a.lvec4) {
-      red_add_v4(c.l0 + 4 * o, u0 * wc, u1 * wc, u2 * wc);
+      red_add_v4(c.l0 + 4 * o, t0, t1, t2);
     } else {
-      red_add(c.l0 + o, u0 * wc);
-      red_add(c.l0 + c.mcells + o, u1 * wc);
-      red_add(c.l0 + 2 * c.mcells + o, u2 * wc);
+      red_add(c.l0 + o, t0);
+      red_add(c.l0 + c.mcells + o, t1);
+      red_add(c.l0 + 2 * c.mcells + o, t2);
     }
   }
   const float3 f = make_float3(__fmul_rn(__fmul_rn(r0, c.fac), c.invb),
@@ -348,6 +392,7 @@ __device__ __forceinline__ void adj_position_one(const SimDev& S,
   lx.x += c.fac * acc.x;
   lx.y += c.fac * acc.y;
   lx.z += c.fac * acc.z;
+  if (AGG && !valid) return;
   st3(a.lam_x, slot, lx);
   // p_it (rec: p_half - ks F_it, or the checkpoint; else p_T), then
   // p_half of step it-1 for the next position
@@ -390,7 +435,7 @@ k_adj_position(const SimDev* __restrict__ sims, int nsims, int64_t nchunks,
       int64_t local;
       if (!walk_particle(S, w, item, i, j, k, local)) continue;
       const int64_t g = S.p_off + local;
-      adj_position_one(S, a, c, g, g, i, j, k);
+      adj_position_one<false>(S, a, c, g, g, i, j, k);
     }
   }
 }
@@ -416,12 +461,15 @@ k_adj_position_sorted(const SimDev* __restrict__ sims, int nsims,
 #pragma unroll 1
     for (int item = 0; item < kItems; ++item) {
       const int64_t i = first + item * kThreads + threadIdx.x;
-      if (i >= end) break;
-      const uint32_t l = a.lag[i];
-      int qi, qj, qk;
-      unpack_site(l, S.qkb, S.qjb, qi, qj, qk);
-      adj_position_one(S, a, c, i, S.p_off + site_local(S, qi, qj, qk), qi,
-                       qj, qk);
+      // every lane of the warp takes part (warp-uniform except in a sim's
+      // last chunk, where lanes past the end only join the shuffles)
+      const bool valid = i < end;
+      if (!FPM_ADJ_SORTED_SEGSUM && !valid) break;  // no warp-wide steps
+      int qi = 0, qj = 0, qk = 0;
+      if (valid) unpack_site(a.lag[i], S.qkb, S.qjb, qi, qj, qk);
+      adj_position_one<FPM_ADJ_SORTED_SEGSUM != 0>(
+          S, a, c, i, S.p_off + site_local(S, qi, qj, qk), qi, qj, qk,
+          valid);
     }
   }
 }

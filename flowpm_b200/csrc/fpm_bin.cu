@@ -106,24 +106,8 @@ __device__ __forceinline__ uint32_t particle_key(const BinRun& R,
   return (uint32_t)r * (uint32_t)R.ncell + cell_key<T>(R, cx, cy, cz);
 }
 
-// Lanes of a warp with equal keys in a row form a run (a sorted input
-// makes the particles of a cell contiguous); the run's first lane (its
-// head) adds or claims for the whole run.  Returns the mask of heads;
-// lanes past the end carry keys of their own (kSentinel - lane).
+// Keys of lanes past the end of a sort's input (kSentinel - lane).
 constexpr uint32_t kSentinel = 0xffffffffu;
-__device__ __forceinline__ unsigned run_heads(uint32_t key, int lane) {
-  const uint32_t up = __shfl_up_sync(0xffffffffu, key, 1);
-  return __ballot_sync(0xffffffffu, lane == 0 || up != key);
-}
-// Lanes from this head to the next head.
-__device__ __forceinline__ int run_length(unsigned heads, int lane) {
-  const unsigned above = heads & ~((2u << lane) - 1u);
-  return (above ? __ffs(above) - 1 : 32) - lane;
-}
-// The head of this lane's run.
-__device__ __forceinline__ int run_head(unsigned heads, int lane) {
-  return 31 - __clz(heads & ((2u << lane) - 1u));
-}
 
 // Chunks of kChunk slots per simulation: the sort kernels walk chunks, so
 // that the simulation of a slot is known per chunk.
