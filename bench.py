@@ -61,10 +61,31 @@ ADJ_SORT_PERIODS = (4, 8, 1 << 20)  # 1 << 20: sorted once, at the start
 ADJ_TILE = 16
 # seed of replica r's linear field: replicas.replica_seed(1000, r)
 REPLICA_SEED_BASE = 1000
-# Accuracy of the C4 gradient at full size, from the offline check against
-# the FP64 oracle (python tests/c4_gradient_check.py export / check); filled
-# in from its summary.
-GRAD_CHECK_C4 = None
+# Accuracy of the C4 gradient at full size (128^3, 20 steps, checkpoints
+# every 5), from the offline check against the FP64 oracle:
+#   python tests/c4_gradient_check.py export C4.npz        (GPU)
+#   python tests/c4_gradient_check.py check C4.npz R.json  (8 host cores,
+#       32 random unit directions, FP64 central differences at three steps)
+# Relative errors per direction, median and max over the 32; the largest
+# comes from the direction whose projection is smallest (0.043 against a
+# median of 1.30), where the oracle's FP32 tape (the reference's own
+# arithmetic) is as far from FP64.
+GRAD_CHECK_C4 = {
+    'directions': 32,
+    'fp64_tape_rel_l2': {'rebuilt': 8.52e-4, 'tape': 8.69e-4,
+                         'oracle_fp32_tape': 1.30e-3},
+    'vs_fp64_tape': {'rebuilt': {'median': 7.50e-4, 'max': 5.85e-2},
+                     'tape': {'median': 6.42e-4, 'max': 5.35e-2},
+                     'oracle_fp32_tape': {'median': 1.28e-3,
+                                          'max': 5.18e-2}},
+    'fd64_vs_fp64_tape': {'eps_1e-3': {'median': 5.94e-5, 'max': 2.21e-3},
+                          'eps_1e-4': {'median': 4.24e-6, 'max': 2.79e-4},
+                          'eps_1e-5': {'median': 3.19e-6, 'max': 8.54e-5}},
+    'gpu_vs_fd64_eps_1e-4': {'rebuilt': {'median': 7.49e-4, 'max': 5.82e-2},
+                             'tape': {'median': 6.40e-4, 'max': 5.33e-2}},
+    'loss': {'gpu_fp32': 2097898.25, 'fp64': 2097898.2496},
+    'eps': 'relative to the linear field standard deviation',
+}
 # Error of a simulation at the C5 spacing against the oracle, from
 # python tests/c5_fp64_check.py (256^3, box 500 Mpc/h, Planck15, seed 5120,
 # 30 steps; the oracle cannot run 512^3 in reasonable time on the host).
