@@ -253,10 +253,11 @@ int fpm_pgd(fpm_plan* plan, float* disp, const double* params, void* stream);
  * arrays stay in Lagrangian
  * order; the results equal the lattice walk's up to the order of the
  * density's FP32 sums.  tile 0 returns to the lattice walk.  Allocates 56
- * bytes per particle and 4 per force-mesh cell (freed by tile 0 or
+ * bytes per particle and 8 per force-mesh cell (freed by tile 0 or
  * fpm_plan_destroy), synchronising the device; every force mesh must divide
- * into tiles (else FPM_ERR_UNSUPPORTED).  Plans with PGD switched on keep
- * the lattice walk.  Captured graphs of the plan must be captured again. */
+ * into tiles, and each simulation's lattice site must pack into 32 bits
+ * (else FPM_ERR_UNSUPPORTED).  Plans with PGD switched on keep the lattice
+ * walk.  Captured graphs of the plan must be captured again. */
 enum {
   FPM_BIN_TILES = 0,
   FPM_BIN_CHUNKS = 1,
@@ -288,8 +289,9 @@ int fpm_plan_set_adjoint_binning(fpm_plan* plan, int sort_every);
  * the state (disp, mom: total_particles x 3, left unchanged), one graph
  * replay of fpm_nbody_run for each of FPM_TUNE_CONFIGS configurations --
  * the lattice walk; the binned step (fpm_plan_set_binning) in chunks with
- * keys in tiles of 8 cells re-sorted every 1, 2 or 4 steps and of 16 cells
- * every 2 or 4; in shared-memory tiles of 8 or 16 cells every 4 -- keeping
+ * keys in tiles of 16 cells re-sorted every 4, 6, 10 or 16 steps, or sorted
+ * once at the start; re-sorted as the particles move (FPM_BIN_FLOW); in
+ * shared-memory tiles of 16 cells every 4 steps -- keeping
  * the best of reps timed replays after one warm-up, and leaves the fastest
  * set on the plan.  choice[0..2] = its (tile, sort_every, mode); ms
  * (FPM_TUNE_CONFIGS
