@@ -345,11 +345,13 @@ def test_adjoint_xpass_vs_cufft(fpm, tape):
   path (FPM_PLAN_CUFFT, a memset per position).  Both are FP32 with the
   same CIC conventions, so they differ by transform rounding only, which
   the reverse integration amplifies where a particle sits next to a cell
-  face (the weight derivative jumps there): a few 1e-4 with the stored
-  potentials, up to ~2e-3 with rebuilt forces.  A missing clear of the
-  adjoint force mesh would give O(1).  (On meshes this elongated the FP32
-  gradient sits ~5e-3 from the FP64 oracle's on either path, for the same
-  reason.)"""
+  face (the weight derivative jumps there): usually below 1e-4.  The
+  order of the FP32 reductions into the meshes also varies from run to
+  run, and on some runs of either path that flips one particle across a
+  face, which moves the cotangents by 1.6e-3 (measured on the B200 over
+  repeated runs of the same path).  A missing clear of the adjoint force
+  mesh would give O(1).  (On meshes this elongated the FP32 gradient sits
+  ~5e-3 from the FP64 oracle's on either path, for the same reason.)"""
   from flowpm_b200 import _lib
   rng = np.random.default_rng(43)
   nc = (256, 16, 16)
@@ -362,7 +364,7 @@ def test_adjoint_xpass_vs_cufft(fpm, tape):
   lp0 = t(rng.standard_normal((2 * n, 3)))
   a = _run_adjoint(sims, d0, p0, lx0, lp0, tape, nc)
   b = _run_adjoint(sims, d0, p0, lx0, lp0, tape, nc, _lib.FPM_PLAN_CUFFT)
-  tol = 1e-3 if tape else 1e-2
+  tol = 5e-3 if tape else 1e-2
   for u, v in zip(a, b):
     assert np.isfinite(u).all()
     assert rel_l2(u, v) < tol, rel_l2(u, v)
