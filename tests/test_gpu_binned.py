@@ -46,7 +46,8 @@ def binned(fpm):
     p.set_binning(0)
 
 
-MODES = [(8, 1, 1), (16, 3, 1), (8, 4, 0), (16, 2, 0), (16, 1, 3), (8, 1, 3)]
+MODES = [(8, 1, 1), (16, 3, 1), (8, 4, 0), (16, 2, 0), (16, 1, 3), (8, 1, 3),
+         (16, 1 << 20, 1)]
 
 
 @pytest.mark.parametrize('tile,every,mode', MODES)
