@@ -190,6 +190,49 @@ def test_capi_rejects_bad_arguments(fpm):
                              0, None) == 1
 
 
+def test_c_host_builds_and_calls_the_library(fpm, tmp_path):
+  """A C99 host (no C++) includes include/flowpm_b200.h, links
+  libflowpm_b200.so and calls it the way a non-Python caller of the
+  drop-in would: version, error text, and argument checks that return
+  before any device work (so it runs without a GPU)."""
+  import shutil
+  import subprocess
+  if shutil.which('gcc') is None:
+    pytest.skip('no C compiler')
+  src = tmp_path / 'host.c'
+  src.write_text(r"""
+#include <stdio.h>
+#include <string.h>
+#include "flowpm_b200.h"
+int main(void) {
+  fpm_plan* plan = NULL;
+  int32_t dims[4] = {16, 16, 16, 0};   /* pm_nc_factor 0: rejected */
+  if (fpm_version() < 100) return 2;
+  if (strcmp(fpm_error_string(FPM_ERR_ARG), "invalid argument") != 0)
+    return 3;
+  if (fpm_plan_create(&plan, 1, dims, 0.0, 0) != FPM_ERR_ARG) return 4;
+  if (fpm_cic_paint(NULL, 1, 8, 8, 8, NULL, 10, NULL, NULL) != FPM_ERR_ARG)
+    return 5;
+  if (fpm_plan_set_binning(NULL, 16, 4, FPM_BIN_CHUNKS) != FPM_ERR_ARG)
+    return 6;
+  if (fpm_pk_bin_noalloc(NULL, 1, 8, 8, 8, NULL, 0.0, 0.1, 4, NULL, NULL) !=
+      FPM_ERR_ARG)
+    return 7;
+  printf("ok %d\n", fpm_version());
+  return 0;
+}
+""")
+  libdir = os.path.dirname(fpm._lib.LIB_PATH)
+  exe = tmp_path / 'host'
+  cmd = ['gcc', '-std=c99', '-Wall', '-Werror', '-o', str(exe), str(src),
+         '-I', os.path.join(ROOT, 'include'), '-L', libdir, '-lflowpm_b200',
+         '-Wl,-rpath,' + libdir]
+  subprocess.run(cmd, check=True, capture_output=True)
+  out = subprocess.run([str(exe)], capture_output=True, text=True)
+  assert out.returncode == 0, (out.returncode, out.stderr)
+  assert out.stdout.startswith('ok ')
+
+
 def test_product_does_not_import_oracle():
   """The product package never references the oracle."""
   pkg = os.path.join(ROOT, 'flowpm_b200')
